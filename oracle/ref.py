@@ -1,0 +1,159 @@
+"""ctypes binding of the oracle harness (oracle/_ref/libmdtkref.so).
+
+Test infrastructure only: imported by tests/, by __graft_entry__.smoke() as
+the checker, and by bench.py's CPU-baseline leg.  The library is the reference
+MDTK code compiled from its own sources (see oracle/Makefile); nothing in the
+product imports this module.
+
+Units at this interface: Angstrom, eV, fs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libmdtkref.so")
+
+POT_REBO = 1
+POT_AIREBO_LJ = 2
+POT_ETORS = 4
+POT_BRENNER = 8
+POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run `make -C oracle`)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_create.restype = vp
+        L.ref_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.ref_destroy.argtypes = [vp]
+        L.ref_num_potentials.argtypes = [vp]
+        L.ref_set_atoms.argtypes = [vp, ctypes.c_int, ip, dp, dp, dp, ip, ctypes.POINTER(ctypes.c_ubyte)]
+        L.ref_compute.argtypes = [vp, dp, dp, dp, dp]
+        L.ref_energy_proxy.argtypes = [vp, dp, dp]
+        L.ref_nl_pairs.restype = ctypes.c_long
+        L.ref_nl_pairs.argtypes = [vp, ctypes.c_int, ip, ctypes.c_long]
+        L.ref_rcutoff.restype = ctypes.c_double
+        L.ref_rcutoff.argtypes = [vp, ctypes.c_int]
+        L.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, ip, dp, dp, dp]
+        L.ref_tables.restype = ctypes.c_long
+        L.ref_tables.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_long]
+        L.ref_spline_eval.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _check(rc):
+    if rc is None or (isinstance(rc, int) and rc < 0):
+        raise RuntimeError("oracle: " + lib().ref_last_error().decode())
+    return rc
+
+
+class RefSystem:
+    """One reference SimLoop with a potential stack and an atom set."""
+
+    def __init__(self, potset: int, brenner_set: int = 1, lj_cut_mode: int = 0):
+        h = lib().ref_create(potset, brenner_set, lj_cut_mode)
+        if not h:
+            raise RuntimeError("oracle: " + lib().ref_last_error().decode())
+        self.h = ctypes.c_void_p(h)
+        self.n = 0
+        self.npot = lib().ref_num_potentials(self.h)
+
+    def close(self):
+        if self.h:
+            lib().ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_atoms(self, z, pos, vel=None, box=(0.0, 0.0, 0.0), pbc=(1, 1, 1), fixed=None):
+        z = np.ascontiguousarray(z, dtype=np.int32)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = len(z)
+        velp = None
+        if vel is not None:
+            self._vel = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
+            velp = _dp(self._vel)
+        boxa = np.ascontiguousarray(box, dtype=np.float64)
+        pbca = np.ascontiguousarray(pbc, dtype=np.int32)
+        fx = None
+        if fixed is not None:
+            self._fixed = np.ascontiguousarray(fixed, dtype=np.uint8)
+            fx = self._fixed.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
+        _check(lib().ref_set_atoms(self.h, n, _ip(z), _dp(pos), velp, _dp(boxa), _ip(pbca), fx))
+        self.n = n
+
+    def compute(self, per_term: bool = False):
+        """Returns (E_total, E_terms[npot], grad[n,3]) (+ grad_terms[npot,n,3])."""
+        e = np.zeros(1)
+        et = np.zeros(self.npot)
+        g = np.zeros((self.n, 3))
+        gt = np.zeros((self.npot, self.n, 3)) if per_term else None
+        _check(lib().ref_compute(self.h, _dp(e), _dp(et), _dp(g), _dp(gt) if per_term else None))
+        if per_term:
+            return float(e[0]), et, g, gt
+        return float(e[0]), et, g
+
+    def nl_pairs(self, index: int) -> np.ndarray:
+        cnt = lib().ref_nl_pairs(self.h, index, None, 0)
+        _check(cnt)
+        out = np.zeros((max(cnt, 1), 2), dtype=np.int32)
+        _check(lib().ref_nl_pairs(self.h, index, _ip(out), cnt))
+        return out[:cnt]
+
+    def rcutoff(self, index: int) -> float:
+        return float(lib().ref_rcutoff(self.h, index))
+
+    def run(self, nsteps: int, dt_fs: float):
+        """Unmodified SimLoop::execute; returns dict of final state + per-step energies."""
+        pos = np.zeros((self.n, 3))
+        vel = np.zeros((self.n, 3))
+        img = np.zeros((self.n, 3), dtype=np.int32)
+        ep = np.zeros(nsteps)
+        et = np.zeros(nsteps)
+        e0 = np.zeros(1)
+        _check(lib().ref_run(self.h, nsteps, dt_fs, _dp(pos), _dp(vel), _ip(img), _dp(ep), _dp(et), _dp(e0)))
+        return {"pos": pos, "vel": vel, "image": img, "epot": ep, "etot": et, "e0": float(e0[0])}
+
+
+def tables(which: int, brenner_set: int = 1) -> np.ndarray:
+    n = lib().ref_tables(which, brenner_set, None, 0)
+    _check(n)
+    out = np.zeros(n)
+    _check(lib().ref_tables(which, brenner_set, _dp(out), n))
+    return out
+
+
+def spline_eval(fn: int, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(len(x))
+    _check(lib().ref_spline_eval(fn, len(x), _dp(x), _dp(out)))
+    return out

@@ -1,0 +1,511 @@
+/*
+ * Oracle harness: a C ABI over the reference MDTK library compiled from its
+ * own sources (test infrastructure only; loaded by tests/ and by bench.py's
+ * CPU-baseline leg, never by the product).
+ *
+ * It drives the unmodified reference code:
+ *   - potential stacks built as applications/common.h:36-77 does
+ *     (REBO, REBO+AIREBO-LJ+ETors, Brenner set 1/2);
+ *   - FProxy::operator() for energy and gradient (mdtk/potentials/FProxy.cxx:46-61);
+ *   - NeighbourList::Update for the pair sets (mdtk/potentials/NeighbourList.cxx:32-107);
+ *   - SimLoop::execute with dt fixed through the reference's own
+ *     doBeforeIteration hook (mdtk/SimLoop.hpp:46, SimLoop.cxx:254) and file
+ *     output off (SimLoop.hpp:49).
+ * Units at this ABI: Angstrom, eV, fs, amu-free (masses are the reference's:
+ * C 12 amu, H 1 amu, mdtk/Atom.hpp:104-105).  Conversions use the reference's
+ * own constants (mdtk/consts.cxx:28-36).
+ */
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <sstream>
+#include <iostream>
+#include <map>
+#include <set>
+
+#include <mdtk/SimLoop.hpp>
+#include <mdtk/potentials/manybody/AIREBO/REBO.hpp>
+#include <mdtk/potentials/manybody/AIREBO/AIREBO_LJ.hpp>
+#include <mdtk/potentials/manybody/AIREBO/AIREBO_ETors.hpp>
+#include <mdtk/potentials/manybody/Brenner/Brenner.hpp>
+
+using namespace mdtk;
+
+namespace {
+
+std::string g_last_error;
+
+enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8 };
+
+class FixedDtLoop : public SimLoop
+{
+public:
+  Float fixed_dt;
+  Float ekin_before;
+  std::vector<double> epot_log, etot_log;
+  FixedDtLoop() : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0) {}
+  virtual void doBeforeIteration()
+  {
+    dt = fixed_dt;
+    ekin_before = energyKin();
+  }
+  virtual void doAfterIteration()
+  {
+    // check.currentEnergy = Epot(x_{n+1}) + Ekin(v_n) (SimLoop.cxx:337 precedes :392)
+    Float epot = check.currentEnergy - ekin_before;
+    epot_log.push_back(epot / eV);
+    etot_log.push_back((epot + energyKin()) / eV);
+  }
+};
+
+struct RefCtx
+{
+  FixedDtLoop loop;
+  int potset;
+  int brenner_set;
+  std::vector<std::string> names;
+  REBO* rebo;
+  AIREBO* lj;
+  ETors* etors;
+  Brenner* brenner;
+  bool nl_ready;
+  RefCtx() : potset(0), brenner_set(1), rebo(0), lj(0), etors(0), brenner(0), nl_ready(false) {}
+};
+
+ElementID el_from_z(int z)
+{
+  if (z == 1) return H_EL;
+  if (z == 6) return C_EL;
+  throw Exception("unknown element (only H=1 and C=6 are on this path)");
+}
+
+void ensure_nl(RefCtx* c)
+{
+  if (c->nl_ready) return;
+  c->loop.atoms.prepareForSimulatation();
+  c->loop.fpot.NL_init(c->loop.atoms);
+  c->loop.fpot.NL_UpdateIfNeeded(c->loop.atoms);
+  c->nl_ready = true;
+}
+
+FGeneral* pot_at(RefCtx* c, int index)
+{
+  if (index < 0 || index >= (int)c->loop.fpot.potentials.size()) return 0;
+  return c->loop.fpot.potentials[index];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_last_error.c_str(); }
+
+void ref_set_verbose(int on) { yaatk::verboseTrace = (on != 0); }
+
+/* potset: bitmask of REBO(1) | AIREBO_LJ(2) | ETORS(4) | BRENNER(8).
+ * The AIREBO LJ term needs REBO (it holds a reference to it, AIREBO_LJ.cxx:204-212).
+ * lj_cut_mode 0 = the reference's cosine cutoff (AIREBO_LJ.cxx:249-262);
+ * lj_cut_mode 1 = cutoff at 3*sigma_CC/3*sigma_CH/3*sigma_HH with a 0.5 A switch. */
+void* ref_create(int potset, int brenner_set, int lj_cut_mode)
+{
+  try {
+    yaatk::verboseTrace = false;
+    RefCtx* c = new RefCtx();
+    c->potset = potset;
+    c->brenner_set = brenner_set;
+    c->loop.preventFileOutput = true;
+    if (potset & POT_REBO) {
+      c->rebo = new REBO();
+      c->loop.fpot.addPotential(c->rebo);
+      c->names.push_back("REBO");
+    }
+    if (potset & POT_AIREBO_LJ) {
+      if (!c->rebo) throw Exception("AIREBO LJ needs REBO");
+      c->lj = new AIREBO(c->rebo);
+      if (lj_cut_mode == 1) {
+        for (int a = 0; a < 2; a++)
+          for (int b = 0; b < 2; b++) {
+            c->lj->R_[a][b][0] = 3.0 * c->lj->sigma_[a][b] - 0.5 * Ao;
+            c->lj->R_[a][b][1] = 3.0 * c->lj->sigma_[a][b];
+          }
+        c->lj->nl.Rcutoff = c->lj->getRcutoff();
+      }
+      c->loop.fpot.addPotential(c->lj);
+      c->names.push_back("AIREBO_LJ");
+    }
+    if (potset & POT_ETORS) {
+      c->etors = new ETors();
+      c->loop.fpot.addPotential(c->etors);
+      c->names.push_back("ETors");
+    }
+    if (potset & POT_BRENNER) {
+      c->brenner = new Brenner(brenner_set == 2 ? Brenner::POTENTIAL2 : Brenner::POTENTIAL1);
+      c->loop.fpot.addPotential(c->brenner);
+      c->names.push_back("Brenner");
+    }
+    return c;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return 0;
+  }
+}
+
+void ref_destroy(void* h) { delete (RefCtx*)h; }
+
+int ref_num_potentials(void* h) { return (int)((RefCtx*)h)->loop.fpot.potentials.size(); }
+
+/* box[a] is the period along axis a in Angstrom; pbc_on[a] = 0 means NO_PBC on
+ * that axis (mdtk/consts.cxx:40).  Positions in Angstrom, velocities in A/fs. */
+int ref_set_atoms(void* h, int n, const int* z, const double* pos, const double* vel,
+                  const double* box, const int* pbc_on, const unsigned char* fixed)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    c->loop.atoms.clear();
+    c->loop.atoms.reserve(n);
+    const Float vconv = Ao / fs;
+    for (int i = 0; i < n; i++) {
+      Atom a(el_from_z(z[i]),
+             Vector3D(pos[3 * i] * Ao, pos[3 * i + 1] * Ao, pos[3 * i + 2] * Ao),
+             vel ? Vector3D(vel[3 * i] * vconv, vel[3 * i + 1] * vconv, vel[3 * i + 2] * vconv)
+                 : Vector3D(0, 0, 0));
+      c->loop.atoms.push_back(a);
+      if (fixed && fixed[i]) c->loop.atoms.back().fix();
+    }
+    Vector3D pbc(pbc_on[0] ? box[0] * Ao : NO_PBC.x,
+                 pbc_on[1] ? box[1] * Ao : NO_PBC.y,
+                 pbc_on[2] ? box[2] * Ao : NO_PBC.z);
+    c->loop.atoms.PBC(pbc);
+    c->nl_ready = false;
+    return 0;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* Energy (eV) and dE/dx (eV/A) through FProxy::operator().  e_terms[p] gets
+ * each potential's energy and, when grad_terms is non-null, grad_terms[p*3n..]
+ * its own gradient; grad gets the total.  Positions are read after the
+ * reference's prepareForSimulatation wrap (applyPBC). */
+int ref_compute(void* h, double* e_total, double* e_terms, double* grad, double* grad_terms)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    ensure_nl(c);
+    AtomsArray& at = c->loop.atoms;
+    const size_t n = at.size();
+    const Float gconv = Ao / eV;
+    Float etot = 0.0;
+    for (size_t i = 0; i < n; i++) at[i].grad = Vector3D(0, 0, 0);
+    std::vector<Vector3D> total(n, Vector3D(0, 0, 0));
+    for (size_t p = 0; p < c->loop.fpot.potentials.size(); p++) {
+      for (size_t i = 0; i < n; i++) at[i].grad = Vector3D(0, 0, 0);
+      Float e = (*c->loop.fpot.potentials[p])(at);
+      etot += e;
+      if (e_terms) e_terms[p] = e / eV;
+      for (size_t i = 0; i < n; i++) {
+        total[i] += at[i].grad;
+        if (grad_terms) {
+          grad_terms[p * 3 * n + 3 * i + 0] = at[i].grad.x * gconv;
+          grad_terms[p * 3 * n + 3 * i + 1] = at[i].grad.y * gconv;
+          grad_terms[p * 3 * n + 3 * i + 2] = at[i].grad.z * gconv;
+        }
+      }
+    }
+    if (e_total) *e_total = etot / eV;
+    if (grad)
+      for (size_t i = 0; i < n; i++) {
+        grad[3 * i + 0] = total[i].x * gconv;
+        grad[3 * i + 1] = total[i].y * gconv;
+        grad[3 * i + 2] = total[i].z * gconv;
+      }
+    return 0;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* Energy through FProxy::operator() exactly (one summed value, as SimLoop sees it). */
+int ref_energy_proxy(void* h, double* e_total, double* grad)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    ensure_nl(c);
+    AtomsArray& at = c->loop.atoms;
+    Float e = c->loop.fpot(at);
+    if (e_total) *e_total = e / eV;
+    if (grad)
+      for (size_t i = 0; i < at.size(); i++) {
+        grad[3 * i + 0] = at[i].grad.x * Ao / eV;
+        grad[3 * i + 1] = at[i].grad.y * Ao / eV;
+        grad[3 * i + 2] = at[i].grad.z * Ao / eV;
+      }
+    return 0;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* Neighbour-list pairs (i<j) of potential `index` after a fresh build.
+ * Writes up to cap pairs as (i, j) int32; returns the total count. */
+long ref_nl_pairs(void* h, int index, int* pairs, long cap)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    ensure_nl(c);
+    FGeneral* p = pot_at(c, index);
+    if (!p) { g_last_error = "bad potential index"; return -1; }
+    AtomsArray& at = c->loop.atoms;
+    long cnt = 0;
+    for (size_t i = 0; i < at.size(); i++) {
+      AtomRefsContainer& l = p->nl.nl[i];
+      for (size_t q = 0; q < l.size(); q++) {
+        size_t j = l[q]->globalIndex;
+        if (j <= i) continue;
+        if (cnt < cap) { pairs[2 * cnt] = (int)i; pairs[2 * cnt + 1] = (int)j; }
+        cnt++;
+      }
+    }
+    return cnt;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+double ref_rcutoff(void* h, int index)
+{
+  FGeneral* p = pot_at((RefCtx*)h, index);
+  return p ? p->getRcutoff() / Ao : -1.0;
+}
+
+/* Unmodified SimLoop::execute for nsteps steps of fixed dt (fs).  Returns the
+ * final wrapped positions (A), velocities (A/fs), image counters, and per-step
+ * potential and total energies (eV) with E_{n+1} = Epot(x_{n+1}) + Ekin(v_{n+1}). */
+int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* image,
+            double* epot_steps, double* etot_steps, double* e0)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    FixedDtLoop& L = c->loop;
+    L.fixed_dt = dt_fs * fs;
+    L.dt = L.fixed_dt;
+    L.simTime = 0.0;
+    L.iteration = 0;
+    L.simTimeFinal = dt_fs * fs * (nsteps - 0.5);
+    L.simTimeSaveTrajInterval = 1e9 * ps;
+    L.epot_log.clear();
+    L.etot_log.clear();
+    int rc = L.execute();
+    if (rc != 0) { g_last_error = "SimLoop::execute failed"; return -1; }
+    if ((int)L.epot_log.size() != nsteps) {
+      std::ostringstream os;
+      os << "ran " << L.epot_log.size() << " steps instead of " << nsteps;
+      g_last_error = os.str();
+      return -1;
+    }
+    if (e0) *e0 = L.check.initialEnergy / eV;
+    AtomsArray& at = L.atoms;
+    const Float vconv = fs / Ao;
+    for (size_t i = 0; i < at.size(); i++) {
+      if (pos) { pos[3*i] = at[i].coords.x / Ao; pos[3*i+1] = at[i].coords.y / Ao; pos[3*i+2] = at[i].coords.z / Ao; }
+      if (vel) { vel[3*i] = at[i].V.x * vconv; vel[3*i+1] = at[i].V.y * vconv; vel[3*i+2] = at[i].V.z * vconv; }
+      if (image) { image[3*i] = at[i].PBC_count.x; image[3*i+1] = at[i].PBC_count.y; image[3*i+2] = at[i].PBC_count.z; }
+    }
+    for (int s = 0; s < nsteps; s++) {
+      if (epot_steps) epot_steps[s] = L.epot_log[s];
+      if (etot_steps) etot_steps[s] = L.etot_log[s];
+    }
+    c->nl_ready = true;
+    return 0;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"
+
+/* ---- spline tables, in the layout the product builds its own copy in ----
+ * Every stored coefficient is multiplier*c of one SplineTerm (the first factor
+ * SplineTerm::operator() forms, mdtk/SplineAux.hpp:82-94), zero when either is
+ * zero, in the SplineMultiD term order (x0 fastest, SplineAux.hpp:179-206). */
+
+static void put_multi(const SplineMultiD& s, std::vector<double>& out, size_t nterms)
+{
+  for (size_t t = 0; t < nterms; t++) {
+    if (t < s.terms.size()) {
+      const SplineTerm& tt = s.terms[t];
+      out.push_back((tt.multiplier == 0.0 || tt.c == 0.0) ? 0.0 : tt.multiplier * tt.c);
+    } else out.push_back(0.0);
+  }
+}
+
+static void put_G(const FuncG& g, std::vector<double>& out)
+{
+  // 4 pieces x (x1, x2, f[6], df[6])
+  for (int p = 0; p < 4; p++) {
+    if (p < g.splineCount) {
+      out.push_back(g.spline[p].x_[0]);
+      out.push_back(g.spline[p].x_[1]);
+      put_multi(g.spline[p].f, out, 6);
+      put_multi(g.spline[p].dfdx, out, 6);
+    } else {
+      for (int q = 0; q < 14; q++) out.push_back(0.0);
+    }
+  }
+}
+
+template <class FP>
+static void put_P(const FP& f, std::vector<double>& out)
+{
+  for (int h = 0; h < 4; h++)
+    for (int c = 0; c < 4; c++) {
+      put_multi(f.spline[h][c].f, out, 16);
+      put_multi(f.spline[h][c].dfdx, out, 16);
+      put_multi(f.spline[h][c].dfdy, out, 16);
+    }
+}
+
+template <class FP>
+static void put_P_intarg(const FP& f, std::vector<double>& out)
+{
+  for (int h = 0; h < 4; h++)
+    for (int c = 0; c < 4; c++) {
+      out.push_back(f.intarg[h][c]);
+      out.push_back(f.dH_intarg[h][c]);
+      out.push_back(f.dC_intarg[h][c]);
+    }
+}
+
+static void put_T(const Func_pi_rc& f, std::vector<double>& out)
+{
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++)
+      for (int k = 0; k < 16; k++) {
+        put_multi(f.spline[i][j][k].f, out, 64);
+        put_multi(f.spline[i][j][k].dfdx, out, 64);
+        put_multi(f.spline[i][j][k].dfdy, out, 64);
+        put_multi(f.spline[i][j][k].dfdz, out, 64);
+      }
+}
+
+static void put_T_intarg(const Func_pi_rc& f, std::vector<double>& out)
+{
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++)
+      for (int k = 0; k < 16; k++) {
+        out.push_back(f.intarg[i][j][k]);
+        out.push_back(f.di_intarg[i][j][k]);
+        out.push_back(f.dj_intarg[i][j][k]);
+        out.push_back(f.dk_intarg[i][j][k]);
+      }
+}
+
+extern "C" {
+
+/* which: 0 = REBO tables (G_C1, G_C2, G_H, P_CC, P_CH, P intarg CC/CH,
+ *            pi_rc CC/CH/HH, Tij, their intarg tables);
+ *        1 = Brenner tables of the given parameter set (H_CC, H_CH, F).
+ * Returns the number of doubles (writes at most cap). */
+long ref_tables(int which, int brenner_set, double* out, long cap)
+{
+  try {
+    std::vector<double> v;
+    if (which == 0) {
+      REBO r;
+      put_G(r.funcG_C1, v);
+      put_G(r.funcG_C2, v);
+      put_G(r.funcG_H, v);
+      put_P(r.funcP_CC, v);
+      put_P(r.funcP_CH, v);
+      put_P_intarg(r.funcP_CC, v);
+      put_P_intarg(r.funcP_CH, v);
+      put_T(r.func_pi_rc_CC, v);
+      put_T(r.func_pi_rc_CH, v);
+      put_T(r.func_pi_rc_HH, v);
+      put_T(r.func_Tij, v);
+      put_T_intarg(r.func_pi_rc_CC, v);
+      put_T_intarg(r.func_pi_rc_CH, v);
+      put_T_intarg(r.func_pi_rc_HH, v);
+      put_T_intarg(r.func_Tij, v);
+    } else {
+      Brenner b(brenner_set == 2 ? Brenner::POTENTIAL2 : Brenner::POTENTIAL1);
+      for (int h = 0; h < 4; h++)
+        for (int c = 0; c < 4; c++) {
+          put_multi(b.funcH_CC.spline[h][c].f, v, 16);
+          put_multi(b.funcH_CC.spline[h][c].dfdx, v, 16);
+          put_multi(b.funcH_CC.spline[h][c].dfdy, v, 16);
+        }
+      for (int h = 0; h < 4; h++)
+        for (int c = 0; c < 4; c++) {
+          put_multi(b.funcH_CH.spline[h][c].f, v, 16);
+          put_multi(b.funcH_CH.spline[h][c].dfdx, v, 16);
+          put_multi(b.funcH_CH.spline[h][c].dfdy, v, 16);
+        }
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+          for (int k = 0; k < 5; k++) {
+            put_multi(b.funcF.spline[i][j][k].f, v, 64);
+            put_multi(b.funcF.spline[i][j][k].dfdx, v, 64);
+            put_multi(b.funcF.spline[i][j][k].dfdy, v, 64);
+            put_multi(b.funcF.spline[i][j][k].dfdz, v, 64);
+          }
+    }
+    for (long i = 0; i < (long)v.size() && i < cap; i++) out[i] = v[i];
+    return (long)v.size();
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* Spline function values through the reference's own evaluators, for
+ * known-answer checks: fn 0..2 = G_C1/G_C2/G_H(x0) value, 3..5 their dCosT;
+ * 10/11/12 = P_CC value/dH/dC(x0,x1); 13/14/15 = P_CH;
+ * 20+4f+d = pi_rc CC(f=0)/CH(1)/HH(2)/Tij(3), d = value/di/dj/dk at (x0,x1,x2). */
+int ref_spline_eval(int fn, int n, const double* x, double* out)
+{
+  try {
+    static REBO* r = 0;
+    if (!r) r = new REBO();
+    for (int q = 0; q < n; q++) {
+      const double* a = x + 3 * q;
+      double v = 0.0;
+      if (fn == 0) v = r->funcG_C1(a[0]);
+      else if (fn == 1) v = r->funcG_C2(a[0]);
+      else if (fn == 2) v = r->funcG_H(a[0]);
+      else if (fn == 3) v = r->funcG_C1.dCosT(a[0]);
+      else if (fn == 4) v = r->funcG_C2.dCosT(a[0]);
+      else if (fn == 5) v = r->funcG_H.dCosT(a[0]);
+      else if (fn == 10) v = r->funcP_CC(a[0], a[1]);
+      else if (fn == 11) v = r->funcP_CC.dH(a[0], a[1]);
+      else if (fn == 12) v = r->funcP_CC.dC(a[0], a[1]);
+      else if (fn == 13) v = r->funcP_CH(a[0], a[1]);
+      else if (fn == 14) v = r->funcP_CH.dH(a[0], a[1]);
+      else if (fn == 15) v = r->funcP_CH.dC(a[0], a[1]);
+      else if (fn >= 20 && fn < 36) {
+        int f = (fn - 20) / 4, d = (fn - 20) % 4;
+        const Func_pi_rc* F = f == 0 ? (const Func_pi_rc*)&r->func_pi_rc_CC
+                            : f == 1 ? (const Func_pi_rc*)&r->func_pi_rc_CH
+                            : f == 2 ? (const Func_pi_rc*)&r->func_pi_rc_HH
+                                     : (const Func_pi_rc*)&r->func_Tij;
+        if (d == 0) v = (*F)(a[0], a[1], a[2]);
+        else if (d == 1) v = F->di(a[0], a[1], a[2]);
+        else if (d == 2) v = F->dj(a[0], a[1], a[2]);
+        else v = F->dk(a[0], a[1], a[2]);
+      } else { g_last_error = "bad spline id"; return -1; }
+      out[q] = v;
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"
