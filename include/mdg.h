@@ -1,0 +1,151 @@
+/*
+ * mdg: B200-native MDTK hot path (REBO / Brenner bond-order forces, AIREBO
+ * Lennard-Jones and torsion terms, Verlet neighbour lists, velocity Verlet)
+ * behind a plain C ABI.
+ *
+ * Every entry point returns an int status (MDG_OK = 0, negative = error) and
+ * never throws; mdg_last_error() returns the message of the last failure on
+ * the calling thread.  Contexts are independent; a context is used by one
+ * host thread at a time.
+ *
+ * The entry points replace the reference's potential interface
+ * (mdtk/potentials/FGeneral.hpp:54-114, aggregated by FProxy,
+ * mdtk/potentials/FProxy.hpp:31-112) and the SimLoop step body
+ * (mdtk/SimLoop.cxx:252-445); each declaration names the reference function
+ * it stands in for.
+ */
+#ifndef MDG_H
+#define MDG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mdg_ctx mdg_ctx;
+
+/* ---- status codes ---- */
+#define MDG_OK 0
+#define MDG_ERR_ARG (-1)            /* bad argument (replaces REQUIRE on inputs) */
+#define MDG_ERR_CUDA (-2)           /* CUDA runtime failure or no device */
+#define MDG_ERR_NL_OVERFLOW (-3)    /* a Verlet list exceeded its capacity */
+#define MDG_ERR_BOND_OVERFLOW (-4)  /* an atom has more REBO bonds than the bond capacity */
+#define MDG_ERR_COS_RANGE (-5)      /* cos(theta) outside [-1-1e-7, 1+1e-7] (FGeneral.hpp:147) */
+#define MDG_ERR_N_NEGATIVE (-6)     /* coordination below -1e-15 (REBO.cxx:434) */
+#define MDG_ERR_NONFINITE (-7)      /* non-finite energy or force */
+#define MDG_ERR_CAPACITY (-8)       /* connectivity / special-pair / record capacity exceeded */
+#define MDG_ERR_SPLINE_DOMAIN (-9)  /* spline argument out of its domain (cubici.hpp:90,211,305) */
+#define MDG_ERR_STATE (-10)         /* call out of order (e.g. compute before set_system) */
+#define MDG_ERR_TIMEOUT (-11)       /* a bounded device wait gave up */
+
+/* ---- potential selection (bitmask) ---- */
+#define MDG_POT_REBO 1        /* REBO (AIREBO/REBO.cxx) */
+#define MDG_POT_AIREBO_LJ 2   /* AIREBO LJ term (AIREBO/AIREBO_LJ.cxx); needs MDG_POT_REBO */
+#define MDG_POT_ETORS 4       /* AIREBO torsion (AIREBO/AIREBO_ETors.cxx) */
+#define MDG_POT_BRENNER 8     /* first-generation Brenner (Brenner/Brenner.cxx) */
+#define MDG_POT_AIREBO (MDG_POT_REBO | MDG_POT_AIREBO_LJ | MDG_POT_ETORS)
+
+/* ---- units at this ABI ---- */
+#define MDG_UNITS_AEVFS 0  /* Angstrom, Angstrom/fs, eV, eV/Angstrom, fs */
+#define MDG_UNITS_CGS 1    /* cm, cm/s, erg, erg/cm, s (the reference's units) */
+
+/* ---- precision ---- */
+#define MDG_PREC_FP64 0        /* everything in FP64 */
+#define MDG_PREC_FP32_MIXED 1  /* FP32 bond-order / LJ arithmetic, FP64 accumulation and integration */
+
+typedef struct mdg_params {
+  int potentials;     /* MDG_POT_* bitmask */
+  int brenner_set;    /* Brenner parameter set 1 or 2 (Brenner::POTENTIAL1/2) */
+  int precision;      /* MDG_PREC_* */
+  int units;          /* MDG_UNITS_* */
+  int lj_cut_mode;    /* 0: reference cosine cutoff 5.0-5.5/4.5-5.0/4.0-4.5 A; 1: 3 sigma */
+  int nl_skin_mode;   /* 0: list range 1.44 Rcut, rebuild at 0.44 Rcut (NeighbourList.cxx:29);
+                         1: list range Rcut + nl_skin, rebuild at nl_skin */
+  double nl_skin;     /* absolute skin in Angstrom for nl_skin_mode 1 */
+  int cap_rebo_list;  /* Verlet-list capacities (partners per atom); 0 = default */
+  int cap_lj_list;
+  int cap_bonds;      /* REBO bonds per atom; 0 = default (16) */
+  int cap_cij;        /* connectivity targets per atom; 0 = default */
+  int cap_special;    /* LJ pairs per atom needing b* or a connectivity gradient; 0 = default */
+  int device;         /* CUDA device ordinal */
+} mdg_params;
+
+/* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */
+void mdg_default_params(mdg_params* p);
+
+/* Create a context (replaces constructing the potentials: REBO::REBO
+ * REBO.cxx:816-854, AIREBO::AIREBO AIREBO_LJ.cxx:204-212, ETors::ETors
+ * AIREBO_ETors.cxx:117-122, Brenner::Brenner Brenner.cxx:474-496; the spline
+ * tables are built once on the host and uploaded). */
+int mdg_create(const mdg_params* p, mdg_ctx** out);
+
+/* Free every device and host resource of the context (FProxy::freePotentials,
+ * FProxy.hpp:49-53). */
+int mdg_destroy(mdg_ctx* ctx);
+
+/* Message of the last error on this thread (yaatk::Exception::what). */
+const char* mdg_last_error(void);
+
+/* Launch all work on this CUDA stream (cudaStream_t passed as void*; NULL =
+ * the context's own stream). */
+int mdg_set_stream(mdg_ctx* ctx, void* stream);
+
+/* Load an atom set (AtomsArray with its PBC, AtomsContainer.hpp:31-104, plus
+ * AtomsArray::prepareForSimulatation AtomsContainer.cxx:107-123: positions are
+ * wrapped into the box on periodic axes and image counters start at 0).
+ * z: atomic numbers (1 = H, 6 = C); pos, vel: [n*3]; box: periods;
+ * pbc[a] != 0 marks a periodic axis; fixed: NULL or [n] flags (Atom::fix).
+ * Neighbour lists are built on the next evaluation (FGeneral::NL_init). */
+int mdg_set_system(mdg_ctx* ctx, int n, const int32_t* z, const double* pos, const double* vel,
+                   const double box[3], const int32_t pbc[3], const uint8_t* fixed);
+
+/* Replace positions (same atoms, same order).  Lists are rebuilt only when
+ * the displacement criterion fires (NeighbourList::MovedTooMuch,
+ * NeighbourList.cxx:109-133). */
+int mdg_set_positions(mdg_ctx* ctx, const double* pos);
+
+/* Energy and gradient of the configured potentials at the current positions
+ * (FProxy::operator(), FProxy.cxx:46-61).  e_total: total energy; e_terms
+ * (NULL or [4]): REBO or Brenner, AIREBO LJ, torsion, 0; grad (NULL or [n*3]):
+ * dE/dx is ADDED into it, as each potential adds into Atom::grad. */
+int mdg_compute(mdg_ctx* ctx, double* e_total, double* e_terms, double* grad);
+
+/* Sorted (i < j) pairs of a Verlet list after the last build: list_id 0 =
+ * REBO/Brenner/torsion list, 1 = AIREBO LJ list (NeighbourList::nl,
+ * NeighbourList.hpp:41-83).  Writes min(count, cap) pairs as int32 (i, j);
+ * *count gets the total. */
+int mdg_nl_pairs(mdg_ctx* ctx, int list_id, int32_t* pairs, int64_t cap, int64_t* count);
+
+/* Advance nsteps velocity-Verlet steps of fixed dt entirely on the device
+ * (SimLoop::executeMain step body, SimLoop.cxx:252-445, with dt fixed, no
+ * thermal bath).  epot/etot: NULL or [nsteps] per-step potential / total
+ * energies E(x_{n+1}, v_{n+1}).  Asynchronous on the context stream unless an
+ * energy array or a status check needs the host: pass NULL arrays and call
+ * mdg_sync() to collect the status. */
+int mdg_run(mdg_ctx* ctx, int nsteps, double dt, double* epot, double* etot);
+
+/* Wait for the context stream and report any device-side status. */
+int mdg_sync(mdg_ctx* ctx);
+
+/* Copy the state back (SimLoop atoms: coords, V, PBC_count).  Any NULL is skipped. */
+int mdg_get_state(mdg_ctx* ctx, double* pos, double* vel, int32_t* image);
+
+/* Replace positions and velocities of the loaded atoms (same order) from
+ * host memory; used by drivers that keep the state on the host. */
+int mdg_set_state(mdg_ctx* ctx, const double* pos, const double* vel);
+
+/* Number of kernels this context has launched so far. */
+int64_t mdg_launch_count(mdg_ctx* ctx);
+
+/* Test hook: the REBO spline tables the library built on the host, flattened
+ * in the oracle's export order; returns the number of doubles (writes at most
+ * cap).  Host only; needs no device. */
+int64_t mdg_debug_rebo_tables(double* out, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDG_H */

@@ -1,0 +1,202 @@
+"""mdtk_b200: the MDTK per-step hot path on one B200, behind the C ABI of
+include/mdg.h (library: mdtk_b200/libmdg.so, built by mdtk_b200.build).
+
+This module is a thin ctypes view of that ABI for tests and benchmarks.  It
+never computes anything itself: without the CUDA library (or without a GPU)
+every call fails loudly.
+
+    ctx = Context(potentials=POT_AIREBO)
+    ctx.set_system(z, pos, vel, box, pbc, fixed)
+    e, e_terms, grad = ctx.compute()          # FProxy::operator()
+    epot, etot = ctx.run(100, dt=0.25)        # SimLoop step loop, fixed dt
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdg.so")
+
+POT_REBO = 1
+POT_AIREBO_LJ = 2
+POT_ETORS = 4
+POT_BRENNER = 8
+POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
+
+UNITS_AEVFS = 0
+UNITS_CGS = 1
+PREC_FP64 = 0
+PREC_FP32_MIXED = 1
+
+
+class MdgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mdg error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("potentials", ctypes.c_int),
+        ("brenner_set", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("units", ctypes.c_int),
+        ("lj_cut_mode", ctypes.c_int),
+        ("nl_skin_mode", ctypes.c_int),
+        ("nl_skin", ctypes.c_double),
+        ("cap_rebo_list", ctypes.c_int),
+        ("cap_lj_list", ctypes.c_int),
+        ("cap_bonds", ctypes.c_int),
+        ("cap_cij", ctypes.c_int),
+        ("cap_special", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libmdg.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -c 'import __graft_entry__ as g; g.build()'`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.mdg_default_params.argtypes = [ctypes.POINTER(Params)]
+        L.mdg_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+        L.mdg_destroy.argtypes = [vp]
+        L.mdg_last_error.restype = ctypes.c_char_p
+        L.mdg_set_stream.argtypes = [vp, vp]
+        L.mdg_set_system.argtypes = [vp, ctypes.c_int, i32p, dp, dp, dp, i32p, ctypes.POINTER(ctypes.c_uint8)]
+        L.mdg_set_positions.argtypes = [vp, dp]
+        L.mdg_set_state.argtypes = [vp, dp, dp]
+        L.mdg_compute.argtypes = [vp, dp, dp, dp]
+        L.mdg_nl_pairs.argtypes = [vp, ctypes.c_int, i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        L.mdg_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
+        L.mdg_sync.argtypes = [vp]
+        L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
+        L.mdg_launch_count.argtypes = [vp]
+        L.mdg_launch_count.restype = ctypes.c_int64
+        L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
+        L.mdg_debug_rebo_tables.restype = ctypes.c_int64
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise MdgError(rc, lib().mdg_last_error().decode())
+
+
+def debug_rebo_tables() -> np.ndarray:
+    n = lib().mdg_debug_rebo_tables(None, 0)
+    out = np.zeros(n)
+    lib().mdg_debug_rebo_tables(_dp(out), n)
+    return out
+
+
+class Context:
+    """One mdg context: a potential stack plus a loaded atom set."""
+
+    def __init__(self, potentials: int = POT_REBO, precision: int = PREC_FP64, units: int = UNITS_AEVFS,
+                 lj_cut_mode: int = 0, nl_skin_mode: int = 0, nl_skin: float = 0.3, brenner_set: int = 1,
+                 device: int = 0, **caps):
+        p = Params()
+        lib().mdg_default_params(ctypes.byref(p))
+        p.potentials = potentials
+        p.precision = precision
+        p.units = units
+        p.lj_cut_mode = lj_cut_mode
+        p.nl_skin_mode = nl_skin_mode
+        p.nl_skin = nl_skin
+        p.brenner_set = brenner_set
+        p.device = device
+        for k, v in caps.items():
+            setattr(p, k, v)
+        h = ctypes.c_void_p()
+        _check(lib().mdg_create(ctypes.byref(p), ctypes.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            lib().mdg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().mdg_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def set_system(self, z, pos, vel=None, box=(0, 0, 0), pbc=(1, 1, 1), fixed=None):
+        z = np.ascontiguousarray(z, dtype=np.int32)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        vel = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
+        box = np.ascontiguousarray(box, dtype=np.float64)
+        pbc = np.ascontiguousarray(pbc, dtype=np.int32)
+        fx = None
+        if fixed is not None:
+            fixed = np.ascontiguousarray(fixed, dtype=np.uint8)
+            fx = fixed.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        _check(lib().mdg_set_system(self.h, len(z), _ip(z), _dp(pos), _dp(vel), _dp(box), _ip(pbc), fx))
+        self.n = len(z)
+
+    def set_state(self, pos, vel=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)
+        _check(lib().mdg_set_state(self.h, _dp(pos), _dp(vel)))
+
+    def compute(self) -> Tuple[float, np.ndarray, np.ndarray]:
+        e = np.zeros(1)
+        et = np.zeros(4)
+        g = np.zeros((self.n, 3))
+        _check(lib().mdg_compute(self.h, _dp(e), _dp(et), _dp(g)))
+        return float(e[0]), et, g
+
+    def nl_pairs(self, list_id: int) -> np.ndarray:
+        cnt = ctypes.c_int64()
+        _check(lib().mdg_nl_pairs(self.h, list_id, None, 0, ctypes.byref(cnt)))
+        out = np.zeros((max(cnt.value, 1), 2), dtype=np.int32)
+        _check(lib().mdg_nl_pairs(self.h, list_id, _ip(out), cnt.value, ctypes.byref(cnt)))
+        return out[: cnt.value]
+
+    def run(self, nsteps: int, dt: float, energies: bool = True):
+        if energies:
+            ep = np.zeros(nsteps)
+            et = np.zeros(nsteps)
+            _check(lib().mdg_run(self.h, nsteps, dt, _dp(ep), _dp(et)))
+            return ep, et
+        _check(lib().mdg_run(self.h, nsteps, dt, None, None))
+        return None
+
+    def sync(self):
+        _check(lib().mdg_sync(self.h))
+
+    def get_state(self):
+        pos = np.zeros((self.n, 3))
+        vel = np.zeros((self.n, 3))
+        img = np.zeros((self.n, 3), dtype=np.int32)
+        _check(lib().mdg_get_state(self.h, _dp(pos), _dp(vel), _ip(img)))
+        return pos, vel, img
+
+    def launch_count(self) -> int:
+        return int(lib().mdg_launch_count(self.h))

@@ -1,0 +1,962 @@
+// mdg context, kernels and C ABI.
+//
+// One force evaluation (REBO [+ torsion] [+ AIREBO LJ]) on the device:
+//   disp check -> (conditional) cell-list Verlet rebuild -> bond list ->
+//   bond-order kernel (each bond from both ends) -> [LJ kernels] ->
+//   gather (deterministic per-atom force sum) -> integration / energy.
+// All launches go to one stream; list rebuilds are decided on the device, so
+// a device-resident MD run needs no host round trip per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mdg.h"
+#include "mdg_step.cuh"
+#include "mdg_tables.h"
+#include "mdg_lj.cuh"
+
+using namespace mdg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(MDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kThreads = 128;
+constexpr int kRedBlocks = 120;
+constexpr double kAo = 1e-8, kEv = 1.6021e-12, kFs = 1e-15;
+
+inline int nblk(int n, int t = kThreads) { return (n + t - 1) / t; }
+
+// ---------------------------------------------------------------- kernels
+
+__global__ void k_disp_partial(State S, NList L, double* part)
+{
+  __shared__ double s1[kThreads], s2[kThreads];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double d1 = 0.0, d2 = 0.0;
+  for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
+    double d = disp_atom(S, L, a);
+    if (d >= d1) { d2 = d1; d1 = d; }
+    else if (d >= d2) d2 = d;
+  }
+  s1[threadIdx.x] = d1;
+  s2[threadIdx.x] = d2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t1 = 0.0, t2 = 0.0;
+    for (int q = 0; q < blockDim.x; q++) {
+      double x[2] = {s1[q], s2[q]};
+      for (int z = 0; z < 2; z++) {
+        if (x[z] >= t1) { t2 = t1; t1 = x[z]; }
+        else if (x[z] >= t2) t2 = x[z];
+      }
+    }
+    part[2 * blockIdx.x] = t1;
+    part[2 * blockIdx.x + 1] = t2;
+  }
+}
+
+// need = force || top1 + top2 > trigger (NeighbourList::MovedTooMuch)
+__global__ void k_disp_final(const double* part, int nparts, double trigger, int* need, int* force)
+{
+  if (threadIdx.x != 0) return;
+  double t1 = 0.0, t2 = 0.0;
+  for (int q = 0; q < 2 * nparts; q++) {
+    double x = part[q];
+    if (x >= t1) { t2 = t1; t1 = x; }
+    else if (x >= t2) t2 = x;
+  }
+  int nd = (*force) || (t1 + t2 > trigger);
+  *need = nd;
+  *force = 0;
+}
+
+__global__ void k_cell_clear(Grid g, const int* need)
+{
+  if (!*need) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < g.ncell) { g.ccount[c] = 0; g.ccursor[c] = 0; }
+}
+
+__global__ void k_cell_count(State S, Grid g, const int* need)
+{
+  if (!*need) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < S.n) atomicAdd(&g.ccount[cell_of(g, S.box, S.pos[i])], 1);
+}
+
+// single-block exclusive scan of the cell counts
+__global__ void k_cell_scan(Grid g, const int* need)
+{
+  if (!*need) return;
+  __shared__ int part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  int chunk = (g.ncell + nt - 1) / nt;
+  int b = t * chunk, e = min(g.ncell, b + chunk);
+  int s = 0;
+  for (int c = b; c < e; c++) s += g.ccount[c];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    int acc = 0;
+    for (int q = 0; q < nt; q++) { int v = part[q]; part[q] = acc; acc += v; }
+    g.cstart[g.ncell] = acc;
+  }
+  __syncthreads();
+  int acc = part[t];
+  for (int c = b; c < e; c++) { g.cstart[c] = acc; acc += g.ccount[c]; }
+}
+
+__global__ void k_cell_fill(State S, Grid g, const int* need)
+{
+  if (!*need) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  int c = cell_of(g, S.box, S.pos[i]);
+  int slot = atomicAdd(&g.ccursor[c], 1);
+  g.catoms[g.cstart[c] + slot] = i;
+}
+
+// ascending atom order inside each cell (the fill order is racy)
+__global__ void k_cell_sort(Grid g, const int* need)
+{
+  if (!*need) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.ncell) return;
+  int b = g.cstart[c], e = g.cstart[c + 1];
+  isort(g.catoms + b, e - b);
+}
+
+__global__ void k_nl_build(State S, Grid g, NList L, const int* need, unsigned int* status)
+{
+  if (!*need) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < S.n) nl_build_atom(S, g, L, i, status);
+}
+
+__global__ void k_bonds(State S, NList L, ReboParams P, BondBuild B, unsigned int* status)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < S.n) bonds_atom(S, L, P, B, a, status);
+}
+
+__global__ void k_brev(BondBuild B)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < B.n) brev_atom(B, a);
+}
+
+__global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, TorsParams TP, int do_rebo,
+                       int do_tors, ForceOut O, unsigned int* status)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.n) return;
+  Rebo R{*P, *T, B, status};
+  rebo_atom(R, TP, do_rebo, do_tors, O, a);
+}
+
+__global__ void k_gather(BondList B, ForceOut O, int with_lj, const double4* gextra, double4* grad)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.n) return;
+  V3 g = gather_atom(B, O, a, with_lj, gextra);
+  grad[a] = make_double4(g.x, g.y, g.z, 0.0);
+}
+
+__global__ void k_verlet_pos(State S, double dt)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < S.n) verlet_pos_atom(S, dt, i);
+}
+
+// initial accelerations (SimLoop.cxx:305-321)
+__global__ void k_init_acc(State S, const double4* grad)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  if (S.fixed && S.fixed[i]) return;
+  double m = S.mass[i];
+  double4 g = grad[i];
+  S.acc[i] = make_double4(-g.x / m * kAccConv, -g.y / m * kAccConv, -g.z / m * kAccConv, 0.0);
+}
+
+__global__ void k_verlet_vel(State S, const double4* grad, double dt, double* ekin, unsigned int* status)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  double4 g = grad[i];
+  verlet_vel_atom(S, v3(g.x, g.y, g.z), dt, i, status);
+  double4 v = S.vel[i];
+  ekin[i] = S.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
+}
+
+__global__ void k_ekin(State S, double* ekin)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  double4 v = S.vel[i];
+  ekin[i] = S.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
+}
+
+// Deterministic sums of up to 4 per-atom arrays: fixed grid, fixed order.
+struct RedArgs {
+  const double* a[4];
+  int narr, n;
+};
+__global__ void k_reduce_partial(RedArgs R, double* part)
+{
+  __shared__ double sh[kThreads];
+  int which = blockIdx.y;
+  const double* x = R.a[which];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n; i += gridDim.x * blockDim.x) s += x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[which * gridDim.x + blockIdx.x] = sh[0];
+}
+// out[w] = sum of partials; also a finiteness check on the gradient sum
+__global__ void k_reduce_final(const double* part, int nparts, int narr, double* out, int slot_stride, int slot,
+                               unsigned int* status)
+{
+  int w = threadIdx.x;
+  if (w >= narr) return;
+  double s = 0.0;
+  for (int q = 0; q < nparts; q++) s += part[w * nparts + q];
+  out[slot * slot_stride + w] = s;
+  if (!isfinite(s)) atomicOr(status, ST_NONFINITE);
+}
+
+__global__ void k_finite(const double4* g, int n, unsigned int* status)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 v = g[i];
+  if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) atomicOr(status, ST_NONFINITE);
+}
+
+template <class T>
+T* dalloc(size_t count)
+{
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+  return (T*)p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- context
+
+struct mdg_ctx {
+  mdg_params prm;
+  ReboParams rp;
+  TorsParams tp;
+  LJParams ljp;
+  ReboTables* d_tables = nullptr;
+  ReboParams* d_rp = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int64_t launches = 0;
+
+  int n = 0;
+  Box box;
+  double unit_len = 1.0, unit_vel = 1.0, unit_e = 1.0, unit_grad = 1.0;
+
+  // state
+  double4 *pos = nullptr, *vel = nullptr, *acc = nullptr, *grad = nullptr;
+  int4* image = nullptr;
+  unsigned char* fixed = nullptr;
+  double* mass = nullptr;
+  bool acc_valid = false;
+
+  // lists: 0 = REBO range, 1 = LJ range
+  NList nl[2];
+  Grid grid[2];
+  int* d_need = nullptr;   // [2]
+  int* d_force = nullptr;  // [2]
+  double* d_part = nullptr;
+  double rcut[2] = {0, 0};
+  bool has_list[2] = {false, false};
+
+  // bonds
+  int mb = 16;
+  BondBuild bb;
+  ForceOut fo;
+  double* e_kin = nullptr;
+  double* d_red_part = nullptr;
+  double* d_energy = nullptr;   // [4] rebo, lj, tors, kin of the last evaluation
+  double* d_elog = nullptr;     // per-step energy log [cap * 4]
+  int elog_cap = 0;
+
+  LJState lj;
+
+  unsigned int* d_status = nullptr;
+
+  State S() const
+  {
+    State s;
+    s.n = n;
+    s.box = box;
+    s.pos = pos;
+    s.vel = vel;
+    s.acc = acc;
+    s.image = image;
+    s.fixed = fixed;
+    s.mass = mass;
+    return s;
+  }
+  BondList BL() const
+  {
+    BondList b;
+    b.n = n;
+    b.mb = mb;
+    b.nb = bb.nb;
+    b.bj = bb.bj;
+    b.brev = bb.brev;
+    b.brv = bb.brv;
+    b.bu = bb.bu;
+    b.bd = bb.bd;
+    b.nco = bb.nco;
+    return b;
+  }
+};
+
+namespace {
+
+void set_rebo_params(ReboParams& p)
+{
+  std::memset(&p, 0, sizeof(p));
+  const int C = kC, H = kH;
+  // REBO::setupPotential1 (REBO.cxx:857-938), converted to A / eV
+  p.Q[C][C] = 0.313460; p.Q[C][H] = p.Q[H][C] = 0.340776; p.Q[H][H] = 0.370471;
+  p.alpha[C][C] = 4.7465391; p.alpha[C][H] = p.alpha[H][C] = 4.1025498; p.alpha[H][H] = 3.5362986;
+  p.A[C][C] = 10953.544; p.A[C][H] = p.A[H][C] = 149.94099; p.A[H][H] = 32.817356;
+  p.B[0][C][C] = 12388.792; p.B[0][C][H] = p.B[0][H][C] = 32.355187; p.B[0][H][H] = 29.632593;
+  p.B[1][C][C] = 17.567065;
+  p.B[2][C][C] = 30.714932;
+  p.beta[0][C][C] = 4.7204523; p.beta[0][C][H] = p.beta[0][H][C] = 1.4344581; p.beta[0][H][H] = 1.7158922;
+  p.beta[1][C][C] = 1.4332132;
+  p.beta[2][C][C] = 1.3826913;
+  p.rho[C][H] = p.rho[H][C] = 1.09; p.rho[H][H] = 0.7415887;
+  p.R[C][C][0] = 1.7; p.R[H][H][0] = 1.1; p.R[C][H][0] = p.R[H][C][0] = 1.3;
+  p.R[C][C][1] = 2.0; p.R[H][H][1] = 1.7; p.R[C][H][1] = p.R[H][C][1] = 1.8;
+  p.Rp[C][C][0] = 1.7; p.Rp[H][H][0] = 1.1; p.Rp[C][H][0] = p.Rp[H][C][0] = 1.3;
+  p.Rp[C][C][1] = 2.0; p.Rp[H][H][1] = 1.7; p.Rp[C][H][1] = p.Rp[H][C][1] = 1.6;
+  p.Ntot[0] = 2;
+  p.Ntot[1] = 3;
+}
+
+void set_tors_params(TorsParams& t)
+{
+  // ETors::setupPotential (AIREBO_ETors.cxx:125-133)
+  t.eps[kC][kC] = 0.3079;
+  t.eps[kH][kH] = 0.1250;
+  t.eps[kC][kH] = t.eps[kH][kC] = 0.1787;
+}
+
+int launch_check(mdg_ctx* c)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return MDG_OK;
+}
+
+int status_to_code(unsigned int st, std::string& msg)
+{
+  if (st == 0) return MDG_OK;
+  msg = "device status:";
+  int code = MDG_OK;
+  auto add = [&](unsigned int bit, int c, const char* m) {
+    if (st & bit) { msg += std::string(" ") + m; if (code == MDG_OK) code = c; }
+  };
+  add(ST_NONFINITE, MDG_ERR_NONFINITE, "non-finite energy or force;");
+  add(ST_NL_OVERFLOW, MDG_ERR_NL_OVERFLOW, "Verlet list capacity exceeded;");
+  add(ST_BOND_OVERFLOW, MDG_ERR_BOND_OVERFLOW, "bond capacity exceeded;");
+  add(ST_COS_RANGE, MDG_ERR_COS_RANGE, "cos(theta) out of range;");
+  add(ST_N_NEGATIVE, MDG_ERR_N_NEGATIVE, "negative coordination;");
+  add(ST_SPLINE_DOMAIN, MDG_ERR_SPLINE_DOMAIN, "spline argument out of domain;");
+  add(ST_CIJ_OVERFLOW, MDG_ERR_CAPACITY, "connectivity table capacity exceeded;");
+  add(ST_SPECIAL_OVERFLOW, MDG_ERR_CAPACITY, "LJ special-pair capacity exceeded;");
+  add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "connectivity record capacity exceeded;");
+  add(ST_CELL_OVERFLOW, MDG_ERR_CAPACITY, "cell grid capacity exceeded;");
+  return code;
+}
+
+void free_system(mdg_ctx* c)
+{
+  void* ptrs[] = {c->pos, c->vel, c->acc, c->grad, c->image, c->fixed, c->mass,
+                  c->bb.nb, c->bb.bj, c->bb.brev, c->bb.brv, c->bb.bu, c->bb.bd, c->bb.nco,
+                  c->fo.A, c->fo.W, c->fo.gown, c->fo.glj, c->fo.e_rebo, c->fo.e_tors, c->fo.e_lj,
+                  c->e_kin, c->d_part, c->d_red_part, c->d_elog};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int l = 0; l < 2; l++) {
+    void* q[] = {c->nl[l].cnt, c->nl[l].list, c->nl[l].pos0, c->grid[l].ccount, c->grid[l].cstart,
+                 c->grid[l].ccursor, c->grid[l].catoms};
+    for (void* p : q)
+      if (p) cudaFree(p);
+    std::memset(&c->nl[l], 0, sizeof(NList));
+    std::memset(&c->grid[l], 0, sizeof(Grid));
+    c->has_list[l] = false;
+  }
+  lj_free(c->lj);
+  c->pos = c->vel = c->acc = c->grad = nullptr;
+  c->image = nullptr;
+  c->fixed = nullptr;
+  c->mass = nullptr;
+  std::memset(&c->bb, 0, sizeof(c->bb));
+  std::memset(&c->fo, 0, sizeof(c->fo));
+  c->e_kin = c->d_part = c->d_red_part = c->d_elog = nullptr;
+  c->elog_cap = 0;
+  c->n = 0;
+}
+
+// Cell grid for a list of the given range over the current box.
+int setup_grid(mdg_ctx* c, int l, const std::vector<double>& hpos)
+{
+  Grid& g = c->grid[l];
+  double range = std::sqrt(c->nl[l].range2);
+  g.brute = 0;
+  for (int ax = 0; ax < 3; ax++) {
+    if (c->box.pbc[ax]) {
+      int nc = (int)std::floor(c->box.L[ax] / range);
+      if (nc < 3) { g.brute = 1; nc = 1; }
+      g.nc[ax] = nc;
+      g.lo[ax] = 0.0;
+      g.cs[ax] = c->box.L[ax] / nc;
+    } else {
+      double lo = 1e300, hi = -1e300;
+      for (int i = 0; i < c->n; i++) {
+        lo = std::fmin(lo, hpos[3 * i + ax]);
+        hi = std::fmax(hi, hpos[3 * i + ax]);
+      }
+      lo -= 2 * range;
+      hi += 2 * range;
+      int nc = (int)std::floor((hi - lo) / range);
+      if (nc < 1) nc = 1;
+      if (nc > 1024) nc = 1024;
+      g.nc[ax] = nc;
+      g.lo[ax] = lo;
+      g.cs[ax] = (hi - lo) / nc;
+    }
+  }
+  if (g.brute) { g.nc[0] = g.nc[1] = g.nc[2] = 1; }
+  long nc = (long)g.nc[0] * g.nc[1] * g.nc[2];
+  if (nc > (1L << 26)) return fail(MDG_ERR_ARG, "cell grid too large");
+  g.ncell = (int)nc;
+  g.ccount = dalloc<int>(nc);
+  g.cstart = dalloc<int>(nc + 1);
+  g.ccursor = dalloc<int>(nc);
+  g.catoms = dalloc<int>(c->n);
+  if (!g.ccount || !g.cstart || !g.ccursor || !g.catoms) return fail(MDG_ERR_CUDA, "cudaMalloc (cell grid)");
+  return MDG_OK;
+}
+
+int rebuild_lists(mdg_ctx* c)
+{
+  State S = c->S();
+  int nparts = 64;
+  for (int l = 0; l < 2; l++) {
+    if (!c->has_list[l]) continue;
+    NList& L = c->nl[l];
+    Grid& g = c->grid[l];
+    int* need = c->d_need + l;
+    k_disp_partial<<<nparts, kThreads, 0, c->stream>>>(S, L, c->d_part);
+    k_disp_final<<<1, 32, 0, c->stream>>>(c->d_part, nparts, L.trigger, need, c->d_force + l);
+    c->launches += 2;
+    if (!g.brute) {
+      k_cell_clear<<<nblk(g.ncell), kThreads, 0, c->stream>>>(g, need);
+      k_cell_count<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, need);
+      k_cell_scan<<<1, 1024, 0, c->stream>>>(g, need);
+      k_cell_fill<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, need);
+      k_cell_sort<<<nblk(g.ncell), kThreads, 0, c->stream>>>(g, need);
+      c->launches += 5;
+    }
+    k_nl_build<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, L, need, c->d_status);
+    c->launches += 1;
+  }
+  return launch_check(c);
+}
+
+// One force evaluation at the current positions; leaves dE/dx in c->grad and
+// per-atom energies in c->fo.  Energies are summed into elog slot `slot`
+// (or d_energy when slot < 0).
+int evaluate(mdg_ctx* c)
+{
+  int rc = rebuild_lists(c);
+  if (rc) return rc;
+  State S = c->S();
+  const int pot = c->prm.potentials;
+  const bool rebo = pot & MDG_POT_REBO, tors = pot & MDG_POT_ETORS, lj = pot & MDG_POT_AIREBO_LJ;
+  k_bonds<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->nl[0], c->rp, c->bb, c->d_status);
+  k_brev<<<nblk(c->n), kThreads, 0, c->stream>>>(c->bb);
+  c->launches += 2;
+  BondList B = c->BL();
+  k_rebo<<<nblk(c->n), kThreads, 0, c->stream>>>(c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0, tors ? 1 : 0, c->fo,
+                                                 c->d_status);
+  c->launches += 1;
+  const double4* gextra = nullptr;
+  if (lj) {
+    rc = lj_evaluate(c->lj, S, c->nl[1], B, c->d_rp, c->d_tables, c->ljp, c->fo, c->stream, c->d_status,
+                     &c->launches, &gextra);
+    if (rc) return fail(MDG_ERR_CUDA, "LJ evaluation launch failed");
+  }
+  k_gather<<<nblk(c->n), kThreads, 0, c->stream>>>(B, c->fo, lj ? 1 : 0, gextra, c->grad);
+  c->launches += 1;
+  return launch_check(c);
+}
+
+int reduce_energies(mdg_ctx* c, double* out_dev, int slot_stride, int slot, bool with_kin)
+{
+  RedArgs R;
+  R.a[0] = c->fo.e_rebo;
+  R.a[1] = c->fo.e_lj;
+  R.a[2] = c->fo.e_tors;
+  R.a[3] = c->e_kin;
+  R.narr = with_kin ? 4 : 3;
+  R.n = c->n;
+  k_reduce_partial<<<dim3(kRedBlocks, R.narr), kThreads, 0, c->stream>>>(R, c->d_red_part);
+  k_reduce_final<<<1, 32, 0, c->stream>>>(c->d_red_part, kRedBlocks, R.narr, out_dev, slot_stride, slot,
+                                          c->d_status);
+  c->launches += 2;
+  return launch_check(c);
+}
+
+int read_status(mdg_ctx* c)
+{
+  unsigned int st = 0;
+  CK(cudaMemcpyAsync(&st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    unsigned int z = 0;
+    CK(cudaMemcpy(c->d_status, &z, sizeof(z), cudaMemcpyHostToDevice));
+    std::string msg;
+    int code = status_to_code(st, msg);
+    return fail(code, msg);
+  }
+  return MDG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+void mdg_default_params(mdg_params* p)
+{
+  std::memset(p, 0, sizeof(*p));
+  p->potentials = MDG_POT_REBO;
+  p->brenner_set = 1;
+  p->precision = MDG_PREC_FP64;
+  p->units = MDG_UNITS_AEVFS;
+  p->nl_skin = 0.3;
+}
+
+const char* mdg_last_error(void) { return g_err.c_str(); }
+
+int mdg_create(const mdg_params* p, mdg_ctx** out)
+{
+  if (!p || !out) return fail(MDG_ERR_ARG, "null argument");
+  *out = nullptr;
+  if ((p->potentials & MDG_POT_AIREBO_LJ) && !(p->potentials & MDG_POT_REBO))
+    return fail(MDG_ERR_ARG, "the AIREBO LJ term needs REBO (AIREBO_LJ.cxx:204-212)");
+  if (p->potentials & MDG_POT_BRENNER) return fail(MDG_ERR_ARG, "Brenner is not available in this build");
+  if (p->precision != MDG_PREC_FP64) return fail(MDG_ERR_ARG, "only FP64 precision is available in this build");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(MDG_ERR_CUDA, "no CUDA device");
+  CK(cudaSetDevice(p->device));
+  mdg_ctx* c = new mdg_ctx();
+  c->prm = *p;
+  if (c->prm.cap_bonds <= 0) c->prm.cap_bonds = 16;
+  if (c->prm.cap_rebo_list <= 0) c->prm.cap_rebo_list = 64;
+  if (c->prm.cap_lj_list <= 0) c->prm.cap_lj_list = 512;
+  if (c->prm.cap_cij <= 0) c->prm.cap_cij = 128;
+  if (c->prm.cap_special <= 0) c->prm.cap_special = 64;
+  c->mb = c->prm.cap_bonds;
+  set_rebo_params(c->rp);
+  set_tors_params(c->tp);
+  set_lj_params(c->ljp, c->prm.lj_cut_mode);
+  if (p->units == MDG_UNITS_CGS) {
+    c->unit_len = 1.0 / kAo;          // cm -> A
+    c->unit_vel = kFs / kAo;          // cm/s -> A/fs
+    c->unit_e = kEv;                  // eV -> erg
+    c->unit_grad = kEv / kAo;         // eV/A -> erg/cm
+  }
+  ReboTables* h = new ReboTables();
+  build_rebo_tables(h, nullptr);
+  c->d_tables = dalloc<ReboTables>(1);
+  c->d_rp = dalloc<ReboParams>(1);
+  if (!c->d_tables || !c->d_rp) { delete h; mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc (tables)"); }
+  cudaMemcpy(c->d_tables, h, sizeof(ReboTables), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_rp, &c->rp, sizeof(ReboParams), cudaMemcpyHostToDevice);
+  delete h;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    mdg_destroy(c);
+    return fail(MDG_ERR_CUDA, "cudaStreamCreate");
+  }
+  c->stream = c->own_stream;
+  c->d_status = dalloc<unsigned int>(1);
+  c->d_need = dalloc<int>(2);
+  c->d_force = dalloc<int>(2);
+  c->d_energy = dalloc<double>(8);
+  if (!c->d_status || !c->d_need || !c->d_force || !c->d_energy) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc"); }
+  cudaMemset(c->d_status, 0, sizeof(unsigned int));
+  cudaMemset(c->d_need, 0, 2 * sizeof(int));
+  cudaMemset(c->d_force, 0, 2 * sizeof(int));
+  if (cudaGetLastError() != cudaSuccess) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "setup copies failed"); }
+  *out = c;
+  return MDG_OK;
+}
+
+int mdg_destroy(mdg_ctx* c)
+{
+  if (!c) return MDG_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_system(c);
+  void* ptrs[] = {c->d_tables, c->d_rp, c->d_status, c->d_need, c->d_force, c->d_energy};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return MDG_OK;
+}
+
+int mdg_set_stream(mdg_ctx* c, void* stream)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return MDG_OK;
+}
+
+int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const double* vel,
+                   const double box[3], const int32_t pbc[3], const uint8_t* fixed)
+{
+  if (!c || n <= 0 || !z || !pos || !box || !pbc) return fail(MDG_ERR_ARG, "bad argument");
+  free_system(c);
+  c->n = n;
+  for (int a = 0; a < 3; a++) {
+    c->box.pbc[a] = pbc[a] ? 1 : 0;
+    c->box.L[a] = c->box.pbc[a] ? box[a] * c->unit_len : 0.0;
+    if (c->box.pbc[a] && !(c->box.L[a] > 0)) return fail(MDG_ERR_ARG, "periodic axis with non-positive period");
+  }
+  // host-side packing: species, wrap (Atom::applyPBC), masses (Atom.hpp:104-105)
+  std::vector<double4> hp(n), hv(n), ha(n);
+  std::vector<int4> him(n);
+  std::vector<double> hm(n), hpos(3 * (size_t)n);
+  std::vector<unsigned char> hf(n, 0);
+  for (int i = 0; i < n; i++) {
+    int t;
+    if (z[i] == 6) t = kC;
+    else if (z[i] == 1) t = kH;
+    else return fail(MDG_ERR_ARG, "unknown element (REBO::e2i handles only H and C)");
+    double x[3];
+    int im[3] = {0, 0, 0};
+    for (int a = 0; a < 3; a++) {
+      x[a] = pos[3 * i + a] * c->unit_len;
+      if (!std::isfinite(x[a])) return fail(MDG_ERR_NONFINITE, "non-finite coordinate");
+      if (c->box.pbc[a] && !wrap1(x[a], im[a], c->box.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
+      hpos[3 * i + a] = x[a];
+    }
+    hp[i] = make_double4(x[0], x[1], x[2], (double)t);
+    hf[i] = (fixed && fixed[i]) ? 1 : 0;
+    if (vel && !hf[i])
+      hv[i] = make_double4(vel[3 * i] * c->unit_vel, vel[3 * i + 1] * c->unit_vel, vel[3 * i + 2] * c->unit_vel, 0.0);
+    else
+      hv[i] = make_double4(0, 0, 0, 0);
+    ha[i] = make_double4(0, 0, 0, 0);
+    him[i] = make_int4(im[0], im[1], im[2], 0);
+    hm[i] = (t == kC) ? 12.0 : 1.0;
+  }
+  // minimum image needs every period above twice the largest cutoff
+  // (SimLoop.cxx:239-245, AtomsArray::checkMIC)
+  double rmax = (c->prm.potentials & MDG_POT_AIREBO_LJ) ? c->ljp.R[0][0][1] : 2.0;
+  for (int a = 0; a < 3; a++)
+    if (c->box.pbc[a] && !(c->box.L[a] > 2.0 * rmax))
+      return fail(MDG_ERR_ARG, "Rcutoff is too large for given PBC (AtomsArray::checkMIC)");
+  c->pos = dalloc<double4>(n);
+  c->vel = dalloc<double4>(n);
+  c->acc = dalloc<double4>(n);
+  c->grad = dalloc<double4>(n);
+  c->image = dalloc<int4>(n);
+  c->fixed = dalloc<unsigned char>(n);
+  c->mass = dalloc<double>(n);
+  if (!c->pos || !c->vel || !c->acc || !c->grad || !c->image || !c->fixed || !c->mass)
+    return fail(MDG_ERR_CUDA, "cudaMalloc (state)");
+  CK(cudaMemcpy(c->pos, hp.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->vel, hv.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->acc, ha.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->image, him.data(), n * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->fixed, hf.data(), n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->mass, hm.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  c->acc_valid = false;
+
+  // neighbour lists (NeighbourList::Update range (1+0.44) Rcut, NeighbourList.cxx:65)
+  const bool with_lj = c->prm.potentials & MDG_POT_AIREBO_LJ;
+  c->rcut[0] = 2.0;  // REBO::getRcutoff = max R2 (REBO.hpp:147)
+  c->rcut[1] = with_lj ? std::fmax(std::fmax(c->ljp.R[0][0][1], c->ljp.R[0][1][1]), c->ljp.R[1][1][1]) : 0.0;
+  c->has_list[0] = true;
+  c->has_list[1] = with_lj;
+  for (int l = 0; l < 2; l++) {
+    if (!c->has_list[l]) continue;
+    NList& L = c->nl[l];
+    double range = c->prm.nl_skin_mode == 0 ? (1.0 + 0.44) * c->rcut[l] : c->rcut[l] + c->prm.nl_skin;
+    L.range2 = range * range;
+    L.trigger = c->prm.nl_skin_mode == 0 ? 0.44 * c->rcut[l] : c->prm.nl_skin;
+    L.cap = (l == 0) ? c->prm.cap_rebo_list : c->prm.cap_lj_list;
+    L.cnt = dalloc<int>(n);
+    L.list = dalloc<int>((size_t)n * L.cap);
+    L.pos0 = dalloc<double4>(n);
+    if (!L.cnt || !L.list || !L.pos0) return fail(MDG_ERR_CUDA, "cudaMalloc (neighbour list)");
+    int rc = setup_grid(c, l, hpos);
+    if (rc) return rc;
+  }
+  int one[2] = {1, 1};
+  CK(cudaMemcpy(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice));
+  c->d_part = dalloc<double>(2 * 64);
+
+  // bonds and force outputs
+  const int mb = c->mb;
+  c->bb.n = n;
+  c->bb.mb = mb;
+  c->bb.nb = dalloc<int>(n);
+  c->bb.bj = dalloc<int>((size_t)n * mb);
+  c->bb.brev = dalloc<int>((size_t)n * mb);
+  c->bb.brv = dalloc<double4>((size_t)n * mb);
+  c->bb.bu = dalloc<double4>((size_t)n * mb);
+  c->bb.bd = dalloc<double4>((size_t)n * mb);
+  c->bb.nco = dalloc<double4>(n);
+  c->fo.mb = mb;
+  c->fo.A = dalloc<double>((size_t)n * mb * 3);
+  c->fo.W = dalloc<double>((size_t)n * mb);
+  c->fo.gown = dalloc<double4>(n);
+  c->fo.glj = dalloc<double4>(n);
+  c->fo.e_rebo = dalloc<double>(n);
+  c->fo.e_tors = dalloc<double>(n);
+  c->fo.e_lj = dalloc<double>(n);
+  c->e_kin = dalloc<double>(n);
+  c->d_red_part = dalloc<double>(4 * kRedBlocks);
+  if (!c->bb.nb || !c->bb.bj || !c->bb.brev || !c->bb.brv || !c->bb.bu || !c->bb.bd || !c->bb.nco || !c->fo.A ||
+      !c->fo.W || !c->fo.gown || !c->fo.glj || !c->fo.e_rebo || !c->fo.e_tors || !c->fo.e_lj || !c->e_kin ||
+      !c->d_red_part)
+    return fail(MDG_ERR_CUDA, "cudaMalloc (bonds)");
+  CK(cudaMemset(c->fo.glj, 0, n * sizeof(double4)));
+  CK(cudaMemset(c->fo.e_lj, 0, n * sizeof(double)));
+  if (with_lj) {
+    int rc = lj_alloc(c->lj, n, c->prm.cap_cij, c->prm.cap_special, mb);
+    if (rc) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
+  }
+  CK(cudaDeviceSynchronize());
+  return MDG_OK;
+}
+
+int mdg_set_positions(mdg_ctx* c, const double* pos)
+{
+  return mdg_set_state(c, pos, nullptr);
+}
+
+int mdg_set_state(mdg_ctx* c, const double* pos, const double* vel)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  const int n = c->n;
+  std::vector<double4> hp(n), hv;
+  std::vector<int4> him(n);
+  std::vector<double4> old(n);
+  CK(cudaMemcpyAsync(old.data(), c->pos, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(him.data(), c->image, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; i++) {
+    double x[3];
+    int im[3] = {him[i].x, him[i].y, him[i].z};
+    for (int a = 0; a < 3; a++) {
+      x[a] = pos[3 * i + a] * c->unit_len;
+      if (!std::isfinite(x[a])) return fail(MDG_ERR_NONFINITE, "non-finite coordinate");
+      if (c->box.pbc[a] && !wrap1(x[a], im[a], c->box.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
+    }
+    hp[i] = make_double4(x[0], x[1], x[2], old[i].w);
+    him[i] = make_int4(im[0], im[1], im[2], 0);
+  }
+  CK(cudaMemcpyAsync(c->pos, hp.data(), n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->image, him.data(), n * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  if (vel) {
+    hv.resize(n);
+    for (int i = 0; i < n; i++)
+      hv[i] = make_double4(vel[3 * i] * c->unit_vel, vel[3 * i + 1] * c->unit_vel, vel[3 * i + 2] * c->unit_vel, 0.0);
+    CK(cudaMemcpyAsync(c->vel, hv.data(), n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->acc_valid = false;
+  return MDG_OK;
+}
+
+int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  int rc = evaluate(c);
+  if (rc) return rc;
+  rc = reduce_energies(c, c->d_energy, 0, 0, false);
+  if (rc) return rc;
+  k_finite<<<nblk(c->n), kThreads, 0, c->stream>>>(c->grad, c->n, c->d_status);
+  c->launches += 1;
+  double he[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(he, c->d_energy, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double4> hg;
+  if (grad) {
+    hg.resize(c->n);
+    CK(cudaMemcpyAsync(hg.data(), c->grad, c->n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  }
+  rc = read_status(c);
+  if (rc) return rc;
+  double E = (he[0] + he[1]) + he[2];
+  if (e_total) *e_total = E * c->unit_e;
+  if (e_terms) {
+    e_terms[0] = he[0] * c->unit_e;
+    e_terms[1] = he[1] * c->unit_e;
+    e_terms[2] = he[2] * c->unit_e;
+    e_terms[3] = 0.0;
+  }
+  if (grad)
+    for (int i = 0; i < c->n; i++) {
+      grad[3 * i] += hg[i].x * c->unit_grad;
+      grad[3 * i + 1] += hg[i].y * c->unit_grad;
+      grad[3 * i + 2] += hg[i].z * c->unit_grad;
+    }
+  return MDG_OK;
+}
+
+int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* count)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (list_id < 0 || list_id > 1 || !c->has_list[list_id]) return fail(MDG_ERR_ARG, "no such list");
+  int rc = rebuild_lists(c);
+  if (rc) return rc;
+  const NList& L = c->nl[list_id];
+  std::vector<int> cnt(c->n), lst((size_t)c->n * L.cap);
+  CK(cudaMemcpyAsync(cnt.data(), L.cnt, c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(lst.data(), L.list, lst.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  std::vector<std::pair<int, int>> out;
+  for (int i = 0; i < c->n; i++)
+    for (int s = 0; s < cnt[i]; s++) {
+      int j = lst[(size_t)i * L.cap + s];
+      if (j > i) out.push_back(std::make_pair(i, j));
+    }
+  std::sort(out.begin(), out.end());
+  if (count) *count = (int64_t)out.size();
+  if (pairs)
+    for (int64_t q = 0; q < (int64_t)out.size() && q < cap; q++) {
+      pairs[2 * q] = out[q].first;
+      pairs[2 * q + 1] = out[q].second;
+    }
+  return MDG_OK;
+}
+
+int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
+  const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
+  State S = c->S();
+  int rc;
+  if (!c->acc_valid) {
+    rc = evaluate(c);
+    if (rc) return rc;
+    k_init_acc<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->grad);
+    c->launches += 1;
+    c->acc_valid = true;
+  }
+  const bool log = epot || etot;
+  if (log && c->elog_cap < nsteps) {
+    if (c->d_elog) cudaFree(c->d_elog);
+    c->d_elog = dalloc<double>((size_t)nsteps * 4);
+    if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
+    c->elog_cap = nsteps;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    k_verlet_pos<<<nblk(c->n), kThreads, 0, c->stream>>>(S, dtf);
+    c->launches += 1;
+    rc = evaluate(c);
+    if (rc) return rc;
+    k_verlet_vel<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->grad, dtf, c->e_kin, c->d_status);
+    c->launches += 1;
+    if (log) {
+      rc = reduce_energies(c, c->d_elog, 4, s, true);
+      if (rc) return rc;
+    }
+  }
+  if (log) {
+    std::vector<double> h((size_t)nsteps * 4);
+    CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    rc = read_status(c);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; s++) {
+      double ep = (h[4 * s] + h[4 * s + 1]) + h[4 * s + 2];
+      if (epot) epot[s] = ep * c->unit_e;
+      if (etot) etot[s] = (ep + h[4 * s + 3]) * c->unit_e;
+    }
+    return MDG_OK;
+  }
+  return launch_check(c);
+}
+
+int mdg_sync(mdg_ctx* c)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  return read_status(c);
+}
+
+int mdg_get_state(mdg_ctx* c, double* pos, double* vel, int32_t* image)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  const int n = c->n;
+  std::vector<double4> hp(n), hv(n);
+  std::vector<int4> him(n);
+  CK(cudaMemcpyAsync(hp.data(), c->pos, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hv.data(), c->vel, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(him.data(), c->image, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  int rc = read_status(c);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) {
+    if (pos) { pos[3*i] = hp[i].x / c->unit_len; pos[3*i+1] = hp[i].y / c->unit_len; pos[3*i+2] = hp[i].z / c->unit_len; }
+    if (vel) { vel[3*i] = hv[i].x / c->unit_vel; vel[3*i+1] = hv[i].y / c->unit_vel; vel[3*i+2] = hv[i].z / c->unit_vel; }
+    if (image) { image[3*i] = him[i].x; image[3*i+1] = him[i].y; image[3*i+2] = him[i].z; }
+  }
+  return MDG_OK;
+}
+
+int64_t mdg_launch_count(mdg_ctx* c) { return c ? c->launches : 0; }
+
+int64_t mdg_debug_rebo_tables(double* out, int64_t cap)
+{
+  ReboTables* h = new ReboTables();
+  std::vector<double> flat;
+  build_rebo_tables(h, &flat);
+  delete h;
+  for (int64_t i = 0; i < (int64_t)flat.size() && i < cap; i++) out[i] = flat[i];
+  return (int64_t)flat.size();
+}
+
+}  // extern "C"

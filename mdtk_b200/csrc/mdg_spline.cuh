@@ -1,0 +1,180 @@
+// Spline evaluation for the REBO correction functions.
+//
+// The reference stores every spline cell as a monomial polynomial in absolute
+// coordinates, solved from corner data at start-up (SplineMultiD,
+// mdtk/SplineAux.hpp:133-241).  Its value is the sequential sum over terms in
+// x0-fastest order of (multiplier*c) * x0^p0 * x1^p1 * x2^p2
+// (SplineTerm::operator(), SplineAux.hpp:82-94; intpow, tools.hpp:107-133).
+// The tables here hold multiplier*c per term; the sum is evaluated in the same
+// order with explicitly rounded multiply/add (no FMA contraction), because the
+// monomial sums cancel heavily (sum |terms| reaches ~3e6 in the pi_rc cells).
+#pragma once
+
+#include "mdg_common.cuh"
+
+namespace mdg {
+
+#if defined(__CUDA_ARCH__)
+MDG_DEV double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+MDG_DEV double add_rn(double a, double b) { return __dadd_rn(a, b); }
+#else
+inline double mul_rn(double a, double b) { return a * b; }
+inline double add_rn(double a, double b) { return a + b; }
+#endif
+
+// intpow for the small non-negative powers the splines use (tools.hpp:107-133),
+// left-to-right products.
+MDG_HD double ipow(double a, int n)
+{
+  double v;
+  switch (n) {
+    case 0: return 1.0;
+    case 1: return a;
+    case 2: return mul_rn(a, a);
+    case 3: v = mul_rn(a, a); return mul_rn(v, a);
+    case 4: v = mul_rn(a, a); v = mul_rn(v, a); return mul_rn(v, a);
+    default: v = mul_rn(a, a); v = mul_rn(v, a); v = mul_rn(v, a); return mul_rn(v, a);
+  }
+}
+
+// Piecewise quintic G(cos theta) (FuncG, AIREBO/cubici.hpp:42-107).
+struct GSpline {
+  int npieces;
+  int pad;
+  double x2[4];
+  double f[4][6];
+  double df[4][6];
+};
+
+// All REBO spline tables, device resident (layout mirrors the host builder).
+struct ReboTables {
+  GSpline G[3];                 // G_C1, G_C2, G_H
+  double P[2][4][4][3][16];     // P_CC / P_CH: cell [h][c], poly f / dH / dC
+  double Pint[2][4][4][3];      // exact-integer shortcut tables (fill_intarg)
+  double T[4][5][5][16][4][64]; // pi_rc CC / CH / HH, Tij: cell [i][j][k], poly f/di/dj/dk
+  double Tint[4][5][5][16][4];  // their exact-integer tables
+};
+
+// 1-D quintic piece: sum_t coef[t] * x^(t - d), d = 0 for the value poly and
+// 1 for the derivative poly (whose term 0 is always zero).
+MDG_HD double poly1(const double* c, double x, int deriv)
+{
+  double val = 0.0;
+  for (int t = 0; t < 6; t++) {
+    double ct = c[t];
+    if (ct == 0.0) continue;
+    val = add_rn(val, mul_rn(ct, ipow(x, t - deriv)));
+  }
+  return val;
+}
+
+// FuncG::operator() / dCosT: first piece whose upper knot is >= CosT.
+MDG_HD double g_eval(const GSpline& g, double cost, int deriv)
+{
+  int p = 0;
+  for (p = 0; p < g.npieces; p++)
+    if (cost <= g.x2[p]) break;
+  if (p >= g.npieces) p = g.npieces - 1;
+  return poly1(deriv ? g.df[p] : g.f[p], cost, deriv);
+}
+
+// Bicubic cell polynomial; d = 0 value, 1 = d/dx0, 2 = d/dx1.
+MDG_HD double poly2(const double* c, double x0, double x1, int d)
+{
+  double val = 0.0;
+  for (int t = 0; t < 16; t++) {
+    double ct = c[t];
+    if (ct == 0.0) continue;
+    int p0 = t & 3, p1 = t >> 2;
+    if (d == 1) p0 -= 1;
+    if (d == 2) p1 -= 1;
+    double v = mul_rn(ct, ipow(x0, p0));
+    v = mul_rn(v, ipow(x1, p1));
+    val = add_rn(val, v);
+  }
+  return val;
+}
+
+// Tricubic cell polynomial; d = 0 value, 1..3 = d/dx0..d/dx2.
+MDG_HD double poly3(const double* c, double x0, double x1, double x2, int d)
+{
+  double val = 0.0;
+  for (int t = 0; t < 64; t++) {
+    double ct = c[t];
+    if (ct == 0.0) continue;
+    int p0 = t & 3, p1 = (t >> 2) & 3, p2 = t >> 4;
+    if (d == 1) p0 -= 1;
+    if (d == 2) p1 -= 1;
+    if (d == 3) p2 -= 1;
+    double v = mul_rn(ct, ipow(x0, p0));
+    v = mul_rn(v, ipow(x1, p1));
+    v = mul_rn(v, ipow(x2, p2));
+    val = add_rn(val, v);
+  }
+  return val;
+}
+
+// P_CC / P_CH (FuncP_*, AIREBO/cubici.hpp:207-298): value and both partials.
+// Zero for h >= 4 or c >= 4; exact-integer arguments read the intarg tables.
+MDG_HD void p_eval(const ReboTables& tb, int fam, double h, double c, double& v, double& dh, double& dc,
+                   unsigned int* status)
+{
+  v = dh = dc = 0.0;
+  if (!(h >= 0 && c >= 0)) { if (status) *status |= ST_SPLINE_DOMAIN; return; }
+  if (h >= 4 || c >= 4) return;
+  int hi = (int)h, ci = (int)c;
+  if ((double)hi == h && (double)ci == c) {
+    v = tb.Pint[fam][hi][ci][0];
+    dh = tb.Pint[fam][hi][ci][1];
+    dc = tb.Pint[fam][hi][ci][2];
+    return;
+  }
+  const double* cell = tb.P[fam][hi][ci][0];
+  v = poly2(cell, h, c, 0);
+  dh = poly2(cell + 16, h, c, 1);
+  dc = poly2(cell + 32, h, c, 2);
+}
+
+MDG_HD double p_value(const ReboTables& tb, int fam, double h, double c)
+{
+  if (!(h >= 0 && c >= 0)) return 0.0;
+  if (h >= 4 || c >= 4) return 0.0;
+  int hi = (int)h, ci = (int)c;
+  if ((double)hi == h && (double)ci == c) return tb.Pint[fam][hi][ci][0];
+  return poly2(tb.P[fam][hi][ci][0], h, c, 0);
+}
+
+// pi_rc CC/CH/HH and Tij (Func_pi_rc, AIREBO/cubici.hpp:301-369): value and
+// the three partials.  Zero for i >= 4 or j >= 4; k is clamped to 15 (cells
+// [.][.][15] are empty, so the function is zero from Nconj = 15 on).
+MDG_HD void t_eval(const ReboTables& tb, int fam, double i, double j, double k, double* out,
+                   unsigned int* status)
+{
+  out[0] = out[1] = out[2] = out[3] = 0.0;
+  if (!(i >= 0 && j >= 0 && k >= 1)) { if (status) *status |= ST_SPLINE_DOMAIN; return; }
+  if (i >= 4 || j >= 4) return;
+  if (k > 15) k = 15;
+  int ii = (int)i, jj = (int)j, kk = (int)k;
+  if ((double)ii == i && (double)jj == j && (double)kk == k) {
+    const double* t = tb.Tint[fam][ii][jj][kk];
+    out[0] = t[0]; out[1] = t[1]; out[2] = t[2]; out[3] = t[3];
+    return;
+  }
+  const double* cell = tb.T[fam][ii][jj][kk][0];
+  out[0] = poly3(cell, i, j, k, 0);
+  out[1] = poly3(cell + 64, i, j, k, 1);
+  out[2] = poly3(cell + 128, i, j, k, 2);
+  out[3] = poly3(cell + 192, i, j, k, 3);
+}
+
+MDG_HD double t_value(const ReboTables& tb, int fam, double i, double j, double k)
+{
+  if (!(i >= 0 && j >= 0 && k >= 1)) return 0.0;
+  if (i >= 4 || j >= 4) return 0.0;
+  if (k > 15) k = 15;
+  int ii = (int)i, jj = (int)j, kk = (int)k;
+  if ((double)ii == i && (double)jj == j && (double)kk == k) return tb.Tint[fam][ii][jj][kk][0];
+  return poly3(tb.T[fam][ii][jj][kk][0], i, j, k, 0);
+}
+
+}  // namespace mdg

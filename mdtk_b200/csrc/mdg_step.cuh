@@ -1,0 +1,368 @@
+// Per-atom work items of one force evaluation and one velocity-Verlet step.
+// Each function is the body of one thread of the matching kernel in
+// mdg_kernels.cu; thread a only ever writes atom a's own outputs.
+#pragma once
+
+#include "mdg_common.cuh"
+#include "mdg_rebo.cuh"
+#include "mdg_etors.cuh"
+
+namespace mdg {
+
+// Verlet neighbour list (full lists, NeighbourList::Update semantics,
+// mdtk/potentials/NeighbourList.cxx:73-106): partners of atom i at
+// list[i * cap + s], s < cnt[i].
+struct NList {
+  int cap;
+  int* cnt;
+  int* list;
+  double range2;      // ((1 + 0.44) * Rcutoff)^2
+  double trigger;     // 0.44 * Rcutoff: rebuild when the two largest displacements exceed it
+  double4* pos0;      // positions at the last build
+};
+
+// Cell grid of one list.
+struct Grid {
+  int nc[3];
+  double lo[3], cs[3];  // origin and cell size per axis
+  int ncell;
+  int brute;            // 1: O(N^2) scan (a periodic axis has fewer than 3 cells)
+  int* ccount;          // [ncell]
+  int* cstart;          // [ncell + 1]
+  int* ccursor;         // [ncell]
+  int* catoms;          // [n]
+};
+
+struct State {
+  int n;
+  Box box;
+  double4* pos;         // x, y, z, w = species index (0 C, 1 H)
+  double4* vel;         // w unused
+  double4* acc;         // an (Angstrom/fs^2)
+  int4* image;          // PBC_count
+  const unsigned char* fixed;
+  double* mass;         // amu
+};
+
+MDG_HD int cell_coord(const Grid& g, const Box& box, int ax, double x)
+{
+  int c = (int)floor((x - g.lo[ax]) / g.cs[ax]);
+  if (box.pbc[ax]) {
+    c %= g.nc[ax];
+    if (c < 0) c += g.nc[ax];
+  } else {
+    if (c < 0) c = 0;
+    if (c >= g.nc[ax]) c = g.nc[ax] - 1;
+  }
+  return c;
+}
+
+MDG_HD int cell_of(const Grid& g, const Box& box, double4 p)
+{
+  int cx = cell_coord(g, box, 0, p.x), cy = cell_coord(g, box, 1, p.y), cz = cell_coord(g, box, 2, p.z);
+  return (cz * g.nc[1] + cy) * g.nc[0] + cx;
+}
+
+// Insertion sort of a short int range (ascending).
+MDG_HD void isort(int* v, int n)
+{
+  for (int a = 1; a < n; a++) {
+    int x = v[a];
+    int b = a - 1;
+    while (b >= 0 && v[b] > x) { v[b + 1] = v[b]; b--; }
+    v[b + 1] = x;
+  }
+}
+
+// Build atom i's list from the cell grid (or by brute force); ascending order.
+MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsigned int* status)
+{
+  const double4 pi = S.pos[i];
+  const V3 xi = v3(pi.x, pi.y, pi.z);
+  int cnt = 0;
+  int* out = L.list + (long)i * L.cap;
+  if (g.brute) {
+    for (int j = 0; j < S.n; j++) {
+      if (j == i) continue;
+      double4 pj = S.pos[j];
+      V3 d = depos(S.box, xi, v3(pj.x, pj.y, pj.z));
+      if (norm2(d) < L.range2) {
+        if (cnt < L.cap) out[cnt] = j;
+        cnt++;
+      }
+    }
+  } else {
+    int c0[3] = {cell_coord(g, S.box, 0, pi.x), cell_coord(g, S.box, 1, pi.y), cell_coord(g, S.box, 2, pi.z)};
+    for (int dz = -1; dz <= 1; dz++) {
+      int cz = c0[2] + dz;
+      if (S.box.pbc[2]) cz = (cz + g.nc[2]) % g.nc[2];
+      else if (cz < 0 || cz >= g.nc[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        int cy = c0[1] + dy;
+        if (S.box.pbc[1]) cy = (cy + g.nc[1]) % g.nc[1];
+        else if (cy < 0 || cy >= g.nc[1]) continue;
+        for (int dx = -1; dx <= 1; dx++) {
+          int cx = c0[0] + dx;
+          if (S.box.pbc[0]) cx = (cx + g.nc[0]) % g.nc[0];
+          else if (cx < 0 || cx >= g.nc[0]) continue;
+          int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+          int b = g.cstart[cell], e = g.cstart[cell + 1];
+          for (int q = b; q < e; q++) {
+            int j = g.catoms[q];
+            if (j == i) continue;
+            double4 pj = S.pos[j];
+            V3 d = depos(S.box, xi, v3(pj.x, pj.y, pj.z));
+            if (norm2(d) < L.range2) {
+              if (cnt < L.cap) out[cnt] = j;
+              cnt++;
+            }
+          }
+        }
+      }
+    }
+    if (cnt <= L.cap) isort(out, cnt);
+  }
+  if (cnt > L.cap) {
+    *status |= ST_NL_OVERFLOW;
+    cnt = L.cap;
+  }
+  L.cnt[i] = cnt;
+  L.pos0[i] = pi;
+}
+
+// Squared displacement since the last build (minimum image).
+MDG_HD double disp_atom(const State& S, const NList& L, int i)
+{
+  double4 p = S.pos[i], q = L.pos0[i];
+  V3 d = depos(S.box, v3(p.x, p.y, p.z), v3(q.x, q.y, q.z));
+  return sqrt(norm2(d));
+}
+
+// Mutable view of the bond list for the builder.
+struct BondBuild {
+  int n, mb;
+  int* nb;
+  int* bj;
+  int* brev;
+  double4* brv;
+  double4* bu;
+  double4* bd;
+  double4* nco;
+};
+
+// Bonds of atom a from its REBO-range Verlet list (ascending, as the
+// reference's NL order), with the REBO cutoffs of each pair
+// (REBO::countNeighbours, REBO.cxx:328-393; AtomsPair, AtomsPair.hpp:137-158).
+MDG_HD void bonds_atom(const State& S, const NList& L, const ReboParams& P, BondBuild& B, int a,
+                       unsigned int* status)
+{
+  const double4 pa = S.pos[a];
+  const int ta = (int)pa.w;
+  const V3 xa = v3(pa.x, pa.y, pa.z);
+  const int cnt = L.cnt[a];
+  const int* lst = L.list + (long)a * L.cap;
+  double Nt = 0.0, NC = 0.0, NH = 0.0;
+  int nb = 0;
+  for (int s = 0; s < cnt; s++) {
+    const int j = lst[s];
+    const double4 pj = S.pos[j];
+    const int tj = (int)pj.w;
+    V3 rv = depos(S.box, xa, v3(pj.x, pj.y, pj.z));
+    double d2 = norm2(rv);
+    const double R1 = P.R[ta][tj][0], R2 = P.R[ta][tj][1];
+    if (d2 > R2 * R2) continue;
+    double r = sqrt(d2);
+    double f, df;
+    cutoff(r, R1, R2, f, df);
+    double Rp1 = P.Rp[ta][tj][0], Rp2 = P.Rp[ta][tj][1];
+    double fp = Sprime(r, Rp1, Rp2), dfp = dSprime(r, Rp1, Rp2);
+    if (!(r > R2)) {
+      Nt += f;
+      if (tj == kH) NH += f;
+      if (tj == kC) NC += f;
+    }
+    if (nb < B.mb) {
+      const int q = a * B.mb + nb;
+      B.bj[q] = j;
+      B.brv[q] = make_double4(rv.x, rv.y, rv.z, r);
+      B.bu[q] = make_double4(rv.x / r, rv.y / r, rv.z / r, f);
+      B.bd[q] = make_double4(df, fp, dfp, 0.0);
+    }
+    nb++;
+  }
+  if (nb > B.mb) {
+    *status |= ST_BOND_OVERFLOW;
+    nb = B.mb;
+  }
+  B.nb[a] = nb;
+  B.nco[a] = make_double4(Nt, NC, NH, (double)ta);
+}
+
+// Slot of atom a in each partner's bond list.
+MDG_HD void brev_atom(BondBuild& B, int a)
+{
+  const int nb = B.nb[a];
+  for (int s = 0; s < nb; s++) {
+    const int j = B.bj[a * B.mb + s];
+    const int nbj = B.nb[j];
+    int r = -1;
+    for (int t = 0; t < nbj; t++)
+      if (B.bj[j * B.mb + t] == a) { r = t; break; }
+    B.brev[a * B.mb + s] = r;
+  }
+}
+
+// Per-atom force-evaluation outputs.
+struct ForceOut {
+  int mb;
+  double* A;        // [n * mb * 3] gradient owed to the partner of each bond slot
+  double* W;        // [n * mb]     third-shell coefficients
+  double4* gown;    // [n] own gradient (REBO + torsion kernel)
+  double4* glj;     // [n] own gradient (LJ kernels)
+  double* e_rebo;   // [n] per-atom energies (lower-index end of each bond)
+  double* e_tors;
+  double* e_lj;
+};
+
+// REBO (+ torsion) for every bond of atom a, evaluated as the reference's
+// bond (min, max) and routed through a Sink for atom a.
+MDG_HD void rebo_atom(const Rebo& R, const TorsParams& TP, int do_rebo, int do_tors, ForceOut& O, int a)
+{
+  const BondList& B = R.B;
+  Sink sink;
+  sink.a = a;
+  sink.g = v3(0, 0, 0);
+  sink.A = O.A + (long)a * O.mb * 3;
+  sink.W = O.W + (long)a * O.mb;
+  for (int s = 0; s < O.mb * 3; s++) sink.A[s] = 0.0;
+  for (int s = 0; s < O.mb; s++) sink.W[s] = 0.0;
+  double er = 0.0, et = 0.0;
+  const int nb = B.nb[a];
+  for (int s = 0; s < nb; s++) {
+    const int q = a * B.mb + s;
+    const int b = B.bj[q];
+    PairG p = pair_from_slot(B, q);
+    int lo = a, hi = b;
+    if (b < a) { lo = b; hi = a; p = pair_reverse(p); }
+    if (do_rebo) {
+      double E = R.bond(lo, hi, p, sink);
+      if (a == lo) er += E;
+    }
+    if (do_tors) {
+      double E = etors_bond(R, TP, lo, hi, p, sink);
+      if (a == lo) et += E;
+    }
+  }
+  O.gown[a] = make_double4(sink.g.x, sink.g.y, sink.g.z, 0.0);
+  O.e_rebo[a] = er;
+  O.e_tors[a] = et;
+}
+
+// Total dE/dx_a: own parts, what bond partners owe a, and the third-shell
+// switching derivatives (dfThem through N_conj) resolved by gathering the
+// coefficients of the bonds around a and around each switching partner.
+MDG_HD V3 gather_atom(const BondList& B, const ForceOut& O, int a, int with_lj, const double4* gextra)
+{
+  double4 g0 = O.gown[a];
+  V3 g = v3(g0.x, g0.y, g0.z);
+  if (with_lj) {
+    double4 g1 = O.glj[a];
+    g += v3(g1.x, g1.y, g1.z);
+  }
+  if (gextra) {
+    double4 g2 = gextra[a];
+    g += v3(g2.x, g2.y, g2.z);
+  }
+  const int nb = B.nb[a];
+  for (int s = 0; s < nb; s++) {
+    const int q = a * B.mb + s;
+    const int k = B.bj[q];
+    const int r = B.brev[q];
+    if (r < 0) continue;  // partner list truncated by an overflow (already flagged)
+    const double* Ak = O.A + ((long)k * O.mb + r) * 3;
+    g += v3(Ak[0], Ak[1], Ak[2]);
+  }
+  for (int s = 0; s < nb; s++) {
+    const int q = a * B.mb + s;
+    const double df = B.bd[q].x;
+    if (df == 0.0) continue;
+    const int m = B.bj[q];
+    double wa = 0.0;
+    for (int t = 0; t < nb; t++) {
+      if (t == s) continue;
+      const int qt = a * B.mb + t;
+      if (B.brev[qt] < 0) continue;
+      wa += O.W[(long)B.bj[qt] * O.mb + B.brev[qt]];
+    }
+    double wm = 0.0;
+    const int nbm = B.nb[m];
+    for (int t = 0; t < nbm; t++) {
+      const int qt = m * B.mb + t;
+      const int c = B.bj[qt];
+      if (c == a || B.brev[qt] < 0) continue;
+      wm += O.W[(long)c * O.mb + B.brev[qt]];
+    }
+    double4 u = B.bu[q];
+    g += v3(u.x, u.y, u.z) * (df * (wa + wm));
+  }
+  return g;
+}
+
+// eq 1 (SimLoop.cxx:323-332): x += v dt + a dt^2 / 2 for free atoms.
+MDG_HD void verlet_pos_atom(State& S, double dt, int i)
+{
+  if (S.fixed && S.fixed[i]) return;
+  double4 p = S.pos[i], v = S.vel[i], ac = S.acc[i];
+  p.x += v.x * dt + ac.x * dt * dt / 2.0;
+  p.y += v.y * dt + ac.y * dt * dt / 2.0;
+  p.z += v.z * dt + ac.z * dt * dt / 2.0;
+  S.pos[i] = p;
+}
+
+// Atom::applyPBC (mdtk/Atom.cxx:94-126): shift into [0, L) and count images.
+// The reference subtracts L one period at a time; a one-period move (the
+// normal case) gives the same value here.  Larger jumps are shifted in one
+// step, and a non-finite coordinate is reported instead of looping forever.
+MDG_HD bool wrap1(double& x, int& im, double L)
+{
+  if (!isfinite(x)) return false;
+  if (x < 0 || x >= L) {
+    double nsh = floor(x / L);
+    if (fabs(nsh) > 1e9) return false;
+    x -= nsh * L;
+    im += (int)nsh;
+    for (int q = 0; q < 2 && x < 0; q++) { x += L; --im; }
+    for (int q = 0; q < 2 && x >= L; q++) { x -= L; ++im; }
+  }
+  return true;
+}
+
+MDG_HD void wrap_atom(State& S, int i, unsigned int* status)
+{
+  double4 p = S.pos[i];
+  int4 im = S.image[i];
+  bool ok = true;
+  if (S.box.pbc[0]) ok &= wrap1(p.x, im.x, S.box.L[0]);
+  if (S.box.pbc[1]) ok &= wrap1(p.y, im.y, S.box.L[1]);
+  if (S.box.pbc[2]) ok &= wrap1(p.z, im.z, S.box.L[2]);
+  if (!ok && status) *status |= ST_NONFINITE;
+  S.pos[i] = p;
+  S.image[i] = im;
+}
+
+// eq 2-4 (SimLoop.cxx:339-399) without the thermal bath: v += a_old dt/2,
+// a = F/M, v += a dt/2; then applyPBC (SimLoop.cxx:401).
+MDG_HD void verlet_vel_atom(State& S, V3 grad, double dt, int i, unsigned int* status)
+{
+  if (!(S.fixed && S.fixed[i])) {
+    double4 v = S.vel[i], ac = S.acc[i];
+    double m = S.mass[i];
+    V3 vdt2 = v3(v.x + ac.x * dt / 2.0, v.y + ac.y * dt / 2.0, v.z + ac.z * dt / 2.0);
+    V3 an = v3(-grad.x / m * kAccConv, -grad.y / m * kAccConv, -grad.z / m * kAccConv);
+    S.acc[i] = make_double4(an.x, an.y, an.z, 0.0);
+    S.vel[i] = make_double4(vdt2.x + an.x * dt / 2.0, vdt2.y + an.y * dt / 2.0, vdt2.z + an.z * dt / 2.0, 0.0);
+  }
+  wrap_atom(S, i, status);
+}
+
+}  // namespace mdg

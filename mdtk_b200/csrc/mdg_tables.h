@@ -1,0 +1,14 @@
+// Host builders of the spline tables (see mdg_tables.cpp).
+#pragma once
+
+#include <vector>
+
+#include "mdg_spline.cuh"
+
+namespace mdg {
+
+// Fills the device-layout REBO tables; when flat_out is given, also returns
+// the tables flattened in the oracle's export order (for the bitwise check).
+void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out);
+
+}  // namespace mdg

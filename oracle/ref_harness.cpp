@@ -415,6 +415,7 @@ extern "C" {
 long ref_tables(int which, int brenner_set, double* out, long cap)
 {
   try {
+    yaatk::verboseTrace = false;
     std::vector<double> v;
     if (which == 0) {
       REBO r;
@@ -472,6 +473,7 @@ int ref_spline_eval(int fn, int n, const double* x, double* out)
 {
   try {
     static REBO* r = 0;
+    yaatk::verboseTrace = false;
     if (!r) r = new REBO();
     for (int q = 0; q < n; q++) {
       const double* a = x + 3 * q;

@@ -1,0 +1,68 @@
+"""CPU checks of the product library: it loads, exports every entry point
+include/mdg.h declares, builds spline tables bitwise equal to the oracle's,
+and refuses to compute without a device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mdtk_b200 as M
+from oracle import ref
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    syms = set()
+    for name in os.listdir(os.path.join(ROOT, "include")):
+        if not name.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", name)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        syms |= set(re.findall(r"\b(mdg_[a-z0-9_]+)\s*\(", text))
+    return sorted(syms)
+
+
+def test_library_loads_and_exports_all_declared_symbols():
+    L = M.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle not built")
+def test_rebo_tables_bitwise_equal_to_oracle():
+    a = M.debug_rebo_tables()
+    b = ref.tables(0)
+    assert a.shape == b.shape
+    assert np.array_equal(a, b)
+
+
+def test_default_params():
+    p = M.Params()
+    M.lib().mdg_default_params(ctypes.byref(p))
+    assert p.potentials == M.POT_REBO and p.precision == M.PREC_FP64 and p.units == M.UNITS_AEVFS
+
+
+def test_create_rejects_lj_without_rebo():
+    with pytest.raises(M.MdgError) as e:
+        M.Context(potentials=M.POT_AIREBO_LJ)
+    assert e.value.code == -1
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="a device is present")
+def test_no_device_fails_loudly():
+    with pytest.raises(M.MdgError) as e:
+        M.Context(potentials=M.POT_REBO)
+    assert e.value.code == -2
