@@ -68,7 +68,8 @@ typedef struct mdg_params {
   int cap_lj_list;
   int cap_bonds;      /* REBO bonds per atom; 0 = default (16) */
   int cap_cij;        /* connectivity targets per atom; 0 = default */
-  int cap_special;    /* LJ pairs per atom needing b* or a connectivity gradient; 0 = default */
+  int cap_records;    /* connectivity middle-bond records per atom (3-bond paths whose middle
+                         bond is in its switching region); 0 = default (64) */
   int device;         /* CUDA device ordinal */
 } mdg_params;
 
@@ -136,8 +137,29 @@ int mdg_get_state(mdg_ctx* ctx, double* pos, double* vel, int32_t* image);
  * host memory; used by drivers that keep the state on the host. */
 int mdg_set_state(mdg_ctx* ctx, const double* pos, const double* vel);
 
+/* Advance nsteps steps from a host-held state (pos, vel [n*3], updated in
+ * place with the final state; epot/etot as in mdg_run): the state is copied to
+ * the device, stepped there, and copied back.  This is SimLoop::execute on
+ * caller-owned AtomsArray data (SimLoop.cxx:141-206) for drivers that keep
+ * the atoms on the host between calls. */
+int mdg_step_host(mdg_ctx* ctx, int nsteps, double dt, double* pos, double* vel, double* epot, double* etot);
+
 /* Number of kernels this context has launched so far. */
 int64_t mdg_launch_count(mdg_ctx* ctx);
+
+/* Per-kernel timing: while on, every launch is bracketed by CUDA events on
+ * the launch stream.  mdg_profile_read waits for the stream and returns, for
+ * up to max kernel names (32-byte NUL-terminated slots in names), the summed
+ * milliseconds and launch counts since profiling was switched on or last
+ * read; *nout gets the number of distinct kernels.  No reference counterpart
+ * (the reference times whole runs with procmon, mdtk/procmon.hpp:99-131). */
+int mdg_set_profiling(mdg_ctx* ctx, int on);
+int mdg_profile_read(mdg_ctx* ctx, int max, char* names, double* ms, int64_t* counts, int* nout);
+
+/* Measured FMA throughput of the FP64 (fp32 = 0) or FP32 (fp32 = 1) CUDA-core
+ * pipe of a device in TFLOP/s (2 flops per FMA): the roofline denominator for
+ * the bond-order kernels.  No reference counterpart. */
+int mdg_pipe_peak(int device, int fp32, double* tflops);
 
 /* Test hook: the REBO spline tables the library built on the host, flattened
  * in the oracle's export order; returns the number of doubles (writes at most

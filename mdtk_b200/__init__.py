@@ -52,7 +52,7 @@ class Params(ctypes.Structure):
         ("cap_lj_list", ctypes.c_int),
         ("cap_bonds", ctypes.c_int),
         ("cap_cij", ctypes.c_int),
-        ("cap_special", ctypes.c_int),
+        ("cap_records", ctypes.c_int),
         ("device", ctypes.c_int),
     ]
 
@@ -84,6 +84,11 @@ def lib():
         L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
         L.mdg_launch_count.argtypes = [vp]
         L.mdg_launch_count.restype = ctypes.c_int64
+        L.mdg_step_host.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, dp, dp]
+        L.mdg_set_profiling.argtypes = [vp, ctypes.c_int]
+        L.mdg_profile_read.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_int)]
+        L.mdg_pipe_peak.argtypes = [ctypes.c_int, ctypes.c_int, dp]
         L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
         L.mdg_debug_rebo_tables.restype = ctypes.c_int64
         _lib = L
@@ -101,6 +106,13 @@ def _ip(a):
 def _check(rc: int):
     if rc != 0:
         raise MdgError(rc, lib().mdg_last_error().decode())
+
+
+def pipe_peak(device: int = 0, fp32: bool = False) -> float:
+    """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 CUDA-core pipe."""
+    out = np.zeros(1)
+    _check(lib().mdg_pipe_peak(device, 1 if fp32 else 0, _dp(out)))
+    return float(out[0])
 
 
 def debug_rebo_tables() -> np.ndarray:
@@ -200,3 +212,27 @@ class Context:
 
     def launch_count(self) -> int:
         return int(lib().mdg_launch_count(self.h))
+
+    def step_host(self, nsteps: int, dt: float, pos: np.ndarray, vel: np.ndarray):
+        """Step from a host-held state (updated in place); returns (epot, etot) per step."""
+        ep = np.zeros(nsteps)
+        et = np.zeros(nsteps)
+        _check(lib().mdg_step_host(self.h, nsteps, dt, _dp(pos), _dp(vel), _dp(ep), _dp(et)))
+        return ep, et
+
+    def set_profiling(self, on: bool):
+        _check(lib().mdg_set_profiling(self.h, 1 if on else 0))
+
+    def profile_read(self, max_kernels: int = 64):
+        """{kernel name: (total ms, launches)} since profiling was switched on / last read."""
+        names = ctypes.create_string_buffer(32 * max_kernels)
+        ms = np.zeros(max_kernels)
+        cnt = np.zeros(max_kernels, dtype=np.int64)
+        nout = ctypes.c_int()
+        _check(lib().mdg_profile_read(self.h, max_kernels, names, _dp(ms),
+                                      cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(nout)))
+        out = {}
+        for k in range(min(nout.value, max_kernels)):
+            nm = names.raw[32 * k: 32 * k + 32].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(cnt[k]))
+        return out

@@ -125,24 +125,34 @@ def ethane_liquid(n_mol: int, density_g_cm3: float = 0.55, temp_k: float = 300.0
     (reference masses: 30 amu per molecule).
 
     Random sequential insertion jams well below liquid density, so each
-    molecule takes a randomly chosen site of an FCC lattice filling the box,
+    molecule takes a randomly chosen site of a lattice filling the box,
     a seeded random displacement of up to `jitter` A per axis and a uniformly
     random orientation; orientations are redrawn until every intermolecular
-    atom pair is at least min_dist apart."""
+    atom pair is at least min_dist apart.  The lattice is FCC or simple cubic,
+    whichever spaces the sites further apart for this molecule count."""
     mass_g = n_mol * 30.0 * AMU_G
     L = (mass_g / density_g_cm3) ** (1.0 / 3.0) * 1e8
     rng = np.random.default_rng(seed)
+    # the lattice (FCC or simple cubic) whose nearest-neighbour spacing is larger
     m = 1
     while 4 * m ** 3 < n_mol:
         m += 1
-    a = L / m
-    fcc = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
-    cells = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
-    sites = ((cells[:, None, :] + fcc[None]).reshape(-1, 3) + 0.25) * a
+    k = 1
+    while k ** 3 < n_mol:
+        k += 1
+    if L / (m * math.sqrt(2.0)) >= L / k:
+        basis = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
+        ncell = m
+    else:
+        basis = np.zeros((1, 3))
+        ncell = k
+    a = L / ncell
+    cells = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell), indexing="ij"), -1).reshape(-1, 3)
+    sites = ((cells[:, None, :] + basis[None]).reshape(-1, 3) + 0.25) * a
     sites = sites[rng.permutation(len(sites))[:n_mol]]
     tmpl = _ethane_template()
-    ncell = max(1, int(L // min_dist))
-    csz = L / ncell
+    ng = max(1, int(L // min_dist))
+    csz = L / ng
     grid: Dict[tuple, list] = {}
     placed = []
     for center0 in sites:
@@ -150,14 +160,14 @@ def ethane_liquid(n_mol: int, density_g_cm3: float = 0.55, temp_k: float = 300.0
             R = _random_rotations(rng, 1)[0]
             center = center0 + rng.uniform(-jitter, jitter, size=3)
             at = np.mod((tmpl @ R.T) + center, L)
-            keys = [tuple((p // csz).astype(int) % ncell) for p in at]
+            keys = [tuple((p // csz).astype(int) % ng) for p in at]
             ok = True
             for p, ci in zip(at, keys):
                 near = []
                 for dx in (-1, 0, 1):
                     for dy in (-1, 0, 1):
                         for dz in (-1, 0, 1):
-                            lst = grid.get(((ci[0] + dx) % ncell, (ci[1] + dy) % ncell, (ci[2] + dz) % ncell))
+                            lst = grid.get(((ci[0] + dx) % ng, (ci[1] + dy) % ng, (ci[2] + dz) % ng))
                             if lst:
                                 near.extend(lst)
                 if near:

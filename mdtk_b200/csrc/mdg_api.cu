@@ -173,11 +173,35 @@ __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, Tor
   rebo_atom(R, TP, do_rebo, do_tors, O, a);
 }
 
-__global__ void k_gather(BondList B, ForceOut O, int with_lj, const double4* gextra, double4* grad)
+constexpr int kCijLocal = 128;  // per-thread connectivity table capacity
+
+__global__ void k_cij(BondList B, CijTable T, unsigned int* status)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
+}
+
+__global__ void k_lj(const ReboParams* P, const ReboTables* Tb, LJParams LP, BondList B, CijTable T, State S, NList L,
+                     ForceOut O, MidRecords M, unsigned int* status)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
-  V3 g = gather_atom(B, O, a, with_lj, gextra);
+  Rebo R{*P, *Tb, B, status};
+  LJ X{LP, R, T};
+  Sink sink;
+  sink.a = a;
+  sink.g = v3(0, 0, 0);
+  sink.A = O.A + (long)a * O.mb * 3;
+  sink.W = O.W + (long)a * O.mb;
+  lj_atom(X, S, L, sink, O.glj, O.e_lj, &M, status);
+}
+
+__global__ void k_gather(BondList B, ForceOut O, int with_lj, MidRecords M, double4* grad)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.n) return;
+  V3 g = gather_atom(B, O, a, with_lj, nullptr);
+  if (with_lj) g += mid_gather_atom(B, M, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
 }
 
@@ -256,6 +280,32 @@ __global__ void k_finite(const double4* g, int n, unsigned int* status)
   if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) atomicOr(status, ST_NONFINITE);
 }
 
+// FMA-throughput probes for the roofline denominators (no peak for the FP64
+// and FP32 CUDA-core pipes is recorded elsewhere): each thread runs 8
+// independent dependent-FMA chains, so the pipes stay full.
+__global__ void k_peak_fp64(double* out, int iters, double a, double b)
+{
+  double x[8];
+  for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-9 + q;
+  for (int it = 0; it < iters; it++)
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = fma(x[q], a, b);
+  double s = 0;
+  for (int q = 0; q < 8; q++) s += x[q];
+  if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+__global__ void k_peak_fp32(float* out, int iters, float a, float b)
+{
+  float x[8];
+  for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-6f + q;
+  for (int it = 0; it < iters; it++)
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = fmaf(x[q], a, b);
+  float s = 0;
+  for (int q = 0; q < 8; q++) s += x[q];
+  if (s == 12345.678f) out[0] = s;
+}
+
 template <class T>
 T* dalloc(size_t count)
 {
@@ -310,9 +360,19 @@ struct mdg_ctx {
   double* d_elog = nullptr;     // per-step energy log [cap * 4]
   int elog_cap = 0;
 
-  LJState lj;
+  CijTable cij;
+  MidRecords mid;
 
   unsigned int* d_status = nullptr;
+
+  // profiling: event pairs bracketing each launch while enabled
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<std::string, size_t>> prof_recs;  // name, index of the start event
+  // host staging for mdg_step_host
+  double4* h_stage = nullptr;
+  std::vector<int> h_type;
 
   State S() const
   {
@@ -344,6 +404,30 @@ struct mdg_ctx {
 };
 
 namespace {
+
+cudaEvent_t pool_event(mdg_ctx* c)
+{
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+
+void prof_begin(mdg_ctx* c, const char* name)
+{
+  if (!c->prof) return;
+  size_t i = c->ev_used;
+  cudaEventRecord(pool_event(c), c->stream);
+  c->prof_recs.push_back(std::make_pair(std::string(name), i));
+}
+
+void prof_end(mdg_ctx* c)
+{
+  if (!c->prof) return;
+  cudaEventRecord(pool_event(c), c->stream);
+}
 
 void set_rebo_params(ReboParams& p)
 {
@@ -398,8 +482,7 @@ int status_to_code(unsigned int st, std::string& msg)
   add(ST_N_NEGATIVE, MDG_ERR_N_NEGATIVE, "negative coordination;");
   add(ST_SPLINE_DOMAIN, MDG_ERR_SPLINE_DOMAIN, "spline argument out of domain;");
   add(ST_CIJ_OVERFLOW, MDG_ERR_CAPACITY, "connectivity table capacity exceeded;");
-  add(ST_SPECIAL_OVERFLOW, MDG_ERR_CAPACITY, "LJ special-pair capacity exceeded;");
-  add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "connectivity record capacity exceeded;");
+    add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "connectivity record capacity exceeded;");
   add(ST_CELL_OVERFLOW, MDG_ERR_CAPACITY, "cell grid capacity exceeded;");
   return code;
 }
@@ -421,7 +504,13 @@ void free_system(mdg_ctx* c)
     std::memset(&c->grid[l], 0, sizeof(Grid));
     c->has_list[l] = false;
   }
-  lj_free(c->lj);
+  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->mid.cnt, c->mid.ent, c->mid.c};
+  for (void* p : lq)
+    if (p) cudaFree(p);
+  std::memset(&c->cij, 0, sizeof(c->cij));
+  std::memset(&c->mid, 0, sizeof(c->mid));
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  c->h_stage = nullptr;
   c->pos = c->vel = c->acc = c->grad = nullptr;
   c->image = nullptr;
   c->fixed = nullptr;
@@ -474,6 +563,18 @@ int setup_grid(mdg_ctx* c, int l, const std::vector<double>& hpos)
   return MDG_OK;
 }
 
+// Every launch goes through LAUNCH: it counts the launch and, when
+// profiling is on, brackets it with CUDA events on the launch stream.
+void prof_begin(mdg_ctx* c, const char* name);
+void prof_end(mdg_ctx* c);
+#define LAUNCH(c, NAME, KERNEL, GRID, BLOCK, ...)                     \
+  do {                                                                \
+    prof_begin(c, NAME);                                              \
+    KERNEL<<<(GRID), (BLOCK), 0, (c)->stream>>>(__VA_ARGS__);         \
+    prof_end(c);                                                      \
+    (c)->launches++;                                                  \
+  } while (0)
+
 int rebuild_lists(mdg_ctx* c)
 {
   State S = c->S();
@@ -483,19 +584,16 @@ int rebuild_lists(mdg_ctx* c)
     NList& L = c->nl[l];
     Grid& g = c->grid[l];
     int* need = c->d_need + l;
-    k_disp_partial<<<nparts, kThreads, 0, c->stream>>>(S, L, c->d_part);
-    k_disp_final<<<1, 32, 0, c->stream>>>(c->d_part, nparts, L.trigger, need, c->d_force + l);
-    c->launches += 2;
+    LAUNCH(c, "nl_disp_partial", k_disp_partial, nparts, kThreads, S, L, c->d_part);
+    LAUNCH(c, "nl_disp_final", k_disp_final, 1, 32, c->d_part, nparts, L.trigger, need, c->d_force + l);
     if (!g.brute) {
-      k_cell_clear<<<nblk(g.ncell), kThreads, 0, c->stream>>>(g, need);
-      k_cell_count<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, need);
-      k_cell_scan<<<1, 1024, 0, c->stream>>>(g, need);
-      k_cell_fill<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, need);
-      k_cell_sort<<<nblk(g.ncell), kThreads, 0, c->stream>>>(g, need);
-      c->launches += 5;
+      LAUNCH(c, "nl_cell_clear", k_cell_clear, nblk(g.ncell), kThreads, g, need);
+      LAUNCH(c, "nl_cell_count", k_cell_count, nblk(c->n), kThreads, S, g, need);
+      LAUNCH(c, "nl_cell_scan", k_cell_scan, 1, 1024, g, need);
+      LAUNCH(c, "nl_cell_fill", k_cell_fill, nblk(c->n), kThreads, S, g, need);
+      LAUNCH(c, "nl_cell_sort", k_cell_sort, nblk(g.ncell), kThreads, g, need);
     }
-    k_nl_build<<<nblk(c->n), kThreads, 0, c->stream>>>(S, g, L, need, c->d_status);
-    c->launches += 1;
+    LAUNCH(c, l == 0 ? "nl_build_rebo" : "nl_build_lj", k_nl_build, nblk(c->n), kThreads, S, g, L, need, c->d_status);
   }
   return launch_check(c);
 }
@@ -510,21 +608,17 @@ int evaluate(mdg_ctx* c)
   State S = c->S();
   const int pot = c->prm.potentials;
   const bool rebo = pot & MDG_POT_REBO, tors = pot & MDG_POT_ETORS, lj = pot & MDG_POT_AIREBO_LJ;
-  k_bonds<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->nl[0], c->rp, c->bb, c->d_status);
-  k_brev<<<nblk(c->n), kThreads, 0, c->stream>>>(c->bb);
-  c->launches += 2;
+  LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->d_status);
+  LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb);
   BondList B = c->BL();
-  k_rebo<<<nblk(c->n), kThreads, 0, c->stream>>>(c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0, tors ? 1 : 0, c->fo,
-                                                 c->d_status);
-  c->launches += 1;
-  const double4* gextra = nullptr;
+  LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0, tors ? 1 : 0,
+         c->fo, c->d_status);
   if (lj) {
-    rc = lj_evaluate(c->lj, S, c->nl[1], B, c->d_rp, c->d_tables, c->ljp, c->fo, c->stream, c->d_status,
-                     &c->launches, &gextra);
-    if (rc) return fail(MDG_ERR_CUDA, "LJ evaluation launch failed");
+    LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
+    LAUNCH(c, "lj_pairs", k_lj, nblk(c->n), kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S, c->nl[1], c->fo,
+           c->mid, c->d_status);
   }
-  k_gather<<<nblk(c->n), kThreads, 0, c->stream>>>(B, c->fo, lj ? 1 : 0, gextra, c->grad);
-  c->launches += 1;
+  LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->mid, c->grad);
   return launch_check(c);
 }
 
@@ -537,10 +631,9 @@ int reduce_energies(mdg_ctx* c, double* out_dev, int slot_stride, int slot, bool
   R.a[3] = c->e_kin;
   R.narr = with_kin ? 4 : 3;
   R.n = c->n;
-  k_reduce_partial<<<dim3(kRedBlocks, R.narr), kThreads, 0, c->stream>>>(R, c->d_red_part);
-  k_reduce_final<<<1, 32, 0, c->stream>>>(c->d_red_part, kRedBlocks, R.narr, out_dev, slot_stride, slot,
-                                          c->d_status);
-  c->launches += 2;
+  LAUNCH(c, "energy_partial", k_reduce_partial, dim3(kRedBlocks, R.narr), kThreads, R, c->d_red_part);
+  LAUNCH(c, "energy_final", k_reduce_final, 1, 32, c->d_red_part, kRedBlocks, R.narr, out_dev, slot_stride, slot,
+         c->d_status);
   return launch_check(c);
 }
 
@@ -594,7 +687,7 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   if (c->prm.cap_rebo_list <= 0) c->prm.cap_rebo_list = 64;
   if (c->prm.cap_lj_list <= 0) c->prm.cap_lj_list = 512;
   if (c->prm.cap_cij <= 0) c->prm.cap_cij = 128;
-  if (c->prm.cap_special <= 0) c->prm.cap_special = 64;
+  if (c->prm.cap_records <= 0) c->prm.cap_records = 64;
   c->mb = c->prm.cap_bonds;
   set_rebo_params(c->rp);
   set_tors_params(c->tp);
@@ -639,6 +732,7 @@ int mdg_destroy(mdg_ctx* c)
   void* ptrs[] = {c->d_tables, c->d_rp, c->d_status, c->d_need, c->d_force, c->d_energy};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return MDG_OK;
@@ -667,6 +761,7 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
   std::vector<int4> him(n);
   std::vector<double> hm(n), hpos(3 * (size_t)n);
   std::vector<unsigned char> hf(n, 0);
+  c->h_type.assign(n, 0);
   for (int i = 0; i < n; i++) {
     int t;
     if (z[i] == 6) t = kC;
@@ -681,6 +776,7 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
       hpos[3 * i + a] = x[a];
     }
     hp[i] = make_double4(x[0], x[1], x[2], (double)t);
+    c->h_type[i] = t;
     hf[i] = (fixed && fixed[i]) ? 1 : 0;
     if (vel && !hf[i])
       hv[i] = make_double4(vel[3 * i] * c->unit_vel, vel[3 * i + 1] * c->unit_vel, vel[3 * i + 2] * c->unit_vel, 0.0);
@@ -765,9 +861,21 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
   CK(cudaMemset(c->fo.glj, 0, n * sizeof(double4)));
   CK(cudaMemset(c->fo.e_lj, 0, n * sizeof(double)));
   if (with_lj) {
-    int rc = lj_alloc(c->lj, n, c->prm.cap_cij, c->prm.cap_special, mb);
-    if (rc) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
+    if (c->prm.cap_cij > kCijLocal) c->prm.cap_cij = kCijLocal;
+    c->cij.cap = c->prm.cap_cij;
+    c->cij.cnt = dalloc<int>(n);
+    c->cij.ent = dalloc<int4>((size_t)n * c->cij.cap);
+    c->cij.w = dalloc<double>((size_t)n * c->cij.cap);
+    c->mid.cap = c->prm.cap_records;
+    c->mid.cnt = dalloc<int>(n);
+    c->mid.ent = dalloc<int4>((size_t)n * c->mid.cap);
+    c->mid.c = dalloc<double>((size_t)n * c->mid.cap);
+    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->mid.cnt || !c->mid.ent || !c->mid.c)
+      return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
+    CK(cudaMemset(c->mid.cnt, 0, n * sizeof(int)));
   }
+  if (cudaHostAlloc((void**)&c->h_stage, 2 * (size_t)n * sizeof(double4), cudaHostAllocDefault) != cudaSuccess)
+    return fail(MDG_ERR_CUDA, "cudaHostAlloc (staging)");
   CK(cudaDeviceSynchronize());
   return MDG_OK;
 }
@@ -818,8 +926,7 @@ int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
   if (rc) return rc;
   rc = reduce_energies(c, c->d_energy, 0, 0, false);
   if (rc) return rc;
-  k_finite<<<nblk(c->n), kThreads, 0, c->stream>>>(c->grad, c->n, c->d_status);
-  c->launches += 1;
+  LAUNCH(c, "finite_check", k_finite, nblk(c->n), kThreads, c->grad, c->n, c->d_status);
   double he[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(he, c->d_energy, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   std::vector<double4> hg;
@@ -884,8 +991,7 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
   if (!c->acc_valid) {
     rc = evaluate(c);
     if (rc) return rc;
-    k_init_acc<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->grad);
-    c->launches += 1;
+    LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
     c->acc_valid = true;
   }
   const bool log = epot || etot;
@@ -896,12 +1002,10 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->elog_cap = nsteps;
   }
   for (int s = 0; s < nsteps; s++) {
-    k_verlet_pos<<<nblk(c->n), kThreads, 0, c->stream>>>(S, dtf);
-    c->launches += 1;
+    LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
     rc = evaluate(c);
     if (rc) return rc;
-    k_verlet_vel<<<nblk(c->n), kThreads, 0, c->stream>>>(S, c->grad, dtf, c->e_kin, c->d_status);
-    c->launches += 1;
+    LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
     if (log) {
       rc = reduce_energies(c, c->d_elog, 4, s, true);
       if (rc) return rc;
@@ -948,6 +1052,105 @@ int mdg_get_state(mdg_ctx* c, double* pos, double* vel, int32_t* image)
 }
 
 int64_t mdg_launch_count(mdg_ctx* c) { return c ? c->launches : 0; }
+
+int mdg_set_profiling(mdg_ctx* c, int on)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  c->prof = on != 0;
+  c->prof_recs.clear();
+  c->ev_used = 0;
+  return MDG_OK;
+}
+
+int mdg_profile_read(mdg_ctx* c, int max, char* names, double* ms, int64_t* counts, int* nout)
+{
+  if (!c || !nout) return fail(MDG_ERR_ARG, "null argument");
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<std::string> keys;
+  std::vector<double> tot;
+  std::vector<int64_t> cnt;
+  for (auto& r : c->prof_recs) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->ev_pool[r.second], c->ev_pool[r.second + 1]));
+    size_t k = 0;
+    while (k < keys.size() && keys[k] != r.first) k++;
+    if (k == keys.size()) { keys.push_back(r.first); tot.push_back(0.0); cnt.push_back(0); }
+    tot[k] += t;
+    cnt[k] += 1;
+  }
+  int n = (int)keys.size();
+  *nout = n;
+  for (int k = 0; k < n && k < max; k++) {
+    if (names) {
+      std::strncpy(names + 32 * k, keys[k].c_str(), 31);
+      names[32 * k + 31] = 0;
+    }
+    if (ms) ms[k] = tot[k];
+    if (counts) counts[k] = cnt[k];
+  }
+  c->prof_recs.clear();
+  c->ev_used = 0;
+  return MDG_OK;
+}
+
+int mdg_step_host(mdg_ctx* c, int nsteps, double dt, double* pos, double* vel, double* epot, double* etot)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (!pos || !vel) return fail(MDG_ERR_ARG, "null state buffer");
+  const int n = c->n;
+  double4* hp = c->h_stage;
+  double4* hv = c->h_stage + n;
+  for (int i = 0; i < n; i++) {
+    hp[i] = make_double4(pos[3 * i] * c->unit_len, pos[3 * i + 1] * c->unit_len, pos[3 * i + 2] * c->unit_len,
+                         (double)c->h_type[i]);
+    hv[i] = make_double4(vel[3 * i] * c->unit_vel, vel[3 * i + 1] * c->unit_vel, vel[3 * i + 2] * c->unit_vel, 0.0);
+  }
+  CK(cudaMemcpyAsync(c->pos, hp, n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->vel, hv, n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  int rc = mdg_run(c, nsteps, dt, epot, etot);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(hp, c->pos, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hv, c->vel, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) {
+    pos[3 * i] = hp[i].x / c->unit_len; pos[3 * i + 1] = hp[i].y / c->unit_len; pos[3 * i + 2] = hp[i].z / c->unit_len;
+    vel[3 * i] = hv[i].x / c->unit_vel; vel[3 * i + 1] = hv[i].y / c->unit_vel; vel[3 * i + 2] = hv[i].z / c->unit_vel;
+  }
+  return MDG_OK;
+}
+
+int mdg_pipe_peak(int device, int fp32, double* tflops)
+{
+  if (!tflops) return fail(MDG_ERR_ARG, "null argument");
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int threads = 256, blocks = sms * 8, iters = 1 << 14;
+  void* buf = nullptr;
+  CK(cudaMalloc(&buf, 64));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best = 0.0;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0);
+    if (fp32) k_peak_fp32<<<blocks, threads>>>((float*)buf, iters, 0.999999f, 1e-7f);
+    else k_peak_fp64<<<blocks, threads>>>((double*)buf, iters, 0.999999999, 1e-12);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+    if (rep > 0) best = std::fmax(best, flops / (t * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  CK(cudaGetLastError());
+  *tflops = best;
+  return MDG_OK;
+}
 
 int64_t mdg_debug_rebo_tables(double* out, int64_t cap)
 {

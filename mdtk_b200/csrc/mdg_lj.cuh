@@ -1,5 +1,7 @@
 // AIREBO intermolecular LJ term (mdtk/potentials/manybody/AIREBO/AIREBO_LJ.cxx):
-// parameters and per-pair device code.
+// parameters, the bond-path connectivity table C_ij, and the per-pair term
+// E_ij = C_ij * [1 - S(t_r) + S(t_r) S(t_b(b*_ij))] * f^LJ * 4 eps [(s/r)^12 - (s/r)^6]
+// with its first-order adjoint.
 #pragma once
 
 #include "mdg_rebo.cuh"
@@ -41,19 +43,345 @@ inline void set_lj_params(LJParams& p, int lj_cut_mode)
   p.b[C][H][1] = p.b[H][C][1] = 0.90;
 }
 
-}  // namespace mdg
-
-#if defined(__CUDACC__)
-namespace mdg {
-struct LJState {
-  int n = 0;
+// Connectivity table of atom i: every atom reachable over at most three REBO
+// bonds with the largest product of bond cutoffs w and the path that gives
+// it (AIREBO::fill_Cij, AIREBO_LJ.cxx:289-367), sorted by target.
+struct CijTable {
+  int cap;
+  int* cnt;        // [n]
+  int4* ent;       // [n * cap] x = target, y = path length, z = k, w = m
+  double* w;       // [n * cap]
 };
-inline void lj_free(LJState& s) { s.n = 0; }
-inline int lj_alloc(LJState& s, int n, int, int, int) { s.n = n; return 0; }
-inline int lj_evaluate(LJState&, const State&, const NList&, const BondList&, const ReboParams*, const ReboTables*,
-                       const LJParams&, const ForceOut&, cudaStream_t, unsigned int*, int64_t*, const double4**)
+
+// Middle-bond records of 3-bond connectivity paths (the bond k-m of
+// i-k-m-j belongs to neither end of the LJ pair): written by the lower-index
+// end, gathered by k and m.
+struct MidRecords {
+  int cap;
+  int* cnt;        // [n]
+  int4* ent;       // [n * cap] x = k, y = slot of m in k's bond list, z = m
+  double* c;       // [n * cap] dE/dr of the bond k-m
+};
+
+MDG_HD int bond_slot(const BondList& B, int c, int k)
 {
+  const int nb = B.nb[c];
+  for (int s = 0; s < nb; s++)
+    if (B.bj[c * B.mb + s] == k) return s;
   return -1;
 }
+
+// Builds atom i's table with the reference's enumeration order and tie rules:
+// a 1-bond path replaces an equal-weight longer one, a 2-bond path an equal
+// 3-bond one, a 3-bond path only a strictly smaller weight.
+template <int CAPL>
+MDG_HD void cij_build_atom(const BondList& B, CijTable& T, int i, unsigned int* status)
+{
+  int tgt[CAPL];
+  int len[CAPL], pk[CAPL], pm[CAPL];
+  double w[CAPL];
+  int n = 0;
+  bool over = false;
+  const int cap = T.cap < CAPL ? T.cap : CAPL;
+  auto upd = [&](int t, double nw, int L, int k, int m) {
+    int idx = -1;
+    for (int e = 0; e < n; e++)
+      if (tgt[e] == t) { idx = e; break; }
+    double cw = idx >= 0 ? w[idx] : 0.0;
+    int cl = idx >= 0 ? len[idx] : 0;
+    bool rep;
+    if (L == 1) rep = nw > cw || (cw > 0.0 && nw == cw && cl > 1);
+    else if (L == 2) rep = nw > cw || (cw > 0.0 && nw == cw && cl > 2);
+    else rep = nw > cw;
+    if (!rep) return;
+    if (idx < 0) {
+      if (n >= cap) { over = true; return; }
+      idx = n++;
+      tgt[idx] = t;
+    }
+    w[idx] = nw;
+    len[idx] = L;
+    pk[idx] = k;
+    pm[idx] = m;
+  };
+  const int nb1 = B.nb[i];
+  for (int s1 = 0; s1 < nb1; s1++) {
+    const int q1 = i * B.mb + s1;
+    const int k = B.bj[q1];
+    const double f1 = B.bu[q1].w;
+    upd(k, f1, 1, -1, -1);
+    const int nb2 = B.nb[k];
+    for (int s2 = 0; s2 < nb2; s2++) {
+      const int q2 = k * B.mb + s2;
+      const int m = B.bj[q2];
+      const double f2 = B.bu[q2].w;
+      upd(m, f1 * f2, 2, k, -1);
+      const int nb3 = B.nb[m];
+      for (int s3 = 0; s3 < nb3; s3++) {
+        const int q3 = m * B.mb + s3;
+        const int t = B.bj[q3];
+        const double f3 = B.bu[q3].w;
+        upd(t, f1 * f2 * f3, 3, k, m);
+      }
+    }
+  }
+  if (over) *status |= ST_CIJ_OVERFLOW;
+  // insertion sort by target, then store
+  for (int a = 1; a < n; a++) {
+    int t = tgt[a], l = len[a], k = pk[a], m = pm[a];
+    double ww = w[a];
+    int b = a - 1;
+    while (b >= 0 && tgt[b] > t) {
+      tgt[b + 1] = tgt[b]; len[b + 1] = len[b]; pk[b + 1] = pk[b]; pm[b + 1] = pm[b]; w[b + 1] = w[b];
+      b--;
+    }
+    tgt[b + 1] = t; len[b + 1] = l; pk[b + 1] = k; pm[b + 1] = m; w[b + 1] = ww;
+  }
+  for (int e = 0; e < n; e++) {
+    T.ent[(long)i * T.cap + e] = make_int4(tgt[e], len[e], pk[e], pm[e]);
+    T.w[(long)i * T.cap + e] = w[e];
+  }
+  T.cnt[i] = n;
+}
+
+// Lookup of target j in the table of i (binary search).  Returns the entry
+// index or -1.
+MDG_HD int cij_find(const CijTable& T, int i, int j)
+{
+  int lo = 0, hi = T.cnt[i] - 1;
+  const int4* e = T.ent + (long)i * T.cap;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    int t = e[mid].x;
+    if (t == j) return mid;
+    if (t < j) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// S(t) switch (AIREBO::S / dS, AIREBO_LJ.cxx:116-156).
+MDG_HD double Slj(double arg, double amin, double amax)
+{
+  if (arg < amin) return 1.0;
+  if (arg > amax) return 0.0;
+  double t = (arg - amin) / (amax - amin);
+  return 1.0 - t * t * (3.0 - 2.0 * t);
+}
+MDG_HD double dSlj(double arg, double amin, double amax)
+{
+  if (arg < amin) return 0.0;
+  if (arg > amax) return 0.0;
+  double t = (arg - amin) / (amax - amin);
+  return (-2.0 * t * (3.0 - 2.0 * t) + 2.0 * t * t) / (amax - amin);
+}
+
+struct LJ {
+  const LJParams& P;
+  const Rebo& R;
+  const CijTable& T;
+
+  // b*_ij: REBO's b_ij average for the pair with r_alter = R1 of REBO
+  // (AIREBO::BijAsterix, AIREBO_LJ.cxx:191-202).
+  template <class S>
+  MDG_HD double bstar(int i, int j, const PairG& pl, double V, S& sink) const
+  {
+    PairG p = pl;
+    const int ti = R.type(i), tj = R.type(j);
+    cutoff(p.r, R.P.R[ti][tj][0], R.P.R[ti][tj][1], p.f, p.df);
+    p.alter = 1;
+    p.ralt = R.P.R[ti][tj][0];
+    return R.baver(i, j, p, V, sink);
+  }
+
+  // One LJ pair i < j (the body of AIREBO::operator(), AIREBO_LJ.cxx:52-70).
+  // pl: the pair i -> j with the LJ cosine cutoff in f/df.  Returns its
+  // energy; the middle bond of a 3-bond path is recorded through `mid` when
+  // non-null (the i end passes it).
+  template <class S>
+  MDG_HD double pair(int i, int j, const PairG& pl, S& sink, MidRecords* mid, unsigned int* status) const
+  {
+    // connectivity (AIREBO::Cij, AIREBO_LJ.cxx:381-408)
+    int e = cij_find(T, i, j);
+    double w = 0.0;
+    int4 path = make_int4(j, 0, -1, -1);
+    if (e >= 0) {
+      w = T.w[(long)i * T.cap + e];
+      path = T.ent[(long)i * T.cap + e];
+    }
+    const double C = 1 - w;
+    if (!(C > 0.0)) return 0.0;
+    const int ti = R.type(i), tj = R.type(j);
+    const double r = pl.r;
+    // StrStb value (AIREBO_LJ.cxx:79-114)
+    const double rmin = P.RLJ[ti][tj][0], rmax = P.RLJ[ti][tj][1];
+    const double Str = Slj(r, rmin, rmax);
+    double Stb = 0.0, bij = 0.0, SrSb = 1.0;
+    Sink dummy;
+    if (Str != 0.0) {
+      bij = bstar(i, j, pl, 0.0, dummy);
+      Stb = Slj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
+      SrSb += Str * Stb - Str;
+    }
+    // VLJ (AIREBO_LJ.cxx:158-189) with seed SrSb*C
+    const double fv = pl.f;
+    if (fv == 0.0) return 0.0;
+    const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
+    const double sdr = sigma / r;
+    double s6 = sdr;
+    for (int q = 2; q <= 6; q++) s6 *= sdr;
+    const double s12 = s6 * s6;
+    const double val = 4.0 * zeta * (s12 - s6);
+    const double V1 = SrSb * C;
+    if (V1 != 0.0) {
+      double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
+      sink.pair(i, j, pl.u * (der * fv * V1));
+      if (pl.df != 0.0) sink.pair(i, j, pl.u * ((val * V1) * pl.df));
+    }
+    const double LJv = fv * val;
+    // StrStb gradient with seed C*LJ
+    const double V2 = C * LJv;
+    if (Str != 0.0 && V2 != 0.0) {
+      double dStr = dSlj(r, rmin, rmax);
+      if (dStr != 0.0) sink.pair(i, j, pl.u * (-dStr * V2));
+      double dStb = dSlj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
+      if (dStr != 0.0 && Stb != 0.0) sink.pair(i, j, pl.u * (dStr * Stb * V2));
+      if (dStb != 0.0) bstar(i, j, pl, Str * dStb * V2, sink);
+    }
+    // Cij gradient with seed SrSb*LJ: -V * (product of the other cutoffs) * df
+    const double V3 = SrSb * LJv;
+    if (e >= 0 && V3 != 0.0 && path.y > 0) {
+      const BondList& B = R.B;
+      if (path.y == 1) {
+        int s = bond_slot(B, i, j);
+        if (s >= 0) {
+          const int q = i * B.mb + s;
+          double df = B.bd[q].x;
+          if (df != 0.0) {
+            double4 u = B.bu[q];
+            sink.pair(i, j, v3(u.x, u.y, u.z) * ((-1.0 * V3) * df));
+          }
+        }
+      } else {
+        const int k = path.z, m = path.w;
+        const int s1 = bond_slot(B, i, k);
+        // the last bond of the path, seen from j
+        const int last = (path.y == 2) ? k : m;
+        const int sj = bond_slot(B, j, last);
+        if (s1 < 0 || sj < 0) { *status |= ST_CIJ_OVERFLOW; return 0.0; }
+        const int q1 = i * B.mb + s1, qj = j * B.mb + sj;
+        const double f1 = B.bu[q1].w, fl = B.bu[qj].w;
+        double fmid = 1.0, dfmid = 0.0;
+        int sm = -1, qm = -1;
+        if (path.y == 3) {
+          sm = bond_slot(B, k, m);
+          if (sm < 0) { *status |= ST_CIJ_OVERFLOW; return 0.0; }
+          qm = k * B.mb + sm;
+          fmid = B.bu[qm].w;
+          dfmid = B.bd[qm].x;
+        }
+        // products in path order (AIREBO_LJ.cxx:396-402)
+        double m1 = (path.y == 2) ? 1.0 * fl : 1.0 * fmid * fl;
+        double ml = (path.y == 2) ? 1.0 * f1 : 1.0 * f1 * fmid;
+        double df1 = B.bd[q1].x, dfl = B.bd[qj].x;
+        if (df1 != 0.0) {
+          double4 u = B.bu[q1];
+          sink.cbond(i, s1, v3(u.x, u.y, u.z) * ((-m1 * V3) * df1));
+        }
+        if (dfl != 0.0) {
+          double4 u = B.bu[qj];
+          sink.cbond(j, sj, v3(u.x, u.y, u.z) * ((-ml * V3) * dfl));
+        }
+        if (path.y == 3 && dfmid != 0.0 && mid) {
+          double mm = 1.0 * f1 * fl;
+          int a = sink.a;
+          int c = mid->cnt[a];
+          if (c < mid->cap) {
+            mid->ent[(long)a * mid->cap + c] = make_int4(k, sm, m, 0);
+            mid->c[(long)a * mid->cap + c] = (-mm * V3) * dfmid;
+            mid->cnt[a] = c + 1;
+          } else {
+            *status |= ST_RECORD_OVERFLOW;
+          }
+        }
+      }
+    }
+    return SrSb * C * LJv;
+  }
+};
+
+// Gradient owed to atom a by recorded middle bonds k-m (a as k, or a as m).
+MDG_HD V3 mid_gather_atom(const BondList& B, const MidRecords& M, int a)
+{
+  V3 g = v3(0, 0, 0);
+  const int nb = B.nb[a];
+  // a as k: records written by any bond partner lo of a with k == a
+  for (int s = 0; s < nb; s++) {
+    const int lo = B.bj[a * B.mb + s];
+    const int c = M.cnt[lo];
+    for (int r = 0; r < c; r++) {
+      int4 e = M.ent[(long)lo * M.cap + r];
+      if (e.x != a) continue;
+      double4 u = B.bu[a * B.mb + e.y];
+      g += v3(u.x, u.y, u.z) * M.c[(long)lo * M.cap + r];
+    }
+  }
+  // a as m: records with k a bond partner of a, written by a partner lo of k
+  for (int s = 0; s < nb; s++) {
+    const int k = B.bj[a * B.mb + s];
+    double4 ua = B.bu[a * B.mb + s];  // (x_a - x_k)/r
+    const int nbk = B.nb[k];
+    for (int t = 0; t < nbk; t++) {
+      const int lo = B.bj[k * B.mb + t];
+      const int c = M.cnt[lo];
+      for (int r = 0; r < c; r++) {
+        int4 e = M.ent[(long)lo * M.cap + r];
+        if (e.x != k || e.z != a) continue;
+        g += v3(ua.x, ua.y, ua.z) * M.c[(long)lo * M.cap + r];
+      }
+    }
+  }
+  return g;
+}
+
+// LJ list pass for atom a: every LJ pair of a, evaluated as the reference's
+// pair (min, max); own gradient into glj[a], bond-slot gradients continue to
+// accumulate in a's A / W slots (after the REBO kernel).
+template <class S>
+MDG_HD void lj_atom(const LJ& X, const State& St, const NList& L, S& sink, double4* glj, double* e_lj,
+                    MidRecords* mid, unsigned int* status)
+{
+  const int a = sink.a;
+  if (mid) mid->cnt[a] = 0;
+  const double4 pa = St.pos[a];
+  const V3 xa = v3(pa.x, pa.y, pa.z);
+  const int ta = (int)pa.w;
+  const int cnt = L.cnt[a];
+  const int* lst = L.list + (long)a * L.cap;
+  double e = 0.0;
+  for (int s = 0; s < cnt; s++) {
+    const int b = lst[s];
+    const double4 pb = St.pos[b];
+    const int tb = (int)pb.w;
+    int lo = a, hi = b;
+    V3 rv;
+    if (a < b) rv = depos(St.box, xa, v3(pb.x, pb.y, pb.z));
+    else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), xa); }
+    const double d2 = norm2(rv);
+    const double R1 = X.P.R[ta][tb][0], R2 = X.P.R[ta][tb][1];
+    if (d2 > R2 * R2) continue;
+    PairG p;
+    p.rv = rv;
+    p.r = sqrt(d2);
+    p.u = rv / p.r;
+    cutoff(p.r, R1, R2, p.f, p.df);
+    p.alter = 0;
+    p.ralt = 0.0;
+    double E = X.pair(lo, hi, p, sink, (a == lo) ? mid : nullptr, status);
+    if (a == lo) e += E;
+  }
+  glj[a] = make_double4(sink.g.x, sink.g.y, sink.g.z, 0.0);
+  e_lj[a] = e;
+}
+
 }  // namespace mdg
-#endif

@@ -51,6 +51,7 @@ def lib():
         L.ref_rcutoff.restype = ctypes.c_double
         L.ref_rcutoff.argtypes = [vp, ctypes.c_int]
         L.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, ip, dp, dp, dp]
+        L.ref_last_run_times.argtypes = [vp, dp, ctypes.c_int]
         L.ref_tables.restype = ctypes.c_long
         L.ref_tables.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_long]
         L.ref_spline_eval.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
@@ -141,7 +142,9 @@ class RefSystem:
         et = np.zeros(nsteps)
         e0 = np.zeros(1)
         _check(lib().ref_run(self.h, nsteps, dt_fs, _dp(pos), _dp(vel), _ip(img), _dp(ep), _dp(et), _dp(e0)))
-        return {"pos": pos, "vel": vel, "image": img, "epot": ep, "etot": et, "e0": float(e0[0])}
+        ts = np.zeros(nsteps + 2)
+        lib().ref_last_run_times(self.h, _dp(ts), nsteps + 2)
+        return {"pos": pos, "vel": vel, "image": img, "epot": ep, "etot": et, "e0": float(e0[0]), "times": ts}
 
 
 def tables(which: int, brenner_set: int = 1) -> np.ndarray:

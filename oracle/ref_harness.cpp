@@ -23,6 +23,7 @@
 #include <iostream>
 #include <map>
 #include <set>
+#include <sys/time.h>
 
 #include <mdtk/SimLoop.hpp>
 #include <mdtk/potentials/manybody/AIREBO/REBO.hpp>
@@ -38,15 +39,23 @@ std::string g_last_error;
 
 enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8 };
 
+double wall_now()
+{
+  struct timeval tv;
+  gettimeofday(&tv, 0);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
 class FixedDtLoop : public SimLoop
 {
 public:
   Float fixed_dt;
   Float ekin_before;
-  std::vector<double> epot_log, etot_log;
+  std::vector<double> epot_log, etot_log, t_log;
   FixedDtLoop() : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0) {}
   virtual void doBeforeIteration()
   {
+    t_log.push_back(wall_now());
     dt = fixed_dt;
     ekin_before = energyKin();
   }
@@ -300,7 +309,11 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
     L.simTimeSaveTrajInterval = 1e9 * ps;
     L.epot_log.clear();
     L.etot_log.clear();
+    L.t_log.clear();
+    double t_start = wall_now();
     int rc = L.execute();
+    L.t_log.insert(L.t_log.begin(), t_start);
+    L.t_log.push_back(wall_now());
     if (rc != 0) { g_last_error = "SimLoop::execute failed"; return -1; }
     if ((int)L.epot_log.size() != nsteps) {
       std::ostringstream os;
@@ -328,6 +341,20 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
   }
 }
 
+}  // extern "C"
+
+extern "C" {
+/* Wall-clock stamps (s) of the last ref_run: [0] = entry to SimLoop::execute,
+ * [1 + s] = start of iteration s (doBeforeIteration), [nsteps + 1] = return.
+ * The list build and the initial energy evaluation happen between [0] and
+ * the end of iteration 0.  Returns the number of stamps. */
+int ref_last_run_times(void* h, double* out, int cap)
+{
+  RefCtx* c = (RefCtx*)h;
+  int n = (int)c->loop.t_log.size();
+  for (int i = 0; i < n && i < cap; i++) out[i] = c->loop.t_log[i];
+  return n;
+}
 }  // extern "C"
 
 /* ---- spline tables, in the layout the product builds its own copy in ----
