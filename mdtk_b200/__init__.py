@@ -52,7 +52,8 @@ class Params(ctypes.Structure):
         ("cap_lj_list", ctypes.c_int),
         ("cap_bonds", ctypes.c_int),
         ("cap_cij", ctypes.c_int),
-        ("cap_records", ctypes.c_int),
+        ("cap_special", ctypes.c_int),
+        ("special_avg", ctypes.c_int),
         ("device", ctypes.c_int),
     ]
 

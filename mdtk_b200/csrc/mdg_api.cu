@@ -181,27 +181,123 @@ __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
 
-__global__ void k_lj(const ReboParams* P, const ReboTables* Tb, LJParams LP, BondList B, CijTable T, State S, NList L,
-                     ForceOut O, MidRecords M, unsigned int* status)
+// Plain LJ pairs, one warp per atom: lanes stride the atom's LJ list;
+// pairs that need b*_ij or a connectivity gradient are compacted, in list
+// order, into the atom's special list.
+__global__ void k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* nbonds, ForceOut O,
+                           SpecialTasks Tk, unsigned int* status)
 {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= B.n) return;
-  Rebo R{*P, *Tb, B, status};
-  LJ X{LP, R, T};
-  Sink sink;
-  sink.a = a;
-  sink.g = v3(0, 0, 0);
-  sink.A = O.A + (long)a * O.mb * 3;
-  sink.W = O.W + (long)a * O.mb;
-  lj_atom(X, S, L, sink, O.glj, O.e_lj, &M, status);
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (a >= S.n) return;
+  const double4 pa = S.pos[a];
+  const V3 xa = v3(pa.x, pa.y, pa.z);
+  const int ta = (int)pa.w;
+  const int cnt = L.cnt[a];
+  const int* lst = L.list + (long)a * L.cap;
+  Sink sk;
+  sk.a = a;
+  sk.g = v3(0, 0, 0);
+  sk.A = nullptr;
+  sk.W = nullptr;
+  double e = 0.0;
+  int nsp = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int s = base + lane;
+    int kind = 0, b = -1;
+    if (s < cnt) {
+      b = lst[s];
+      kind = lj_plain_pair(P, T, S, a, b, xa, ta, sk, e);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
+    if (kind == 2) {
+      const int pos = nsp + __popc(m & ((1u << lane) - 1u));
+      if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
+    }
+    nsp += __popc(m);
+  }
+  double gx = sk.g.x, gy = sk.g.y, gz = sk.g.z;
+  for (int o = 16; o > 0; o >>= 1) {
+    gx += __shfl_xor_sync(0xffffffffu, gx, o);
+    gy += __shfl_xor_sync(0xffffffffu, gy, o);
+    gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+  }
+  if (lane == 0) {
+    O.glj[a] = make_double4(gx, gy, gz, 0.0);
+    O.e_lj[a] = e;
+    if (nsp > Tk.cap) {
+      atomicOr(status, ST_RECORD_OVERFLOW);
+      nsp = Tk.cap;
+    }
+    Tk.cnt[a] = nsp;
+    Tk.rsz[a] = nsp * rec_size(nbonds[a]);
+  }
 }
 
-__global__ void k_gather(BondList B, ForceOut O, int with_lj, MidRecords M, double4* grad)
+// Single-block exclusive scan: off[i] = sum cnt[0..i), off[n] = total.
+__global__ void k_exscan(const int* cnt, int n, int* off)
+{
+  __shared__ int part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  int chunk = (n + nt - 1) / nt;
+  int b = t * chunk, e = min(n, b + chunk);
+  int s = 0;
+  for (int c = b; c < e; c++) s += cnt[c];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    int acc = 0;
+    for (int q = 0; q < nt; q++) { int v = part[q]; part[q] = acc; acc += v; }
+    off[n] = acc;
+  }
+  __syncthreads();
+  int acc = part[t];
+  for (int c = b; c < e; c++) { off[c] = acc; acc += cnt[c]; }
+}
+
+__global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, unsigned int* status)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int c = Tk.cnt[a], o = Tk.off[a];
+  const int rs = rec_size(nbonds[a]);
+  for (int q = 0; q < c; q++) {
+    const int t = o + q;
+    const long ro = (long)Tk.roff[a] + (long)q * rs;
+    if (t < Tk.task_cap) {
+      Tk.flat[t] = make_int2(a, Tk.part[(long)a * Tk.cap + q]);
+      if (ro + rs <= Tk.rec_cap) Tk.trec[t] = ro;
+      else { Tk.trec[t] = -1; atomicOr(status, ST_RECORD_OVERFLOW); }
+    } else {
+      atomicOr(status, ST_RECORD_OVERFLOW);
+    }
+  }
+}
+
+// Special LJ pairs, one thread per (atom, pair) task.
+__global__ void k_lj_special(const ReboParams* P, const ReboTables* Tb, LJParams LP, BondList B, CijTable T,
+                             State S, SpecialTasks Tk, unsigned int* status)
+{
+  const int total = min(Tk.off[S.n], Tk.task_cap);
+  Rebo R{*P, *Tb, B, status};
+  LJ X{LP, R, T};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
+    lj_special_task(X, S, Tk, t, status);
+}
+
+__global__ void k_lj_reduce(BondList B, SpecialTasks Tk, ForceOut O)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < B.n) lj_reduce_atom(B, Tk, O, a);
+}
+
+__global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   V3 g = gather_atom(B, O, a, with_lj, nullptr);
-  if (with_lj) g += mid_gather_atom(B, M, a);
+  if (with_lj) g += mid_gather_atom(B, Tk, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
 }
 
@@ -361,9 +457,10 @@ struct mdg_ctx {
   int elog_cap = 0;
 
   CijTable cij;
-  MidRecords mid;
+  SpecialTasks spc;
 
   unsigned int* d_status = nullptr;
+  int special_blocks = 0;
 
   // profiling: event pairs bracketing each launch while enabled
   bool prof = false;
@@ -504,11 +601,12 @@ void free_system(mdg_ctx* c)
     std::memset(&c->grid[l], 0, sizeof(Grid));
     c->has_list[l] = false;
   }
-  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->mid.cnt, c->mid.ent, c->mid.c};
+  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
+                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc};
   for (void* p : lq)
     if (p) cudaFree(p);
   std::memset(&c->cij, 0, sizeof(c->cij));
-  std::memset(&c->mid, 0, sizeof(c->mid));
+  std::memset(&c->spc, 0, sizeof(c->spc));
   if (c->h_stage) cudaFreeHost(c->h_stage);
   c->h_stage = nullptr;
   c->pos = c->vel = c->acc = c->grad = nullptr;
@@ -615,10 +713,16 @@ int evaluate(mdg_ctx* c)
          c->fo, c->d_status);
   if (lj) {
     LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
-    LAUNCH(c, "lj_pairs", k_lj, nblk(c->n), kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S, c->nl[1], c->fo,
-           c->mid, c->d_status);
+    LAUNCH(c, "lj_plain", k_lj_plain, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb, c->fo,
+           c->spc, c->d_status);
+    LAUNCH(c, "lj_scan", k_exscan, 1, 1024, c->spc.cnt, c->n, c->spc.off);
+    LAUNCH(c, "lj_scan_rec", k_exscan, 1, 1024, c->spc.rsz, c->n, c->spc.roff);
+    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, c->d_status);
+    LAUNCH(c, "lj_special", k_lj_special, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
+           c->spc, c->d_status);
+    LAUNCH(c, "lj_reduce", k_lj_reduce, nblk(c->n), kThreads, B, c->spc, c->fo);
   }
-  LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->mid, c->grad);
+  LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
   return launch_check(c);
 }
 
@@ -687,7 +791,8 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   if (c->prm.cap_rebo_list <= 0) c->prm.cap_rebo_list = 64;
   if (c->prm.cap_lj_list <= 0) c->prm.cap_lj_list = 512;
   if (c->prm.cap_cij <= 0) c->prm.cap_cij = 128;
-  if (c->prm.cap_records <= 0) c->prm.cap_records = 64;
+  if (c->prm.cap_special <= 0) c->prm.cap_special = 64;
+  if (c->prm.special_avg <= 0) c->prm.special_avg = 48;
   c->mb = c->prm.cap_bonds;
   set_rebo_params(c->rp);
   set_tors_params(c->tp);
@@ -866,13 +971,29 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
     c->cij.cnt = dalloc<int>(n);
     c->cij.ent = dalloc<int4>((size_t)n * c->cij.cap);
     c->cij.w = dalloc<double>((size_t)n * c->cij.cap);
-    c->mid.cap = c->prm.cap_records;
-    c->mid.cnt = dalloc<int>(n);
-    c->mid.ent = dalloc<int4>((size_t)n * c->mid.cap);
-    c->mid.c = dalloc<double>((size_t)n * c->mid.cap);
-    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->mid.cnt || !c->mid.ent || !c->mid.c)
+    SpecialTasks& X = c->spc;
+    X.cap = c->prm.cap_special;
+    X.task_cap = (int)std::min<long>((long)n * c->prm.special_avg, 1L << 30);
+    X.rec_cap = (long)X.task_cap * rec_size(6);
+    X.cnt = dalloc<int>(n);
+    X.rsz = dalloc<int>(n);
+    X.part = dalloc<int>((size_t)n * X.cap);
+    X.off = dalloc<int>(n + 1);
+    X.roff = dalloc<int>(n + 1);
+    X.flat = dalloc<int2>(X.task_cap);
+    X.trec = dalloc<long>(X.task_cap);
+    X.rec = dalloc<double>(X.rec_cap);
+    X.mid = dalloc<int4>(X.task_cap);
+    X.midc = dalloc<double>(X.task_cap);
+    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
+        !X.trec || !X.rec || !X.mid || !X.midc)
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
-    CK(cudaMemset(c->mid.cnt, 0, n * sizeof(int)));
+    CK(cudaMemset(X.cnt, 0, n * sizeof(int)));
+    CK(cudaMemset(X.off, 0, (n + 1) * sizeof(int)));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    c->special_blocks = sms * 8;
   }
   if (cudaHostAlloc((void**)&c->h_stage, 2 * (size_t)n * sizeof(double4), cudaHostAllocDefault) != cudaSuccess)
     return fail(MDG_ERR_CUDA, "cudaHostAlloc (staging)");

@@ -53,14 +53,12 @@ struct CijTable {
   double* w;       // [n * cap]
 };
 
-// Middle-bond records of 3-bond connectivity paths (the bond k-m of
-// i-k-m-j belongs to neither end of the LJ pair): written by the lower-index
-// end, gathered by k and m.
-struct MidRecords {
-  int cap;
-  int* cnt;        // [n]
-  int4* ent;       // [n * cap] x = k, y = slot of m in k's bond list, z = m
-  double* c;       // [n * cap] dE/dr of the bond k-m
+// The middle bond k-m of a 3-bond connectivity path i-k-m-j belongs to
+// neither end of the LJ pair; its gradient is returned with the pair's task
+// (written by the lower-index end) and gathered later by k and m.
+struct MidOut {
+  int k, sm, m, valid;  // sm = slot of m in k's bond list
+  double c;             // dE/dr of the bond k-m
 };
 
 MDG_HD int bond_slot(const BondList& B, int c, int k)
@@ -176,6 +174,31 @@ MDG_HD double dSlj(double arg, double amin, double amax)
   return (-2.0 * t * (3.0 - 2.0 * t) + 2.0 * t * t) / (amax - amin);
 }
 
+// VLJ (AIREBO_LJ.cxx:158-189): f^LJ * 4 eps [(s/r)^12 - (s/r)^6]; with
+// V != 0 routes V * d/dr to the pair i-j.  Returns f*Val in `lj`, Val in `val`.
+template <class S>
+MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairG& pl, double V, S& sink, double& lj,
+                double& val)
+{
+  const double fv = pl.f;
+  lj = 0.0;
+  val = 0.0;
+  if (fv == 0.0) return;
+  const double r = pl.r;
+  const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
+  const double sdr = sigma / r;
+  double s6 = sdr;
+  for (int q = 2; q <= 6; q++) s6 *= sdr;
+  const double s12 = s6 * s6;
+  val = 4.0 * zeta * (s12 - s6);
+  if (V != 0.0) {
+    double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
+    sink.pair(i, j, pl.u * (der * fv * V));
+    if (pl.df != 0.0) sink.pair(i, j, pl.u * ((val * V) * pl.df));
+  }
+  lj = fv * val;
+}
+
 struct LJ {
   const LJParams& P;
   const Rebo& R;
@@ -199,7 +222,7 @@ struct LJ {
   // energy; the middle bond of a 3-bond path is recorded through `mid` when
   // non-null (the i end passes it).
   template <class S>
-  MDG_HD double pair(int i, int j, const PairG& pl, S& sink, MidRecords* mid, unsigned int* status) const
+  MDG_HD double pair(int i, int j, const PairG& pl, S& sink, MidOut* mid, unsigned int* status) const
   {
     // connectivity (AIREBO::Cij, AIREBO_LJ.cxx:381-408)
     int e = cij_find(T, i, j);
@@ -223,22 +246,10 @@ struct LJ {
       Stb = Slj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
       SrSb += Str * Stb - Str;
     }
-    // VLJ (AIREBO_LJ.cxx:158-189) with seed SrSb*C
-    const double fv = pl.f;
-    if (fv == 0.0) return 0.0;
-    const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
-    const double sdr = sigma / r;
-    double s6 = sdr;
-    for (int q = 2; q <= 6; q++) s6 *= sdr;
-    const double s12 = s6 * s6;
-    const double val = 4.0 * zeta * (s12 - s6);
-    const double V1 = SrSb * C;
-    if (V1 != 0.0) {
-      double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
-      sink.pair(i, j, pl.u * (der * fv * V1));
-      if (pl.df != 0.0) sink.pair(i, j, pl.u * ((val * V1) * pl.df));
-    }
-    const double LJv = fv * val;
+    // VLJ with seed SrSb*C
+    if (pl.f == 0.0) return 0.0;
+    double LJv, val;
+    vlj(P, ti, tj, i, j, pl, SrSb * C, sink, LJv, val);
     // StrStb gradient with seed C*LJ
     const double V2 = C * LJv;
     if (Str != 0.0 && V2 != 0.0) {
@@ -294,15 +305,11 @@ struct LJ {
         }
         if (path.y == 3 && dfmid != 0.0 && mid) {
           double mm = 1.0 * f1 * fl;
-          int a = sink.a;
-          int c = mid->cnt[a];
-          if (c < mid->cap) {
-            mid->ent[(long)a * mid->cap + c] = make_int4(k, sm, m, 0);
-            mid->c[(long)a * mid->cap + c] = (-mm * V3) * dfmid;
-            mid->cnt[a] = c + 1;
-          } else {
-            *status |= ST_RECORD_OVERFLOW;
-          }
+          mid->k = k;
+          mid->sm = sm;
+          mid->m = m;
+          mid->valid = 1;
+          mid->c = (-mm * V3) * dfmid;
         }
       }
     }
@@ -310,78 +317,164 @@ struct LJ {
   }
 };
 
-// Gradient owed to atom a by recorded middle bonds k-m (a as k, or a as m).
-MDG_HD V3 mid_gather_atom(const BondList& B, const MidRecords& M, int a)
+// Special LJ pairs (those needing b*_ij or a connectivity gradient) are
+// evaluated one task per (atom, pair); each task writes its own record and a
+// per-atom pass sums an atom's records in list order.
+struct SpecialTasks {
+  int cap;          // special pairs per atom
+  int task_cap;     // total tasks
+  long rec_cap;     // total record doubles
+  int* cnt;         // [n] special pairs of each atom (LJ-list order)
+  int* rsz;         // [n] record doubles of each atom: cnt * rec_size(bonds)
+  int* part;        // [n * cap] partner of each
+  int* off;         // [n + 1] exclusive prefix of cnt; off[n] = total
+  int* roff;        // [n + 1] exclusive prefix of rsz
+  int2* flat;       // [task_cap] (atom, partner)
+  long* trec;       // [task_cap] record offset of each task
+  double* rec;      // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]
+  int4* mid;        // [task_cap] middle-bond output (k, slot of m in k, m, valid)
+  double* midc;     // [task_cap]
+};
+
+// Record size of a task owned by an atom with nb bonds.
+MDG_HD int rec_size(int nb) { return 4 + 4 * nb; }
+
+// Classifies one LJ pair seen from atom a: returns 0 (skip), 1 (plain: C = 1
+// and S(t_r) = 0, so E = VLJ) or 2 (special).  For plain pairs adds the own
+// gradient and, at the lower end, the energy.
+template <class S>
+MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, int a, int b, V3 xa, int ta,
+                         S& sink, double& e)
+{
+  const double4 pb = St.pos[b];
+  const int tb = (int)pb.w;
+  int lo = a, hi = b;
+  V3 rv;
+  if (a < b) rv = depos(St.box, xa, v3(pb.x, pb.y, pb.z));
+  else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), xa); }
+  const double d2 = norm2(rv);
+  const double R1 = P.R[ta][tb][0], R2 = P.R[ta][tb][1];
+  if (d2 > R2 * R2) return 0;
+  const int ei = cij_find(T, lo, hi);
+  const double w = ei >= 0 ? T.w[(long)lo * T.cap + ei] : 0.0;
+  const double C = 1 - w;
+  if (!(C > 0.0)) return 0;
+  PairG p;
+  p.rv = rv;
+  p.r = sqrt(d2);
+  const double Str = Slj(p.r, P.RLJ[ta][tb][0], P.RLJ[ta][tb][1]);
+  if (Str != 0.0 || w != 0.0) return 2;
+  p.u = rv / p.r;
+  cutoff(p.r, R1, R2, p.f, p.df);
+  p.alter = 0;
+  p.ralt = 0.0;
+  double LJv, val;
+  const int tlo = lo == a ? ta : tb, thi = lo == a ? tb : ta;
+  vlj(P, tlo, thi, lo, hi, p, 1.0 * C, sink, LJv, val);
+  if (a == lo) e += 1.0 * C * LJv;
+  return 1;
+}
+
+// Gradient owed to atom a by middle bonds k-m of connectivity paths (a as k
+// or as m); the tasks of every bond partner lo of k are scanned in order.
+MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
 {
   V3 g = v3(0, 0, 0);
   const int nb = B.nb[a];
-  // a as k: records written by any bond partner lo of a with k == a
   for (int s = 0; s < nb; s++) {
     const int lo = B.bj[a * B.mb + s];
-    const int c = M.cnt[lo];
-    for (int r = 0; r < c; r++) {
-      int4 e = M.ent[(long)lo * M.cap + r];
-      if (e.x != a) continue;
+    const int t0 = X.off[lo], t1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+    for (int t = t0; t < t1; t++) {
+      int4 e = X.mid[t];
+      if (!e.w || e.x != a) continue;
       double4 u = B.bu[a * B.mb + e.y];
-      g += v3(u.x, u.y, u.z) * M.c[(long)lo * M.cap + r];
+      g += v3(u.x, u.y, u.z) * X.midc[t];
     }
   }
-  // a as m: records with k a bond partner of a, written by a partner lo of k
   for (int s = 0; s < nb; s++) {
     const int k = B.bj[a * B.mb + s];
-    double4 ua = B.bu[a * B.mb + s];  // (x_a - x_k)/r
+    double4 ua = B.bu[a * B.mb + s];
     const int nbk = B.nb[k];
-    for (int t = 0; t < nbk; t++) {
-      const int lo = B.bj[k * B.mb + t];
-      const int c = M.cnt[lo];
-      for (int r = 0; r < c; r++) {
-        int4 e = M.ent[(long)lo * M.cap + r];
-        if (e.x != k || e.z != a) continue;
-        g += v3(ua.x, ua.y, ua.z) * M.c[(long)lo * M.cap + r];
+    for (int q = 0; q < nbk; q++) {
+      const int lo = B.bj[k * B.mb + q];
+      const int t0 = X.off[lo], t1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+      for (int t = t0; t < t1; t++) {
+        int4 e = X.mid[t];
+        if (!e.w || e.x != k || e.z != a) continue;
+        g += v3(ua.x, ua.y, ua.z) * X.midc[t];
       }
     }
   }
   return g;
 }
 
-// LJ list pass for atom a: every LJ pair of a, evaluated as the reference's
-// pair (min, max); own gradient into glj[a], bond-slot gradients continue to
-// accumulate in a's A / W slots (after the REBO kernel).
-template <class S>
-MDG_HD void lj_atom(const LJ& X, const State& St, const NList& L, S& sink, double4* glj, double* e_lj,
-                    MidRecords* mid, unsigned int* status)
+// Records one special task: the full pair term from end a with a private sink.
+MDG_HD void lj_special_task(const LJ& X, const State& St, SpecialTasks& Tk, int t, unsigned int* status)
 {
-  const int a = sink.a;
-  if (mid) mid->cnt[a] = 0;
-  const double4 pa = St.pos[a];
-  const V3 xa = v3(pa.x, pa.y, pa.z);
-  const int ta = (int)pa.w;
-  const int cnt = L.cnt[a];
-  const int* lst = L.list + (long)a * L.cap;
-  double e = 0.0;
-  for (int s = 0; s < cnt; s++) {
-    const int b = lst[s];
-    const double4 pb = St.pos[b];
-    const int tb = (int)pb.w;
-    int lo = a, hi = b;
-    V3 rv;
-    if (a < b) rv = depos(St.box, xa, v3(pb.x, pb.y, pb.z));
-    else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), xa); }
-    const double d2 = norm2(rv);
-    const double R1 = X.P.R[ta][tb][0], R2 = X.P.R[ta][tb][1];
-    if (d2 > R2 * R2) continue;
-    PairG p;
-    p.rv = rv;
-    p.r = sqrt(d2);
-    p.u = rv / p.r;
-    cutoff(p.r, R1, R2, p.f, p.df);
-    p.alter = 0;
-    p.ralt = 0.0;
-    double E = X.pair(lo, hi, p, sink, (a == lo) ? mid : nullptr, status);
-    if (a == lo) e += E;
+  const int2 ap = Tk.flat[t];
+  const int a = ap.x, b = ap.y;
+  const int nba = X.R.B.nb[a];
+  const long ro = Tk.trec[t];
+  if (ro < 0) return;  // beyond the record capacity (already flagged)
+  double* rec = Tk.rec + ro;
+  Sink sink;
+  sink.a = a;
+  sink.g = v3(0, 0, 0);
+  sink.A = rec + 4;
+  sink.W = rec + 4 + 3 * nba;
+  for (int s = 0; s < nba; s++) {
+    sink.A[3 * s] = sink.A[3 * s + 1] = sink.A[3 * s + 2] = 0.0;
+    sink.W[s] = 0.0;
   }
-  glj[a] = make_double4(sink.g.x, sink.g.y, sink.g.z, 0.0);
-  e_lj[a] = e;
+  const double4 pa = St.pos[a], pb = St.pos[b];
+  int lo = a, hi = b;
+  V3 rv;
+  if (a < b) rv = depos(St.box, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z));
+  else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), v3(pa.x, pa.y, pa.z)); }
+  const int tlo = (int)St.pos[lo].w, thi = (int)St.pos[hi].w;
+  PairG p;
+  p.rv = rv;
+  p.r = sqrt(norm2(rv));
+  p.u = rv / p.r;
+  cutoff(p.r, X.P.R[tlo][thi][0], X.P.R[tlo][thi][1], p.f, p.df);
+  p.alter = 0;
+  p.ralt = 0.0;
+  MidOut mo;
+  mo.valid = 0;
+  double E = X.pair(lo, hi, p, sink, (a == lo) ? &mo : nullptr, status);
+  rec[0] = sink.g.x;
+  rec[1] = sink.g.y;
+  rec[2] = sink.g.z;
+  rec[3] = (a == lo) ? E : 0.0;
+  Tk.mid[t] = make_int4(mo.k, mo.sm, mo.m, mo.valid);
+  Tk.midc[t] = mo.valid ? mo.c : 0.0;
+}
+
+// Sums atom a's special-task records (in list order) into its accumulators.
+MDG_HD void lj_reduce_atom(const BondList& B, const SpecialTasks& Tk, ForceOut& O, int a)
+{
+  const int nb = B.nb[a];
+  double4 g0 = O.glj[a];
+  V3 g = v3(g0.x, g0.y, g0.z);
+  double e = O.e_lj[a];
+  double* A = O.A + (long)a * O.mb * 3;
+  double* W = O.W + (long)a * O.mb;
+  const int t0 = Tk.off[a], t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
+  for (int t = t0; t < t1; t++) {
+    const long ro = Tk.trec[t];
+    if (ro < 0) continue;
+    const double* rec = Tk.rec + ro;
+    g += v3(rec[0], rec[1], rec[2]);
+    e += rec[3];
+    for (int s = 0; s < nb; s++) {
+      A[3 * s] += rec[4 + 3 * s];
+      A[3 * s + 1] += rec[4 + 3 * s + 1];
+      A[3 * s + 2] += rec[4 + 3 * s + 2];
+      W[s] += rec[4 + 3 * nb + s];
+    }
+  }
+  O.glj[a] = make_double4(g.x, g.y, g.z, 0.0);
+  O.e_lj[a] = e;
 }
 
 }  // namespace mdg

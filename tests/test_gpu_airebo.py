@@ -109,7 +109,7 @@ def test_deterministic_repeat():
 
 def test_record_capacity_overflow_is_reported():
     s = SYSTEMS["diamond4_hot"]()
-    ctx = _gpu(s, cap_records=1)
+    ctx = _gpu(s, cap_special=1)
     with pytest.raises(M.MdgError) as e:
         ctx.compute()
     assert e.value.code == -8
