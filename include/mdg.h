@@ -163,6 +163,24 @@ int mdg_profile_read(mdg_ctx* ctx, int max, char* names, double* ms, int64_t* co
  * the bond-order kernels.  No reference counterpart. */
 int mdg_pipe_peak(int device, int fp32, double* tflops);
 
+/* REBO energy and gradient (plus the torsion term when with_torsion != 0)
+ * for callers that cannot allocate device memory: hosts whose device memory
+ * is all owned by their own allocator, which forbids driver allocations by
+ * plugins, and time-critical loops that cannot afford the device-wide
+ * synchronisation cudaMalloc/cudaFree imply.  Nothing is allocated: every
+ * intermediate lives in a fixed static device array (about 11 MiB, held by
+ * every GPU that loads the library until the process exits), so n is limited
+ * to 4096 atoms; larger n is rejected with MDG_ERR_ARG.  pos (n*3, Angstrom),
+ * z (n atomic numbers), energy (2 doubles: REBO, torsion, eV) and grad (n*3,
+ * eV/Angstrom, overwritten) are DEVICE pointers owned by the caller; box and
+ * pbc are host arrays.  Work runs on `stream` (cudaStream_t as void*; NULL =
+ * legacy default stream) and the call waits for it to report the status.
+ * The first call on a device sets that device up with synchronous copies, so
+ * make it before any stream capture.  Calls share the one scratch array:
+ * calls that overlap on the GPU race.  No counterpart in the reference. */
+int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const double box[3], const int32_t pbc[3],
+                             int with_torsion, double* energy, double* grad, void* stream);
+
 /* Test hook: the REBO spline tables the library built on the host, flattened
  * in the oracle's export order; returns the number of doubles (writes at most
  * cap).  Host only; needs no device. */

@@ -22,7 +22,7 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in ("mdg_api.cu", "mdg_tables.cpp")]
+    return [os.path.join(CSRC, f) for f in ("mdg_api.cu", "mdg_noalloc.cu", "mdg_tables.cpp")]
 
 
 def headers():

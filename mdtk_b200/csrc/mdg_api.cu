@@ -758,6 +758,9 @@ int read_status(mdg_ctx* c)
 
 }  // namespace
 
+// Lets the library's other translation units report through mdg_last_error().
+__attribute__((visibility("hidden"))) void mdg_set_last_error_internal(const char* msg) { g_err = msg; }
+
 // ---------------------------------------------------------------- C ABI
 
 extern "C" {
