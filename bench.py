@@ -182,7 +182,9 @@ def main():
     n = len(s["z"])
     ctx = M.Context(potentials=M.POT_AIREBO, device=local)
     ctx.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
-    stream = torch.cuda.current_stream()
+    # one explicit stream for the library's kernels, the L2 flush and the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     # warm-up (also builds the lists and the initial accelerations)

@@ -57,7 +57,8 @@ typedef struct mdg_ctx mdg_ctx;
 
 typedef struct mdg_params {
   int potentials;     /* MDG_POT_* bitmask */
-  int brenner_set;    /* Brenner parameter set 1 or 2 (Brenner::POTENTIAL1/2) */
+  int brenner_set;    /* Brenner parameter set 1 or 2 (Brenner::POTENTIAL1/2); Brenner excludes
+                         REBO and the LJ term in one context (the LJ term is built on REBO) */
   int precision;      /* MDG_PREC_* */
   int units;          /* MDG_UNITS_* */
   int lj_cut_mode;    /* 0: reference cosine cutoff 5.0-5.5/4.5-5.0/4.0-4.5 A; 1: 3 sigma */
@@ -185,6 +186,10 @@ int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const d
  * in the oracle's export order; returns the number of doubles (writes at most
  * cap).  Host only; needs no device. */
 int64_t mdg_debug_rebo_tables(double* out, int64_t cap);
+
+/* Test hook: the Brenner tables of parameter set 1 or 2 (H_CC, H_CH, F), in
+ * the oracle's export order.  Host only. */
+int64_t mdg_debug_brenner_tables(int set, double* out, int64_t cap);
 
 #ifdef __cplusplus
 }

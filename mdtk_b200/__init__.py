@@ -90,6 +90,8 @@ def lib():
         L.mdg_profile_read.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_int)]
         L.mdg_pipe_peak.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.mdg_debug_brenner_tables.argtypes = [ctypes.c_int, dp, ctypes.c_int64]
+        L.mdg_debug_brenner_tables.restype = ctypes.c_int64
         L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
         L.mdg_debug_rebo_tables.restype = ctypes.c_int64
         _lib = L
@@ -114,6 +116,13 @@ def pipe_peak(device: int = 0, fp32: bool = False) -> float:
     out = np.zeros(1)
     _check(lib().mdg_pipe_peak(device, 1 if fp32 else 0, _dp(out)))
     return float(out[0])
+
+
+def debug_brenner_tables(set_: int) -> np.ndarray:
+    n = lib().mdg_debug_brenner_tables(set_, None, 0)
+    out = np.zeros(n)
+    lib().mdg_debug_brenner_tables(set_, _dp(out), n)
+    return out
 
 
 def debug_rebo_tables() -> np.ndarray:

@@ -19,6 +19,7 @@
 #include "mdg_step.cuh"
 #include "mdg_tables.h"
 #include "mdg_lj.cuh"
+#include "mdg_brenner.cuh"
 
 using namespace mdg;
 
@@ -173,6 +174,15 @@ __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, Tor
   rebo_atom(R, TP, do_rebo, do_tors, O, a);
 }
 
+__global__ void k_brenner(const BrennerParams* P, const BrennerTables* T, BondList B, ForceOut O,
+                          unsigned int* status)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.n) return;
+  Brenner R{*P, *T, B, status};
+  brenner_atom(R, O, a);
+}
+
 constexpr int kCijLocal = 128;  // per-thread connectivity table capacity
 
 __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
@@ -254,6 +264,65 @@ __global__ void k_exscan(const int* cnt, int n, int* off)
   __syncthreads();
   int acc = part[t];
   for (int c = b; c < e; c++) { off[c] = acc; acc += cnt[c]; }
+}
+
+// Tiled exclusive scan of up to two int arrays at once (blockIdx.y picks the
+// array): per-tile block scan, a scan of the tile sums, then the tile offsets
+// added back.  off has n + 1 entries; off[n] = total.
+struct ScanPair {
+  const int* in[2];
+  int* out[2];
+  int* tile[2];   // [ntiles + 1] tile sums, then tile offsets
+  int n, ntiles;
+};
+constexpr int kScanTile = 1024;
+
+__global__ void k_scan_tiles(ScanPair P)
+{
+  __shared__ int wsum[32];
+  const int y = blockIdx.y;
+  const int i = blockIdx.x * kScanTile + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int v = (i < P.n) ? P.in[y][i] : 0;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  const int incl = x + (wid > 0 ? wsum[wid - 1] : 0);
+  if (i < P.n) P.out[y][i] = incl - v;
+  if (threadIdx.x == kScanTile - 1) P.tile[y][blockIdx.x] = incl;
+}
+
+__global__ void k_scan_top(ScanPair P)
+{
+  const int y = blockIdx.y;
+  if (threadIdx.x != 0) return;
+  int acc = 0;
+  for (int t = 0; t < P.ntiles; t++) {
+    int v = P.tile[y][t];
+    P.tile[y][t] = acc;
+    acc += v;
+  }
+  P.out[y][P.n] = acc;
+}
+
+__global__ void k_scan_add(ScanPair P)
+{
+  const int y = blockIdx.y;
+  const int i = blockIdx.x * kScanTile + threadIdx.x;
+  if (i < P.n && blockIdx.x > 0) P.out[y][i] += P.tile[y][blockIdx.x];
 }
 
 __global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, unsigned int* status)
@@ -422,6 +491,8 @@ struct mdg_ctx {
   LJParams ljp;
   ReboTables* d_tables = nullptr;
   ReboParams* d_rp = nullptr;
+  BrennerTables* d_btables = nullptr;
+  BrennerParams* d_bp = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int64_t launches = 0;
@@ -461,6 +532,13 @@ struct mdg_ctx {
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
+  int* scan_tiles = nullptr;  // 2 * (n / 1024 + 2)
+
+  // one MD step captured as a CUDA graph (replayed when no per-step energies are wanted)
+  cudaGraphExec_t step_graph = nullptr;
+  double graph_dt = 0.0;
+  cudaStream_t graph_stream = nullptr;
+  int graph_launches = 0;
 
   // profiling: event pairs bracketing each launch while enabled
   bool prof = false;
@@ -602,7 +680,10 @@ void free_system(mdg_ctx* c)
     c->has_list[l] = false;
   }
   void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
-                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc};
+                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->scan_tiles};
+  c->scan_tiles = nullptr;
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
   for (void* p : lq)
     if (p) cudaFree(p);
   std::memset(&c->cij, 0, sizeof(c->cij));
@@ -711,12 +792,24 @@ int evaluate(mdg_ctx* c)
   BondList B = c->BL();
   LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0, tors ? 1 : 0,
          c->fo, c->d_status);
+  if (pot & MDG_POT_BRENNER)
+    LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
     LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
     LAUNCH(c, "lj_plain", k_lj_plain, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb, c->fo,
            c->spc, c->d_status);
-    LAUNCH(c, "lj_scan", k_exscan, 1, 1024, c->spc.cnt, c->n, c->spc.off);
-    LAUNCH(c, "lj_scan_rec", k_exscan, 1, 1024, c->spc.rsz, c->n, c->spc.roff);
+    ScanPair sp;
+    sp.in[0] = c->spc.cnt;
+    sp.in[1] = c->spc.rsz;
+    sp.out[0] = c->spc.off;
+    sp.out[1] = c->spc.roff;
+    sp.tile[0] = c->scan_tiles;
+    sp.tile[1] = c->scan_tiles + (c->n / kScanTile + 2);
+    sp.n = c->n;
+    sp.ntiles = (c->n + kScanTile - 1) / kScanTile;
+    LAUNCH(c, "lj_scan_tiles", k_scan_tiles, dim3(sp.ntiles, 2), kScanTile, sp);
+    LAUNCH(c, "lj_scan_top", k_scan_top, dim3(1, 2), 32, sp);
+    LAUNCH(c, "lj_scan_add", k_scan_add, dim3(sp.ntiles, 2), kScanTile, sp);
     LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, c->d_status);
     LAUNCH(c, "lj_special", k_lj_special, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
            c->spc, c->d_status);
@@ -783,7 +876,12 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   *out = nullptr;
   if ((p->potentials & MDG_POT_AIREBO_LJ) && !(p->potentials & MDG_POT_REBO))
     return fail(MDG_ERR_ARG, "the AIREBO LJ term needs REBO (AIREBO_LJ.cxx:204-212)");
-  if (p->potentials & MDG_POT_BRENNER) return fail(MDG_ERR_ARG, "Brenner is not available in this build");
+  if ((p->potentials & MDG_POT_BRENNER) && (p->potentials & (MDG_POT_REBO | MDG_POT_AIREBO_LJ)))
+    return fail(MDG_ERR_ARG, "choose one bond-order potential: Brenner or REBO (the LJ term uses REBO)");
+  if ((p->potentials & MDG_POT_BRENNER) && p->brenner_set != 1 && p->brenner_set != 2)
+    return fail(MDG_ERR_ARG, "Brenner parameter set must be 1 or 2");
+  if (!(p->potentials & (MDG_POT_REBO | MDG_POT_BRENNER | MDG_POT_ETORS)))
+    return fail(MDG_ERR_ARG, "no potential selected");
   if (p->precision != MDG_PREC_FP64) return fail(MDG_ERR_ARG, "only FP64 precision is available in this build");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(MDG_ERR_CUDA, "no CUDA device");
@@ -814,6 +912,18 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   cudaMemcpy(c->d_tables, h, sizeof(ReboTables), cudaMemcpyHostToDevice);
   cudaMemcpy(c->d_rp, &c->rp, sizeof(ReboParams), cudaMemcpyHostToDevice);
   delete h;
+  if (p->potentials & MDG_POT_BRENNER) {
+    BrennerTables* bt = new BrennerTables();
+    BrennerParams bp;
+    build_brenner_tables(p->brenner_set, bt, nullptr);
+    set_brenner_params(bp, p->brenner_set);
+    c->d_btables = dalloc<BrennerTables>(1);
+    c->d_bp = dalloc<BrennerParams>(1);
+    if (!c->d_btables || !c->d_bp) { delete bt; mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc (Brenner)"); }
+    cudaMemcpy(c->d_btables, bt, sizeof(BrennerTables), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_bp, &bp, sizeof(BrennerParams), cudaMemcpyHostToDevice);
+    delete bt;
+  }
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     mdg_destroy(c);
     return fail(MDG_ERR_CUDA, "cudaStreamCreate");
@@ -837,7 +947,7 @@ int mdg_destroy(mdg_ctx* c)
   if (!c) return MDG_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_system(c);
-  void* ptrs[] = {c->d_tables, c->d_rp, c->d_status, c->d_need, c->d_force, c->d_energy};
+  void* ptrs[] = {c->d_tables, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -993,6 +1103,8 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
     CK(cudaMemset(X.cnt, 0, n * sizeof(int)));
     CK(cudaMemset(X.off, 0, (n + 1) * sizeof(int)));
+    c->scan_tiles = dalloc<int>(2 * (n / kScanTile + 2));
+    if (!c->scan_tiles) return fail(MDG_ERR_CUDA, "cudaMalloc (scan)");
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1124,6 +1236,35 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->d_elog = dalloc<double>((size_t)nsteps * 4);
     if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
     c->elog_cap = nsteps;
+  }
+  // Without per-step energies (and without profiling) a step is replayed
+  // from a CUDA graph: same kernels, same arguments, no host launch cost.
+  if (!log && !c->prof && nsteps > 0) {
+    if (!c->step_graph || c->graph_dt != dtf || c->graph_stream != c->stream) {
+      if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+      c->step_graph = nullptr;
+      cudaGraph_t g = nullptr;
+      int64_t l0 = c->launches;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
+      rc = evaluate(c);
+      LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+      c->graph_launches = (int)(c->launches - l0);
+      c->launches = l0;
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&c->step_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      c->graph_dt = dtf;
+      c->graph_stream = c->stream;
+    }
+    for (int s = 0; s < nsteps; s++) {
+      CK(cudaGraphLaunch(c->step_graph, c->stream));
+      c->launches += c->graph_launches;
+    }
+    return launch_check(c);
   }
   for (int s = 0; s < nsteps; s++) {
     LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
@@ -1274,6 +1415,16 @@ int mdg_pipe_peak(int device, int fp32, double* tflops)
   CK(cudaGetLastError());
   *tflops = best;
   return MDG_OK;
+}
+
+int64_t mdg_debug_brenner_tables(int set, double* out, int64_t cap)
+{
+  BrennerTables* h = new BrennerTables();
+  std::vector<double> flat;
+  build_brenner_tables(set, h, &flat);
+  delete h;
+  for (int64_t i = 0; i < (int64_t)flat.size() && i < cap; i++) out[i] = flat[i];
+  return (int64_t)flat.size();
 }
 
 int64_t mdg_debug_rebo_tables(double* out, int64_t cap)

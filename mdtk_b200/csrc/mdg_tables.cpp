@@ -15,6 +15,7 @@
 
 #include "mdg_spline.cuh"
 #include "mdg_tables.h"
+#include "mdg_brenner.cuh"
 
 namespace mdg {
 namespace {
@@ -447,7 +448,116 @@ void put_t(const TStep* steps, size_t ns, double T[5][5][16][4][64], double Tint
         for (int d = 0; d < 4; d++) flat_int.push_back(Tint[i][j][k][d]);
 }
 
+// ---- Brenner tables (Brenner/cubici.cxx:36-346) ----
+struct Knot2v { int i, j; double v; };
+// H_CC knots, parameter sets 1 and 2 (Brenner/cubici.cxx:47-60)
+const Knot2v kHCC[2][5] = {
+  {{1, 1, -0.0175}, {2, 0, -0.0070}, {3, 0, 0.0119}, {1, 2, 0.0115}, {2, 1, 0.0118}},
+  {{1, 1, -0.0226}, {2, 0, -0.0061}, {3, 0, 0.0173}, {1, 2, 0.0149}, {2, 1, 0.0160}}};
+// H_CH knots and corner derivatives (Brenner/cubici.cxx:115-148)
+const Knot2v kHCH[2][9] = {
+  {{1, 0, -0.0760}, {2, 0, -0.2163}, {3, 0, -0.3375}, {0, 1, -0.1792}, {0, 2, -0.2407},
+   {1, 1, -0.2477}, {2, 1, -0.3320}, {0, 3, -0.3323}, {1, 2, -0.3321}},
+  {{1, 0, -0.0984}, {2, 0, -0.2878}, {3, 0, -0.4507}, {0, 1, -0.2479}, {0, 2, -0.3221},
+   {1, 1, -0.3344}, {2, 1, -0.4438}, {0, 3, -0.4460}, {1, 2, -0.4449}}};
+const Knot2v kHCHdH[2][2] = {{{2, 0, -0.13075}, {1, 1, -0.0764}}, {{2, 0, -0.17615}, {1, 1, -0.09795}}};
+const Knot2v kHCHdC[2][2] = {{{0, 2, -0.07655}, {1, 1, -0.12805}}, {{0, 2, -0.09905}, {1, 1, -0.17325}}};
+
+struct Knot3v { int i, j, k; double v; };
+// F knots (value, symmetric in i, j), and its i/j derivatives (Brenner/cubici.cxx:205-278)
+const Knot3v kFv[2][14] = {
+  {{2, 3, 1, -0.0465}, {2, 3, 2, -0.0465}, {1, 2, 2, -0.0355}, {1, 2, 1, 0.0126}, {1, 3, 1, -0.1130},
+   {1, 3, 2, -0.1130}, {0, 3, 1, -0.1220}, {0, 3, 2, -0.1220}, {0, 2, 2, -0.0445}, {0, 2, 1, 0.0320},
+   {0, 1, 1, 0.1100}, {1, 1, 2, 0.0074}, {1, 1, 1, 0.1511}, {2, 2, 1, 0.0750}},
+  {{2, 3, 1, -0.0363}, {2, 3, 2, -0.0363}, {1, 2, 2, -0.0243}, {1, 2, 1, 0.0120}, {1, 3, 1, -0.0903},
+   {1, 3, 2, -0.0903}, {0, 3, 1, -0.0904}, {0, 3, 2, -0.0904}, {0, 2, 2, -0.0269}, {0, 2, 1, 0.0427},
+   {0, 1, 1, 0.0996}, {1, 1, 2, 0.0108}, {1, 1, 1, 0.1264}, {2, 2, 1, 0.0605}}};
+const Knot3v kFdI[2][8] = {
+  {{2, 0, 1, -0.1160}, {2, 1, 1, -0.13205}, {2, 0, 2, -0.0610}, {1, 2, 2, 0.02225}, {1, 3, 2, 0.03775},
+   {2, 3, 2, 0.0565}, {2, 3, 1, 0.0565}, {2, 1, 2, -0.0602}},
+  {{2, 0, 1, -0.0950}, {2, 1, 1, -0.10835}, {2, 0, 2, -0.0452}, {1, 2, 2, 0.01345}, {1, 3, 2, 0.02705},
+   {2, 3, 2, 0.04515}, {2, 3, 1, 0.04515}, {2, 1, 2, -0.05055}}};
+const Knot3v kFdJ[2][8] = {
+  {{0, 2, 1, -0.1160}, {1, 2, 1, -0.13205}, {0, 2, 2, -0.0610}, {2, 1, 2, 0.02225}, {3, 1, 2, 0.03775},
+   {3, 2, 2, 0.0565}, {3, 2, 1, 0.0565}, {1, 2, 2, -0.0602}},
+  {{0, 2, 1, -0.0950}, {1, 2, 1, -0.10835}, {0, 2, 2, -0.0452}, {2, 1, 2, 0.01345}, {3, 1, 2, 0.02705},
+   {3, 2, 2, 0.04515}, {3, 2, 1, 0.04515}, {1, 2, 2, -0.05055}}};
+
+void put_h(const double H[5][5], const double DH[5][5], const double DC[5][5], double out[4][4][3][16],
+           std::vector<double>& flat)
+{
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double x[2] = {(double)i, (double)i + 1}, y[2] = {(double)j, (double)j + 1};
+      double z[2][2] = {{H[i][j], H[i][j + 1]}, {H[i + 1][j], H[i + 1][j + 1]}};
+      double dx[2][2] = {{DH[i][j], DH[i][j + 1]}, {DH[i + 1][j], DH[i + 1][j + 1]}};
+      double dy[2][2] = {{DC[i][j], DC[i][j + 1]}, {DC[i + 1][j], DC[i + 1][j + 1]}};
+      Poly cell = bicubic(x, y, z, dx, dy);
+      for (int d = 0; d < 3; d++) {
+        std::vector<double> c;
+        emit(cell, d, c);
+        for (int t = 0; t < 16; t++) { out[i][j][d][t] = c[t]; flat.push_back(c[t]); }
+      }
+    }
+}
+
 }  // namespace
+
+void build_brenner_tables(int set, BrennerTables* tb, std::vector<double>* flat_out)
+{
+  const int ps = (set == 2) ? 1 : 0;
+  std::vector<double> flat;
+  double H[5][5], Z[5][5], DH[5][5], DC[5][5];
+  std::memset(Z, 0, sizeof(Z));
+  // H_CC: corner values only (Brenner/cubici.cxx:36-96)
+  std::memset(H, 0, sizeof(H));
+  for (int q = 0; q < 5; q++) H[kHCC[ps][q].i][kHCC[ps][q].j] = kHCC[ps][q].v;
+  put_h(H, Z, Z, tb->H[0], flat);
+  // H_CH with its corner derivatives (Brenner/cubici.cxx:98-183)
+  std::memset(H, 0, sizeof(H));
+  std::memset(DH, 0, sizeof(DH));
+  std::memset(DC, 0, sizeof(DC));
+  for (int q = 0; q < 9; q++) H[kHCH[ps][q].i][kHCH[ps][q].j] = kHCH[ps][q].v;
+  for (int q = 0; q < 2; q++) DH[kHCHdH[ps][q].i][kHCHdH[ps][q].j] = kHCHdH[ps][q].v;
+  for (int q = 0; q < 2; q++) DC[kHCHdC[ps][q].i][kHCHdC[ps][q].j] = kHCHdC[ps][q].v;
+  put_h(H, DH, DC, tb->H[1], flat);
+  // F: values symmetric in (i, j), k >= 3 copied from k = 2 (Brenner/cubici.cxx:186-346)
+  static double F[5][5][6], FI[5][5][6], FJ[5][5][6];
+  std::memset(F, 0, sizeof(F));
+  std::memset(FI, 0, sizeof(FI));
+  std::memset(FJ, 0, sizeof(FJ));
+  for (int q = 0; q < 14; q++) {
+    const Knot3v& k = kFv[ps][q];
+    F[k.i][k.j][k.k] = F[k.j][k.i][k.k] = k.v;
+  }
+  for (int q = 0; q < 8; q++) FI[kFdI[ps][q].i][kFdI[ps][q].j][kFdI[ps][q].k] = kFdI[ps][q].v;
+  for (int q = 0; q < 8; q++) FJ[kFdJ[ps][q].i][kFdJ[ps][q].j][kFdJ[ps][q].k] = kFdJ[ps][q].v;
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++)
+      for (int k = 3; k < 6; k++) F[i][j][k] = F[i][j][2];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 5; k++) {
+        double x[2] = {(double)i, (double)i + 1}, y[2] = {(double)j, (double)j + 1},
+               z[2] = {(double)k, (double)k + 1};
+        double v[2][2][2], dx[2][2][2], dy[2][2][2], dz[2][2][2];
+        for (int a = 0; a < 2; a++)
+          for (int b = 0; b < 2; b++)
+            for (int c = 0; c < 2; c++) {
+              v[a][b][c] = F[i + a][j + b][k + c];
+              dx[a][b][c] = FI[i + a][j + b][k + c];
+              dy[a][b][c] = FJ[i + a][j + b][k + c];
+              dz[a][b][c] = 0.0;
+            }
+        Poly cell = tricubic(x, y, z, v, dx, dy, dz);
+        for (int d = 0; d < 4; d++) {
+          std::vector<double> c;
+          emit(cell, d, c);
+          for (int t = 0; t < 64; t++) { tb->F[i][j][k][d][t] = c[t]; flat.push_back(c[t]); }
+        }
+      }
+  if (flat_out) *flat_out = flat;
+}
 
 void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out)
 {

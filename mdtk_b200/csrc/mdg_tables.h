@@ -11,4 +11,8 @@ namespace mdg {
 // the tables flattened in the oracle's export order (for the bitwise check).
 void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out);
 
+struct BrennerTables;
+// Brenner H_CC / H_CH / F tables of parameter set 1 or 2, same layout rules.
+void build_brenner_tables(int set, BrennerTables* tb, std::vector<double>* flat_out);
+
 }  // namespace mdg

@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libmdtkref.so")
+RS_PATH = os.path.join(HERE, "_ref", "librestate.so")
 
 POT_REBO = 1
 POT_AIREBO_LJ = 2
@@ -160,3 +161,63 @@ def spline_eval(fn: int, x: np.ndarray) -> np.ndarray:
     out = np.zeros(len(x))
     _check(lib().ref_spline_eval(fn, len(x), _dp(x), _dp(out)))
     return out
+
+
+# ---------------------------------------------------------------- restatement
+_rs = None
+
+
+def restatement_available() -> bool:
+    return os.path.exists(RS_PATH)
+
+
+def rs_lib():
+    global _rs
+    if _rs is None:
+        if not restatement_available():
+            raise RuntimeError(f"restatement library missing: {RS_PATH} (run `make -C oracle restate`)")
+        L = ctypes.CDLL(RS_PATH)
+        ip, dp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.rs_energy.argtypes = [ctypes.c_int] * 4 + [ip, dp, dp, ip, dp]
+        L.rs_energy_dir.argtypes = [ctypes.c_int] * 4 + [ip, dp, dp, dp, ip, dp]
+        L.rs_opcount.argtypes = [ctypes.c_int] * 3 + [ip, dp, dp, ip, ctypes.POINTER(ctypes.c_long)]
+        _rs = L
+    return _rs
+
+
+def _sys_args(s):
+    z = np.ascontiguousarray(s["z"], dtype=np.int32)
+    pos = np.ascontiguousarray(s["pos"], dtype=np.float64)
+    box = np.ascontiguousarray(s["box"], dtype=np.float64)
+    pbc = np.ascontiguousarray(s["pbc"], dtype=np.int32)
+    return z, pos, box, pbc
+
+
+def rs_energy(s, potset, brenner_set=1, lj_cut_mode=0) -> np.ndarray:
+    """Restated energies (eV): [REBO, AIREBO LJ, torsion, Brenner]."""
+    z, pos, box, pbc = _sys_args(s)
+    out = np.zeros(4)
+    rs_lib().rs_energy(potset, brenner_set, lj_cut_mode, len(z), _ip(z), _dp(pos), _dp(box), _ip(pbc), _dp(out))
+    return out
+
+
+def rs_energy_dir(s, potset, direction, brenner_set=1, lj_cut_mode=0) -> np.ndarray:
+    """Exact directional derivatives dE/d(direction) of each term (forward-mode duals)."""
+    z, pos, box, pbc = _sys_args(s)
+    d = np.ascontiguousarray(direction, dtype=np.float64)
+    out = np.zeros(4)
+    rs_lib().rs_energy_dir(potset, brenner_set, lj_cut_mode, len(z), _ip(z), _dp(pos), _dp(d), _dp(box), _ip(pbc),
+                           _dp(out))
+    return out
+
+
+OP_NAMES = ("add", "mul", "div", "sqrt", "exp", "cos", "pow")
+
+
+def rs_opcount(s, potset, brenner_set=1) -> dict:
+    """Floating-point operations of one restated energy evaluation."""
+    z, pos, box, pbc = _sys_args(s)
+    out = np.zeros(8, dtype=np.int64)
+    rs_lib().rs_opcount(potset, brenner_set, len(z), _ip(z), _dp(pos), _dp(box), _ip(pbc),
+                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
+    return {k: int(v) for k, v in zip(OP_NAMES, out[:7])}

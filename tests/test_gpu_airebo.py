@@ -113,3 +113,15 @@ def test_record_capacity_overflow_is_reported():
     with pytest.raises(M.MdgError) as e:
         ctx.compute()
     assert e.value.code == -8
+
+
+def test_graph_replay_matches_eager_steps():
+    s = B.ethane_liquid(30, seed=39, temp_k=300.0)
+    a = _gpu(s)
+    a.run(25, 0.25, energies=False)
+    a.sync()
+    pa, va, _ = a.get_state()
+    b = _gpu(s)
+    b.run(25, 0.25, energies=True)
+    pb, vb, _ = b.get_state()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)

@@ -41,6 +41,15 @@ def test_rebo_tables_bitwise_equal_to_oracle():
     assert np.array_equal(a, b)
 
 
+@pytest.mark.skipif(not ref.available(), reason="oracle not built")
+@pytest.mark.parametrize("bset", [1, 2])
+def test_brenner_tables_bitwise_equal_to_oracle(bset):
+    a = M.debug_brenner_tables(bset)
+    b = ref.tables(1, bset)
+    assert a.shape == b.shape
+    assert np.array_equal(a, b)
+
+
 def test_default_params():
     p = M.Params()
     M.lib().mdg_default_params(ctypes.byref(p))

@@ -75,3 +75,63 @@ def test_oracle_run_conserves_energy():
     et = out["etot"]
     assert np.all(np.isfinite(et))
     assert np.ptp(et) / len(s["z"]) < 2e-4  # eV/atom
+
+
+# ---------------------------------------------------------------- restatement
+RS_CASES = {
+    "c2h6": lambda: B.c2h6_example(),
+    "diamond3_disp": lambda: B.diamond(3, disp_sigma=0.15, seed=61),
+    "ach250": lambda: B.amorphous_carbon(250, h_fraction=0.3, seed=62),
+    "ethane30": lambda: B.ethane_liquid(30, seed=63, min_dist=1.6, jitter=0.4),
+}
+RS_POTS = {"rebo": (ref.POT_REBO, 0), "tors": (ref.POT_REBO | ref.POT_ETORS, None),
+           "brenner": (ref.POT_BRENNER, 3), "airebo": (ref.POT_AIREBO, None)}
+
+
+def _oracle_eg(s, pot):
+    r = ref.RefSystem(pot)
+    r.set_atoms(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    return r.compute()
+
+
+@pytest.mark.skipif(not ref.restatement_available(), reason="restatement not built")
+@pytest.mark.parametrize("pot", sorted(RS_POTS))
+@pytest.mark.parametrize("name", sorted(RS_CASES))
+def test_restatement_energy_matches_reference(name, pot):
+    s = RS_CASES[name]()
+    if pot == "airebo" and s["pbc"][0] and s["box"][0] < 11.1:
+        pytest.skip("box below twice the LJ cutoff")
+    bits = RS_POTS[pot][0]
+    e = ref.rs_energy(s, bits).sum()
+    eo, _, _ = _oracle_eg(s, bits)
+    # the reference's spline coefficients carry ~1e-11 of LU noise; the
+    # restatement evaluates the exact Hermite interpolants
+    assert abs(e - eo) <= 5e-11 * max(abs(eo), 1.0) + 1e-10
+
+
+@pytest.mark.skipif(not ref.restatement_available(), reason="restatement not built")
+@pytest.mark.parametrize("pot", ["rebo", "brenner"])
+@pytest.mark.parametrize("name", sorted(RS_CASES))
+def test_reference_adjoint_is_exact_gradient(name, pot):
+    # forward-mode derivatives of the restated energy equal the reference's
+    # hand-written gradient for REBO and Brenner
+    s = RS_CASES[name]()
+    bits = RS_POTS[pot][0]
+    _, _, go = _oracle_eg(s, bits)
+    rng = np.random.default_rng(7)
+    for _ in range(2):
+        d = rng.normal(size=s["pos"].shape)
+        dd = ref.rs_energy_dir(s, bits, d).sum()
+        assert abs(dd - np.sum(go * d)) <= 1e-9 * np.linalg.norm(go) * np.linalg.norm(d) + 1e-12
+
+
+@pytest.mark.skipif(not ref.restatement_available(), reason="restatement not built")
+def test_reference_torsion_force_is_not_the_energy_gradient():
+    # AIREBO_ETors.cxx:110 differentiates ((1+cos w)/2)^5 without the factor 5;
+    # the restatement's exact derivative exposes the difference
+    s = RS_CASES["diamond3_disp"]()
+    bits = ref.POT_REBO | ref.POT_ETORS
+    _, _, go = _oracle_eg(s, bits)
+    d = np.random.default_rng(8).normal(size=s["pos"].shape)
+    dd = ref.rs_energy_dir(s, bits, d).sum()
+    assert abs(dd - np.sum(go * d)) > 1e-6 * np.linalg.norm(go) * np.linalg.norm(d)
