@@ -233,6 +233,8 @@ def main():
 
     # roofline of the dominant kernel: FP64-pipe bound (bond-order / LJ arithmetic)
     fp64_peak = M.pipe_peak(local, fp32=False)
+    top = max((k for k in kern if k in FLOPS_PER_ATOM),
+              key=lambda k: kern[k]["ms_per_launch"] * kern[k]["launches"], default=top)
     flops_per_atom = FLOPS_PER_ATOM.get(top)
     roof = None
     if flops_per_atom:
@@ -240,7 +242,10 @@ def main():
         roof = {"kernel": top, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak, "traffic": TRAFFIC_PER_LAUNCH.get(top),
                 "peak_source": "measured FP64 FMA probe (mdg_pipe_peak) on this GPU",
-                "flops_per_atom": flops_per_atom}
+                "flops_per_atom": flops_per_atom,
+                "step": {"flops_per_atom": STEP_FLOPS_PER_ATOM,
+                         "achieved": STEP_FLOPS_PER_ATOM * n / (total_ms / args.steps * 1e-3) / 1e12,
+                         "frac": STEP_FLOPS_PER_ATOM * n / (total_ms / args.steps * 1e-3) / 1e12 / fp64_peak}}
 
     # end to end through the C ABI with host buffers (pinned), one step per call
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -291,11 +296,16 @@ def main():
 
 
 # Algorithmic FP64 flops per atom for one launch of each kernel on this
-# workload, from the op-counting restatement (oracle/opcount); filled in by
-# that measurement.
-FLOPS_PER_ATOM = {}
-# dram read+write bytes per launch from an ncu capture (profiles/), or None.
-TRAFFIC_PER_LAUNCH = {}
+# workload (ethane liquid, 43,688 atoms, step-0 state, seed 1), from the
+# op-counting restatement: `python oracle/opcount.py` (add/mul 1, div/sqrt 4,
+# exp/cos 12, pow 24; energy + gradient = 3 x energy).  rebo_tors = REBO +
+# torsion terms; lj_plain = the LJ pair terms (V_LJ, switches, C_ij path
+# products); lj_special = the b*_ij bond orders of close non-bonded pairs.
+FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_plain": 5151.5, "lj_special": 5205.5}
+STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
+# dram read+write bytes per launch from an ncu capture of the same workload
+# (profiles/hot_kernels_airebo_ethane43688_fp64.md), or None.
+TRAFFIC_PER_LAUNCH = {"rebo_tors": 21.66e6, "lj_plain": 47.39e6, "lj_special": 25.20e6, "lj_reduce": 35.44e6}
 
 
 if __name__ == "__main__":

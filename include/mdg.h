@@ -67,13 +67,16 @@ typedef struct mdg_params {
   double nl_skin;     /* absolute skin in Angstrom for nl_skin_mode 1 */
   int cap_rebo_list;  /* Verlet-list capacities (partners per atom); 0 = default */
   int cap_lj_list;
-  int cap_bonds;      /* REBO bonds per atom; 0 = default (48) */
+  int cap_bonds;      /* REBO bonds per atom; 0 = default (16) */
   int cap_cij;        /* connectivity targets per atom; 0 = default */
   int cap_special;    /* LJ pairs per atom that need b*_ij or a connectivity gradient;
                          0 = default (64) */
   int special_avg;    /* capacity of those pairs over the whole system, per atom on average;
                          0 = default (48) */
   int device;         /* CUDA device ordinal */
+  int bond_rec_avg;   /* capacity of the per-bond REBO records over the whole system, doubles per
+                         atom on average (a bond slot of an atom with b bonds takes 5 + 4b);
+                         0 = default (174: six bonds per atom) */
 } mdg_params;
 
 /* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */

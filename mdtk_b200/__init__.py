@@ -55,6 +55,7 @@ class Params(ctypes.Structure):
         ("cap_special", ctypes.c_int),
         ("special_avg", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("bond_rec_avg", ctypes.c_int),
     ]
 
 

@@ -153,16 +153,64 @@ __global__ void k_nl_build(State S, Grid g, NList L, const int* need, unsigned i
   if (i < S.n) nl_build_atom(S, g, L, i, status);
 }
 
-__global__ void k_bonds(State S, NList L, ReboParams P, BondBuild B, unsigned int* status)
+__global__ void k_bonds(State S, NList L, ReboParams P, BondBuild B, BondTasks K, unsigned int* status)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0 && K.ctr) K.ctr[0] = K.ctr[1] = K.ctr[2] = 0;
   if (a < S.n) bonds_atom(S, L, P, B, a, status);
 }
 
-__global__ void k_brev(BondBuild B)
+// Exclusive offset of this lane's v within a block handed out to the warp by
+// one atomicAdd on *ctr.  All 32 lanes must call it.
+__device__ unsigned long long warp_alloc(unsigned long long v, unsigned long long* ctr)
 {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a < B.n) brev_atom(B, a);
+  const int lane = threadIdx.x & 31;
+  unsigned long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  unsigned long long base = 0;
+  if (lane == 31 && x) base = atomicAdd(ctr, x);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + x - v;
+}
+
+// Reverse slots, then the REBO bond tasks of each atom: record space and the
+// task queue (C-C bonds, which carry the torsion and dihedral terms, first).
+// Positions in the queue and the record pool depend on scheduling; the values
+// written to each slot's record do not.
+__global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = a < B.n;
+  int nb = 0, ncc = 0;
+  if (ok) {
+    brev_atom(B, a);
+    if (K.ctr) {
+      nb = B.nb[a];
+      if ((int)B.nco[a].w == kC)
+        for (int s = 0; s < nb; s++) ncc += ((int)B.nco[B.bj[a * B.mb + s]].w == kC);
+    }
+  }
+  if (!K.ctr) return;  // uniform over the launch
+  const unsigned long long need = ok ? (unsigned long long)nb * bond_rec_size(nb) : 0ull;
+  const unsigned long long rb = warp_alloc(need, &K.ctr[2]);
+  const unsigned long long i0 = warp_alloc(ncc, &K.ctr[0]);
+  const unsigned long long i1 = warp_alloc(nb - ncc, &K.ctr[1]);
+  if (!ok) return;
+  if ((long)(rb + need) > K.rec_cap) {
+    K.rbase[a] = -1;
+    atomicOr(status, ST_RECORD_OVERFLOW);
+  } else {
+    K.rbase[a] = (long)rb;
+  }
+  int f = (int)i0, b = (int)i1;
+  for (int s = 0; s < nb; s++) {
+    const bool cc = ncc && (int)B.nco[B.bj[a * B.mb + s]].w == kC;
+    if (cc) K.q[f++] = a * B.mb + s;
+    else K.q[K.cap - 1 - (b++)] = a * B.mb + s;
+  }
 }
 
 __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, TorsParams TP, int do_rebo,
@@ -172,6 +220,87 @@ __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, Tor
   if (a >= B.n) return;
   Rebo R{*P, *T, B, status};
   rebo_atom(R, TP, do_rebo, do_tors, O, a);
+}
+
+// REBO + torsion, one thread per directed bond slot, over a grid sized to the
+// resident capacity of the GPU (grid-stride over the queue).
+__global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const ReboTables* T, BondList B,
+                                                   TorsParams TP, int do_rebo, int do_tors, BondTasks K,
+                                                   unsigned int* status)
+{
+  const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
+  Rebo R{*P, *T, B, status};
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
+    const int q = t < n0 ? K.q[t] : K.q[K.cap - 1 - (t - n0)];
+    const int a = q / B.mb, s = q - a * B.mb;
+    const long rb = K.rbase[a];
+    if (rb < 0) continue;
+    rebo_task(R, TP, do_rebo, do_tors, K.rec + rb + (long)s * bond_rec_size(B.nb[a]), a, s);
+  }
+}
+
+// Per-atom sums of the bond-task records (REBO + torsion) and the special LJ
+// records, a group of G lanes per atom.  Lane l owns elements l, l+G, ... of
+//   [g_own(3), e_rebo, e_tors, g_lj(3), e_lj, A(3 nb), W(nb)]
+// and adds each element's terms left to right: the atom's REBO slots in slot
+// order, then its LJ tasks in task order.  Without REBO tasks the REBO-side
+// elements keep what the per-atom kernels wrote; g_lj and e_lj start from the
+// plain-pair kernel's values.
+template <int G>
+__global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTasks Tk, int with_lj, ForceOut O)
+{
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = gid / G, l = gid - (gid / G) * G;
+  if (a >= B.n) return;
+  const int nb = B.nb[a];
+  const int nel = 9 + 4 * nb;
+  const long rb = rebo_tasks ? K.rbase[a] : -1;
+  const int rs = bond_rec_size(nb);
+  int t0 = 0, t1 = 0;
+  if (with_lj) {
+    t0 = Tk.off[a];
+    t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
+  }
+  for (int e = l; e < nel; e += G) {
+    int roff = -1, loff = -1;
+    double* dst;
+    if (e < 3) { roff = e; dst = reinterpret_cast<double*>(O.gown + a) + e; }
+    else if (e == 3) { roff = 3; dst = O.e_rebo + a; }
+    else if (e == 4) { roff = 4; dst = O.e_tors + a; }
+    else if (e < 8) { loff = e - 5; dst = reinterpret_cast<double*>(O.glj + a) + (e - 5); }
+    else if (e == 8) { loff = 3; dst = O.e_lj + a; }
+    else {
+      const int k = e - 9;
+      roff = 5 + k;
+      loff = 4 + k;
+      dst = k < 3 * nb ? O.A + (long)a * O.mb * 3 + k : O.W + (long)a * O.mb + (k - 3 * nb);
+    }
+    if (!rebo_tasks) roff = -1;
+    if (!with_lj) loff = -1;
+    if (roff < 0 && loff < 0) continue;
+    double acc = roff >= 0 ? 0.0 : *dst;
+    if (roff >= 0 && rb >= 0)
+      for (int s = 0; s < nb; s++) acc += K.rec[rb + (long)s * rs + roff];
+    if (loff >= 0) {
+      int t = t0;
+      for (; t + 3 < t1; t += 4) {
+        const long r0 = Tk.trec[t], r1 = Tk.trec[t + 1], r2 = Tk.trec[t + 2], r3 = Tk.trec[t + 3];
+        const double v0 = r0 >= 0 ? Tk.rec[r0 + loff] : 0.0;
+        const double v1 = r1 >= 0 ? Tk.rec[r1 + loff] : 0.0;
+        const double v2 = r2 >= 0 ? Tk.rec[r2 + loff] : 0.0;
+        const double v3_ = r3 >= 0 ? Tk.rec[r3 + loff] : 0.0;
+        if (r0 >= 0) acc += v0;
+        if (r1 >= 0) acc += v1;
+        if (r2 >= 0) acc += v2;
+        if (r3 >= 0) acc += v3_;
+      }
+      for (; t < t1; t++) {
+        const long r0 = Tk.trec[t];
+        if (r0 >= 0) acc += Tk.rec[r0 + loff];
+      }
+    }
+    *dst = acc;
+  }
 }
 
 __global__ void k_brenner(const BrennerParams* P, const BrennerTables* T, BondList B, ForceOut O,
@@ -276,6 +405,7 @@ struct ScanPair {
   int n, ntiles;
 };
 constexpr int kScanTile = 1024;
+constexpr int kReduceLanes = 8;
 
 __global__ void k_scan_tiles(ScanPair P)
 {
@@ -353,12 +483,6 @@ __global__ void k_lj_special(const ReboParams* P, const ReboTables* Tb, LJParams
   LJ X{LP, R, T};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
     lj_special_task(X, S, Tk, t, status);
-}
-
-__global__ void k_lj_reduce(BondList B, SpecialTasks Tk, ForceOut O)
-{
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a < B.n) lj_reduce_atom(B, Tk, O, a);
 }
 
 __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad)
@@ -529,6 +653,8 @@ struct mdg_ctx {
 
   CijTable cij;
   SpecialTasks spc;
+  BondTasks bt;
+  int rebo_task_blocks = 0;
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
@@ -657,7 +783,7 @@ int status_to_code(unsigned int st, std::string& msg)
   add(ST_N_NEGATIVE, MDG_ERR_N_NEGATIVE, "negative coordination;");
   add(ST_SPLINE_DOMAIN, MDG_ERR_SPLINE_DOMAIN, "spline argument out of domain;");
   add(ST_CIJ_OVERFLOW, MDG_ERR_CAPACITY, "connectivity table capacity exceeded;");
-    add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "connectivity record capacity exceeded;");
+  add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "bond or connectivity record capacity exceeded;");
   add(ST_CELL_OVERFLOW, MDG_ERR_CAPACITY, "cell grid capacity exceeded;");
   return code;
 }
@@ -688,6 +814,10 @@ void free_system(mdg_ctx* c)
     if (p) cudaFree(p);
   std::memset(&c->cij, 0, sizeof(c->cij));
   std::memset(&c->spc, 0, sizeof(c->spc));
+  void* bq[] = {c->bt.q, c->bt.ctr, c->bt.rbase, c->bt.rec};
+  for (void* p : bq)
+    if (p) cudaFree(p);
+  std::memset(&c->bt, 0, sizeof(c->bt));
   if (c->h_stage) cudaFreeHost(c->h_stage);
   c->h_stage = nullptr;
   c->pos = c->vel = c->acc = c->grad = nullptr;
@@ -787,11 +917,16 @@ int evaluate(mdg_ctx* c)
   State S = c->S();
   const int pot = c->prm.potentials;
   const bool rebo = pot & MDG_POT_REBO, tors = pot & MDG_POT_ETORS, lj = pot & MDG_POT_AIREBO_LJ;
-  LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->d_status);
-  LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb);
+  const bool tasks = c->bt.ctr != nullptr;
+  LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
+  LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
-  LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0, tors ? 1 : 0,
-         c->fo, c->d_status);
+  if (tasks)
+    LAUNCH(c, "rebo_tors", k_rebo_task, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp,
+           rebo ? 1 : 0, tors ? 1 : 0, c->bt, c->d_status);
+  else
+    LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
+           tors ? 1 : 0, c->fo, c->d_status);
   if (pot & MDG_POT_BRENNER)
     LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
@@ -813,8 +948,10 @@ int evaluate(mdg_ctx* c)
     LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, c->d_status);
     LAUNCH(c, "lj_special", k_lj_special, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
            c->spc, c->d_status);
-    LAUNCH(c, "lj_reduce", k_lj_reduce, nblk(c->n), kThreads, B, c->spc, c->fo);
   }
+  if (tasks || lj)
+    LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
+           tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
   LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
   return launch_check(c);
 }
@@ -889,6 +1026,7 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   mdg_ctx* c = new mdg_ctx();
   c->prm = *p;
   if (c->prm.cap_bonds <= 0) c->prm.cap_bonds = 16;
+  if (c->prm.bond_rec_avg <= 0) c->prm.bond_rec_avg = 6 * (5 + 4 * 6);
   if (c->prm.cap_rebo_list <= 0) c->prm.cap_rebo_list = 64;
   if (c->prm.cap_lj_list <= 0) c->prm.cap_lj_list = 512;
   if (c->prm.cap_cij <= 0) c->prm.cap_cij = 128;
@@ -1078,6 +1216,22 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
     return fail(MDG_ERR_CUDA, "cudaMalloc (bonds)");
   CK(cudaMemset(c->fo.glj, 0, n * sizeof(double4)));
   CK(cudaMemset(c->fo.e_lj, 0, n * sizeof(double)));
+  if (c->prm.potentials & (MDG_POT_REBO | MDG_POT_ETORS) && !(c->prm.potentials & MDG_POT_BRENNER)) {
+    BondTasks& K = c->bt;
+    K.cap = n * mb;
+    K.rec_cap = (long)n * c->prm.bond_rec_avg;
+    K.q = dalloc<int>((size_t)K.cap);
+    K.ctr = dalloc<unsigned long long>(4);
+    K.rbase = dalloc<long>(n);
+    K.rec = dalloc<double>((size_t)K.rec_cap);
+    if (!K.q || !K.ctr || !K.rbase || !K.rec) return fail(MDG_ERR_CUDA, "cudaMalloc (bond tasks)");
+    CK(cudaMemset(K.ctr, 0, 4 * sizeof(unsigned long long)));
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rebo_task, kThreads, 0);
+    c->rebo_task_blocks = sms * (per > 0 ? per : 1);
+  }
   if (with_lj) {
     if (c->prm.cap_cij > kCijLocal) c->prm.cap_cij = kCijLocal;
     c->cij.cap = c->prm.cap_cij;

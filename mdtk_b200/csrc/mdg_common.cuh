@@ -40,7 +40,7 @@ enum StatusBits : unsigned int {
   ST_N_NEGATIVE = 1u << 3,      // coordination below -1e-15 (REBO.cxx:434,462,489)
   ST_NONFINITE = 1u << 4,       // NaN/Inf energy or force
   ST_CIJ_OVERFLOW = 1u << 5,    // connectivity table capacity exceeded
-  ST_RECORD_OVERFLOW = 1u << 7, // connectivity middle-bond record capacity exceeded
+  ST_RECORD_OVERFLOW = 1u << 7, // bond-task or special-pair record capacity exceeded
   ST_SPLINE_DOMAIN = 1u << 8,   // spline argument outside its domain (cubici.hpp:90,211,305)
   ST_CELL_OVERFLOW = 1u << 9,   // cell grid capacity exceeded
 };

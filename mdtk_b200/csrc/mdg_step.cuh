@@ -258,6 +258,54 @@ MDG_HD void rebo_atom(const Rebo& R, const TorsParams& TP, int do_rebo, int do_t
   O.e_tors[a] = et;
 }
 
+// REBO (+ torsion) as one task per directed bond slot (a, s): the bond
+// (min, max) is evaluated in full and routed through a Sink for atom a into a
+// private record [g(3), e_rebo, e_tors, A(3 nb_a), W(nb_a)].  The records of
+// an atom's slots lie consecutively from rbase[a]; a per-atom reduction sums
+// them in slot order.  Splitting an atom's bonds over threads shortens the
+// longest serial chain from all of a carbon's bonds to one bond.
+struct BondTasks {
+  int cap;                  // queue capacity (n * mb)
+  int* q;                   // slots a*mb+s: C-C bonds from the front, the rest from the back
+  unsigned long long* ctr;  // [0] C-C tasks, [1] other tasks, [2] record doubles handed out
+  long* rbase;              // [n] first record double of atom a (-1: over capacity, flagged)
+  double* rec;
+  long rec_cap;
+};
+
+MDG_HD int bond_rec_size(int nb) { return 5 + 4 * nb; }
+
+MDG_HD void rebo_task(const Rebo& R, const TorsParams& TP, int do_rebo, int do_tors, double* rec, int a, int s)
+{
+  const BondList& B = R.B;
+  const int nb = B.nb[a];
+  Sink sink;
+  sink.a = a;
+  sink.g = v3(0, 0, 0);
+  sink.A = rec + 5;
+  sink.W = rec + 5 + 3 * nb;
+  for (int t = 0; t < 4 * nb; t++) sink.A[t] = 0.0;  // A and W are contiguous
+  const int q = a * B.mb + s;
+  const int b = B.bj[q];
+  PairG p = pair_from_slot(B, q);
+  int lo = a, hi = b;
+  if (b < a) { lo = b; hi = a; p = pair_reverse(p); }
+  double er = 0.0, et = 0.0;
+  if (do_rebo) {
+    double E = R.bond(lo, hi, p, sink);
+    if (a == lo) er = E;
+  }
+  if (do_tors) {
+    double E = etors_bond(R, TP, lo, hi, p, sink);
+    if (a == lo) et = E;
+  }
+  rec[0] = sink.g.x;
+  rec[1] = sink.g.y;
+  rec[2] = sink.g.z;
+  rec[3] = er;
+  rec[4] = et;
+}
+
 // Total dE/dx_a: own parts, what bond partners owe a, and the third-shell
 // switching derivatives (dfThem through N_conj) resolved by gathering the
 // coefficients of the bonds around a and around each switching partner.

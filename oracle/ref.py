@@ -214,10 +214,12 @@ def rs_energy_dir(s, potset, direction, brenner_set=1, lj_cut_mode=0) -> np.ndar
 OP_NAMES = ("add", "mul", "div", "sqrt", "exp", "cos", "pow")
 
 
-def rs_opcount(s, potset, brenner_set=1) -> dict:
-    """Floating-point operations of one restated energy evaluation."""
+def rs_opcount(s, potset, brenner_set=1, bstar=False) -> dict:
+    """Floating-point operations of one restated energy evaluation (with
+    bstar=True: only those spent in the LJ term's b*_ij evaluations)."""
     z, pos, box, pbc = _sys_args(s)
-    out = np.zeros(8, dtype=np.int64)
+    out = np.zeros(16, dtype=np.int64)
     rs_lib().rs_opcount(potset, brenner_set, len(z), _ip(z), _dp(pos), _dp(box), _ip(pbc),
                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
-    return {k: int(v) for k, v in zip(OP_NAMES, out[:7])}
+    o = out[8:15] if bstar else out[:7]
+    return {k: int(v) for k, v in zip(OP_NAMES, o)}

@@ -475,7 +475,9 @@ struct Eval {
         T Str = Slj(rr, P.RLJ[ti][tj][0], P.RLJ[ti][tj][1]);
         T SrSb = 1.0;
         if (val(Str) != 0.0) {
+          tally_bucket() = 1;
           T b = bbar(i, j, T(P.R[ti][tj][0]));
+          tally_bucket() = 0;
           SrSb = 1.0 - Str + Str * Slj(b, P.bw[ti][tj][0], P.bw[ti][tj][1]);
         }
         T s6 = pow(P.sigma[ti][tj] / rr, 6.0);
@@ -685,7 +687,8 @@ int rs_energy_dir(int potset, int brenner_set, int lj_cut_mode, int n, const int
 }
 
 /* Operation counts of one energy evaluation of the selected terms:
- * out[8] = add/sub, mul, div, sqrt, exp, cos, pow, (unused). */
+ * out[0..7] = add/sub, mul, div, sqrt, exp, cos, pow, (unused) over the whole
+ * evaluation; out[8..15] the same for the part spent in the LJ term's b*_ij. */
 int rs_opcount(int potset, int brenner_set, int n, const int* z, const double* pos, const double* box,
                const int* pbc, long* out)
 {
@@ -694,13 +697,21 @@ int rs_opcount(int potset, int brenner_set, int n, const int* z, const double* p
   std::vector<V3<Counted>> x(n);
   for (int i = 0; i < n; i++) x[i] = {Counted(p[3 * i]), Counted(p[3 * i + 1]), Counted(p[3 * i + 2])};
   Params P(0);
-  tally() = OpTally();
+  for (int b = 1; b >= 0; b--) { tally_bucket() = b; tally() = OpTally(); }
   Eval<Counted> E(s, x, P, brenner_set, (potset & 2) != 0);
   Counted t[4];
   terms(E, potset, t);
-  OpTally& c = tally();
-  out[0] = c.add; out[1] = c.mul; out[2] = c.div; out[3] = c.sqrt_;
-  out[4] = c.exp_; out[5] = c.cos_; out[6] = c.pow_; out[7] = 0;
+  for (int b = 0; b < 2; b++) {
+    tally_bucket() = 1;
+    const OpTally c1 = tally();
+    tally_bucket() = 0;
+    const OpTally c = b == 0 ? tally() : c1;
+    long* o = out + 8 * b;
+    o[0] = c.add + (b == 0 ? c1.add : 0); o[1] = c.mul + (b == 0 ? c1.mul : 0);
+    o[2] = c.div + (b == 0 ? c1.div : 0); o[3] = c.sqrt_ + (b == 0 ? c1.sqrt_ : 0);
+    o[4] = c.exp_ + (b == 0 ? c1.exp_ : 0); o[5] = c.cos_ + (b == 0 ? c1.cos_ : 0);
+    o[6] = c.pow_ + (b == 0 ? c1.pow_ : 0); o[7] = 0;
+  }
   return 0;
 }
 

@@ -58,7 +58,10 @@ template <int N> inline Dual<N> fabs(const Dual<N>& a) { return a.v < 0 ? -a : a
 struct OpTally {
   long add = 0, mul = 0, div = 0, sqrt_ = 0, exp_ = 0, cos_ = 0, pow_ = 0, cmp = 0;
 };
-inline OpTally& tally() { static OpTally t; return t; }
+// Two buckets: 0 = everything else, 1 = the REBO bond order b*_ij that the
+// LJ term evaluates for close non-bonded pairs (AIREBO_LJ.cxx:191-202).
+inline int& tally_bucket() { static int b = 0; return b; }
+inline OpTally& tally() { static OpTally t[2]; return t[tally_bucket()]; }
 struct Counted {
   double v;
   Counted(double x = 0.0) : v(x) {}
