@@ -138,6 +138,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -267,6 +268,44 @@ def main():
            "h2d_bytes_per_step": 2 * 32 * n, "d2h_bytes_per_step": 2 * 32 * n + 16,
            "steps": args.e2e_steps, "timer": "host wall clock around mdg_step_host calls (each ends synchronised)"}
 
+    # FP32-mixed variant on the same workload, from the FP64 run's final state:
+    # device time per step (same protocol) and its force error against the
+    # FP64 path at that state
+    mixed = None
+    if not args.no_variants:
+        p1, v1, _ = ctx.get_state()
+        _, _, g64 = ctx.compute()
+        mx = M.Context(potentials=M.POT_AIREBO, precision=M.PREC_FP32_MIXED, device=local)
+        mx.set_system(s["z"], p1, v1, s["box"], s["pbc"], s["fixed"])
+        mx.set_stream(stream.cuda_stream)
+        _, _, g32 = mx.compute()
+        d = g32 - g64
+        rel = float(np.linalg.norm(d) / np.linalg.norm(g64))
+        maxrms = float(np.abs(d).max() / np.sqrt((g64 ** 2).mean()))
+        mx.run(max(args.warmup, 3), DT_FS, energies=False)
+        mx.sync()
+        kmix = min(args.steps, 200)
+        evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kmix)]
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(kmix):
+            flush.zero_()
+            evm[k][0].record(stream)
+            mx.run(1, DT_FS, energies=False)
+            evm[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        mix_ms = sum(a.elapsed_time(b) for a, b in evm)
+        if dist is not None:
+            t = torch.tensor([mix_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mix_ms = float(t.item())
+        mixed = {"value": world * n * kmix / (mix_ms * 1e-3), "unit": "atom-steps/s", "steps": kmix,
+                 "ms_per_step": mix_ms / kmix,
+                 "force_err_vs_fp64": {"norm_rel": rel, "max_abs_over_rms": maxrms},
+                 "scope": "FP32 bond orders (REBO, torsion) and plain LJ pairs; FP64 pair exponentials, LJ "
+                          "powers and switches, b* of close non-bonded pairs, accumulation, integration"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
@@ -277,6 +316,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches, "clocks": clk, "kernels": kern, "roofline": roof, "e2e": e2e,
             "fp64_peak_tflops": fp64_peak,
+            "variants": {"fp32_mixed": mixed},
         }
         if world == 1 and not args.no_cpu_baseline:
             try:

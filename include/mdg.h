@@ -194,6 +194,13 @@ int64_t mdg_debug_rebo_tables(double* out, int64_t cap);
  * the oracle's export order.  Host only. */
 int64_t mdg_debug_brenner_tables(int set, double* out, int64_t cap);
 
+/* Host evaluation of one REBO spline family in the given precision's tables
+ * (test support): kind 0 = G (fam 0..2 = G_C1, G_C2, G_H; args cos theta;
+ * out value, d/dcos), 1 = P (fam 0..1 = CC, CH; args (N^H, N^C); out value,
+ * d/dN^H, d/dN^C), 2 = pi_rc / T_ij (fam 0..3 = CC, CH, HH, Tij; args
+ * (N_ij, N_ji, N_conj); out value and the three partials). */
+int mdg_debug_spline(int precision, int kind, int fam, int n, const double* args, double* out);
+
 #ifdef __cplusplus
 }
 #endif

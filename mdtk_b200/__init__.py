@@ -93,6 +93,7 @@ def lib():
         L.mdg_pipe_peak.argtypes = [ctypes.c_int, ctypes.c_int, dp]
         L.mdg_debug_brenner_tables.argtypes = [ctypes.c_int, dp, ctypes.c_int64]
         L.mdg_debug_brenner_tables.restype = ctypes.c_int64
+        L.mdg_debug_spline.argtypes = [ctypes.c_int] * 4 + [dp, dp]
         L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
         L.mdg_debug_rebo_tables.restype = ctypes.c_int64
         _lib = L
@@ -123,6 +124,15 @@ def debug_brenner_tables(set_: int) -> np.ndarray:
     n = lib().mdg_debug_brenner_tables(set_, None, 0)
     out = np.zeros(n)
     lib().mdg_debug_brenner_tables(set_, _dp(out), n)
+    return out
+
+
+def debug_spline(precision: int, kind: int, fam: int, args) -> np.ndarray:
+    """Host evaluation of a REBO spline family (kind 0 = G, 1 = P, 2 = pi_rc/T)."""
+    nin, nout = {0: (1, 2), 1: (2, 3), 2: (3, 4)}[kind]
+    a = np.ascontiguousarray(np.asarray(args, dtype=np.float64).reshape(-1, nin))
+    out = np.zeros((a.shape[0], nout))
+    _check(lib().mdg_debug_spline(precision, kind, fam, a.shape[0], _dp(a), _dp(out)))
     return out
 
 

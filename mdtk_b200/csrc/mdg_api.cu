@@ -224,12 +224,12 @@ __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, Tor
 
 // REBO + torsion, one thread per directed bond slot, over a grid sized to the
 // resident capacity of the GPU (grid-stride over the queue).
-__global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const ReboTables* T, BondList B,
-                                                   TorsParams TP, int do_rebo, int do_tors, BondTasks K,
-                                                   unsigned int* status)
+template <class Real, class TB>
+__global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const TB* T, BondList B, TorsParams TP,
+                                                   int do_rebo, int do_tors, BondTasks K, unsigned int* status)
 {
   const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
-  Rebo R{*P, *T, B, status};
+  ReboT<Real, TB> R{*P, *T, B, status};
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
     const int q = t < n0 ? K.q[t] : K.q[K.cap - 1 - (t - n0)];
     const int a = q / B.mb, s = q - a * B.mb;
@@ -323,6 +323,7 @@ __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
 // Plain LJ pairs, one warp per atom: lanes stride the atom's LJ list;
 // pairs that need b*_ij or a connectivity gradient are compacted, in list
 // order, into the atom's special list.
+template <class Real>
 __global__ void k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* nbonds, ForceOut O,
                            SpecialTasks Tk, unsigned int* status)
 {
@@ -334,7 +335,7 @@ __global__ void k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* 
   const int ta = (int)pa.w;
   const int cnt = L.cnt[a];
   const int* lst = L.list + (long)a * L.cap;
-  Sink sk;
+  SinkT<Real> sk;
   sk.a = a;
   sk.g = v3(0, 0, 0);
   sk.A = nullptr;
@@ -346,7 +347,7 @@ __global__ void k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* 
     int kind = 0, b = -1;
     if (s < cnt) {
       b = lst[s];
-      kind = lj_plain_pair(P, T, S, a, b, xa, ta, sk, e);
+      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
     }
     const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
     if (kind == 2) {
@@ -475,12 +476,13 @@ __global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, unsigne
 }
 
 // Special LJ pairs, one thread per (atom, pair) task.
-__global__ void k_lj_special(const ReboParams* P, const ReboTables* Tb, LJParams LP, BondList B, CijTable T,
-                             State S, SpecialTasks Tk, unsigned int* status)
+template <class Real, class TB>
+__global__ void k_lj_special(const ReboParams* P, const TB* Tb, LJParams LP, BondList B, CijTable T, State S,
+                             SpecialTasks Tk, unsigned int* status)
 {
   const int total = min(Tk.off[S.n], Tk.task_cap);
-  Rebo R{*P, *Tb, B, status};
-  LJ X{LP, R, T};
+  ReboT<Real, TB> R{*P, *Tb, B, status};
+  LJT<Real, TB> X{LP, R, T};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
     lj_special_task(X, S, Tk, t, status);
 }
@@ -614,6 +616,7 @@ struct mdg_ctx {
   TorsParams tp;
   LJParams ljp;
   ReboTables* d_tables = nullptr;
+  ReboTables32* d_tables32 = nullptr;  // FP32-mixed path only
   ReboParams* d_rp = nullptr;
   BrennerTables* d_btables = nullptr;
   BrennerParams* d_bp = nullptr;
@@ -921,9 +924,16 @@ int evaluate(mdg_ctx* c)
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
   LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
-  if (tasks)
-    LAUNCH(c, "rebo_tors", k_rebo_task, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp,
-           rebo ? 1 : 0, tors ? 1 : 0, c->bt, c->d_status);
+  const bool f32p = c->prm.precision == MDG_PREC_FP32_MIXED;
+  if (tasks && f32p) {
+    auto kern = k_rebo_task<f32, ReboTables32>;
+    LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, rebo ? 1 : 0,
+           tors ? 1 : 0, c->bt, c->d_status);
+  } else if (tasks) {
+    auto kern = k_rebo_task<double, ReboTables>;
+    LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
+           tors ? 1 : 0, c->bt, c->d_status);
+  }
   else
     LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
            tors ? 1 : 0, c->fo, c->d_status);
@@ -931,8 +941,12 @@ int evaluate(mdg_ctx* c)
     LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
     LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
-    LAUNCH(c, "lj_plain", k_lj_plain, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb, c->fo,
-           c->spc, c->d_status);
+    if (f32p)
+      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb,
+             c->fo, c->spc, c->d_status);
+    else
+      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb,
+             c->fo, c->spc, c->d_status);
     ScanPair sp;
     sp.in[0] = c->spc.cnt;
     sp.in[1] = c->spc.rsz;
@@ -946,8 +960,14 @@ int evaluate(mdg_ctx* c)
     LAUNCH(c, "lj_scan_top", k_scan_top, dim3(1, 2), 32, sp);
     LAUNCH(c, "lj_scan_add", k_scan_add, dim3(sp.ntiles, 2), kScanTile, sp);
     LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, c->d_status);
-    LAUNCH(c, "lj_special", k_lj_special, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
-           c->spc, c->d_status);
+    // b*_ij of close non-bonded pairs stays FP64 in the mixed mode too: the
+    // S(t_b) window (0.04 wide for C-C) multiplies an error of b* by up to
+    // 1/0.04^2 in the pair force, beyond what float b* can carry.
+    {
+      auto kern = k_lj_special<double, ReboTables>;
+      LAUNCH(c, "lj_special", kern, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
+             c->spc, c->d_status);
+    }
   }
   if (tasks || lj)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
@@ -1019,7 +1039,10 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
     return fail(MDG_ERR_ARG, "Brenner parameter set must be 1 or 2");
   if (!(p->potentials & (MDG_POT_REBO | MDG_POT_BRENNER | MDG_POT_ETORS)))
     return fail(MDG_ERR_ARG, "no potential selected");
-  if (p->precision != MDG_PREC_FP64) return fail(MDG_ERR_ARG, "only FP64 precision is available in this build");
+  if (p->precision != MDG_PREC_FP64 && p->precision != MDG_PREC_FP32_MIXED)
+    return fail(MDG_ERR_ARG, "unknown precision mode");
+  if (p->precision == MDG_PREC_FP32_MIXED && (p->potentials & MDG_POT_BRENNER))
+    return fail(MDG_ERR_ARG, "the FP32-mixed mode covers REBO, the LJ term and torsion; Brenner is FP64 only");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(MDG_ERR_CUDA, "no CUDA device");
   CK(cudaSetDevice(p->device));
@@ -1049,6 +1072,14 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   if (!c->d_tables || !c->d_rp) { delete h; mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc (tables)"); }
   cudaMemcpy(c->d_tables, h, sizeof(ReboTables), cudaMemcpyHostToDevice);
   cudaMemcpy(c->d_rp, &c->rp, sizeof(ReboParams), cudaMemcpyHostToDevice);
+  if (p->precision == MDG_PREC_FP32_MIXED) {
+    ReboTables32* h32 = new ReboTables32();
+    build_rebo_tables32(*h, h32);
+    c->d_tables32 = dalloc<ReboTables32>(1);
+    if (!c->d_tables32) { delete h; delete h32; mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc (tables)"); }
+    cudaMemcpy(c->d_tables32, h32, sizeof(ReboTables32), cudaMemcpyHostToDevice);
+    delete h32;
+  }
   delete h;
   if (p->potentials & MDG_POT_BRENNER) {
     BrennerTables* bt = new BrennerTables();
@@ -1085,7 +1116,7 @@ int mdg_destroy(mdg_ctx* c)
   if (!c) return MDG_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_system(c);
-  void* ptrs[] = {c->d_tables, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy};
+  void* ptrs[] = {c->d_tables, c->d_tables32, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -1229,7 +1260,10 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
     int dev = 0, sms = 148, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rebo_task, kThreads, 0);
+    if (c->prm.precision == MDG_PREC_FP32_MIXED)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rebo_task<f32, ReboTables32>, kThreads, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rebo_task<double, ReboTables>, kThreads, 0);
     c->rebo_task_blocks = sms * (per > 0 ? per : 1);
   }
   if (with_lj) {
@@ -1589,6 +1623,52 @@ int64_t mdg_debug_rebo_tables(double* out, int64_t cap)
   delete h;
   for (int64_t i = 0; i < (int64_t)flat.size() && i < cap; i++) out[i] = flat[i];
   return (int64_t)flat.size();
+}
+
+int mdg_debug_spline(int precision, int kind, int fam, int n, const double* args, double* out)
+{
+  if (!args || !out || n < 0 || kind < 0 || kind > 2) return fail(MDG_ERR_ARG, "bad spline query");
+  if ((kind == 0 && (fam < 0 || fam > 2)) || (kind == 1 && (fam < 0 || fam > 1)) ||
+      (kind == 2 && (fam < 0 || fam > 3)))
+    return fail(MDG_ERR_ARG, "bad spline family");
+  ReboTables* d = new ReboTables();
+  build_rebo_tables(d, nullptr);
+  ReboTables32* f = nullptr;
+  if (precision == MDG_PREC_FP32_MIXED) {
+    f = new ReboTables32();
+    build_rebo_tables32(*d, f);
+  }
+  unsigned int st = 0;
+  for (int q = 0; q < n; q++) {
+    if (kind == 0) {
+      if (f) {
+        out[2 * q] = dbl(g_eval(f->G[fam], f32(args[q]), 0));
+        out[2 * q + 1] = dbl(g_eval(f->G[fam], f32(args[q]), 1));
+      } else {
+        out[2 * q] = g_eval(d->G[fam], args[q], 0);
+        out[2 * q + 1] = g_eval(d->G[fam], args[q], 1);
+      }
+    } else if (kind == 1) {
+      if (f) {
+        f32 v, dh, dc;
+        p_eval(*f, fam, f32(args[2 * q]), f32(args[2 * q + 1]), v, dh, dc, &st);
+        out[3 * q] = dbl(v); out[3 * q + 1] = dbl(dh); out[3 * q + 2] = dbl(dc);
+      } else {
+        p_eval(*d, fam, args[2 * q], args[2 * q + 1], out[3 * q], out[3 * q + 1], out[3 * q + 2], &st);
+      }
+    } else {
+      if (f) {
+        f32 r[4];
+        t_eval(*f, fam, f32(args[3 * q]), f32(args[3 * q + 1]), f32(args[3 * q + 2]), r, &st);
+        for (int t = 0; t < 4; t++) out[4 * q + t] = dbl(r[t]);
+      } else {
+        t_eval(*d, fam, args[3 * q], args[3 * q + 1], args[3 * q + 2], out + 4 * q, &st);
+      }
+    }
+  }
+  delete d;
+  delete f;
+  return MDG_OK;
 }
 
 }  // extern "C"

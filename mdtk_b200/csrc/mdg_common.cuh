@@ -45,23 +45,90 @@ enum StatusBits : unsigned int {
   ST_CELL_OVERFLOW = 1u << 9,   // cell grid capacity exceeded
 };
 
-struct V3 {
-  double x, y, z;
+// FP32 scalar of the mixed-precision path: float arithmetic; double operands
+// (parameters, literals, loads from the FP64 bond list) convert to float
+// implicitly, conversion back to double is explicit (dbl()).
+struct f32 {
+  float v;
+  f32() = default;
+  MDG_HD f32(double x) : v((float)x) {}
+  MDG_HD explicit operator double() const { return (double)v; }
+  // Math functions as hidden friends: found only through an f32 argument, so
+  // they never hide the double functions for FP64 code in this namespace.
+  friend MDG_HD f32 exp(f32 a) { f32 r; r.v = expf(a.v); return r; }
+  friend MDG_HD f32 sqrt(f32 a) { f32 r; r.v = sqrtf(a.v); return r; }
+  friend MDG_HD f32 cos(f32 a) { f32 r; r.v = cosf(a.v); return r; }
+  friend MDG_HD f32 sin(f32 a) { f32 r; r.v = sinf(a.v); return r; }
+  friend MDG_HD f32 fabs(f32 a) { f32 r; r.v = fabsf(a.v); return r; }
+  friend MDG_HD f32 pow(f32 a, f32 b) { f32 r; r.v = powf(a.v, b.v); return r; }
 };
+MDG_HD f32 mkf(float x) { f32 r; r.v = x; return r; }
+MDG_HD f32 operator+(f32 a, f32 b) { return mkf(a.v + b.v); }
+MDG_HD f32 operator-(f32 a, f32 b) { return mkf(a.v - b.v); }
+MDG_HD f32 operator*(f32 a, f32 b) { return mkf(a.v * b.v); }
+MDG_HD f32 operator/(f32 a, f32 b) { return mkf(a.v / b.v); }
+MDG_HD f32 operator-(f32 a) { return mkf(-a.v); }
+MDG_HD f32& operator+=(f32& a, f32 b) { a.v += b.v; return a; }
+MDG_HD f32& operator-=(f32& a, f32 b) { a.v -= b.v; return a; }
+MDG_HD f32& operator*=(f32& a, f32 b) { a.v *= b.v; return a; }
+MDG_HD bool operator<(f32 a, f32 b) { return a.v < b.v; }
+MDG_HD bool operator>(f32 a, f32 b) { return a.v > b.v; }
+MDG_HD bool operator<=(f32 a, f32 b) { return a.v <= b.v; }
+MDG_HD bool operator>=(f32 a, f32 b) { return a.v >= b.v; }
+MDG_HD bool operator==(f32 a, f32 b) { return a.v == b.v; }
+MDG_HD bool operator!=(f32 a, f32 b) { return a.v != b.v; }
+MDG_HD double dbl(double x) { return x; }
+// Slack of the reference's coordination check N > -1e-15 (REBO.cxx:434): in
+// float, N = N_t - f rounds to about -5e-7 where it is 0.
+MDG_HD double n_neg_tol(double) { return 1e-15; }
+MDG_HD double n_neg_tol(f32) { return 1e-5; }
+MDG_HD double dbl(f32 x) { return (double)x.v; }
+
+template <class T> struct Id { typedef T type; };
+
+template <class Real>
+struct V3T {
+  Real x, y, z;
+};
+typedef V3T<double> V3;
 MDG_HD V3 v3(double x, double y, double z) { V3 r; r.x = x; r.y = y; r.z = z; return r; }
-MDG_HD V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-MDG_HD V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-MDG_HD V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
-MDG_HD V3 operator*(V3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
-MDG_HD V3 operator*(double s, V3 a) { return v3(a.x * s, a.y * s, a.z * s); }
-MDG_HD V3 operator/(V3 a, double s) { return v3(a.x / s, a.y / s, a.z / s); }
-MDG_HD void operator+=(V3& a, V3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
-MDG_HD void operator-=(V3& a, V3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
+template <class Real>
+MDG_HD V3T<Real> v3r(Real x, Real y, Real z) { V3T<Real> r; r.x = x; r.y = y; r.z = z; return r; }
+// xyz of a double4 in the arithmetic type Real
+template <class Real>
+MDG_HD V3T<Real> xyz(double4 q) { return v3r<Real>(Real(q.x), Real(q.y), Real(q.z)); }
+template <class Real>
+MDG_HD V3T<Real> cvt3(V3 a) { return v3r<Real>(Real(a.x), Real(a.y), Real(a.z)); }
+template <class Real>
+MDG_HD V3 to_d(V3T<Real> a) { return v3(dbl(a.x), dbl(a.y), dbl(a.z)); }
+template <class Real>
+MDG_HD V3T<Real> operator+(V3T<Real> a, V3T<Real> b) { return v3r<Real>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class Real>
+MDG_HD V3T<Real> operator-(V3T<Real> a, V3T<Real> b) { return v3r<Real>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class Real>
+MDG_HD V3T<Real> operator-(V3T<Real> a) { return v3r<Real>(-a.x, -a.y, -a.z); }
+template <class Real>
+MDG_HD V3T<Real> operator*(V3T<Real> a, typename Id<Real>::type s) { return v3r<Real>(a.x * s, a.y * s, a.z * s); }
+template <class Real>
+MDG_HD V3T<Real> operator*(typename Id<Real>::type s, V3T<Real> a) { return v3r<Real>(a.x * s, a.y * s, a.z * s); }
+template <class Real>
+MDG_HD V3T<Real> operator/(V3T<Real> a, typename Id<Real>::type s) { return v3r<Real>(a.x / s, a.y / s, a.z / s); }
+template <class Real>
+MDG_HD void operator+=(V3T<Real>& a, V3T<Real> b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+template <class Real>
+MDG_HD void operator-=(V3T<Real>& a, V3T<Real> b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
 // same evaluation order as mdtk Vector3D scalarmul/vectormul (Vector3D.hpp:272-282)
-MDG_HD double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-MDG_HD V3 cross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-MDG_HD double norm2(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
-MDG_HD double SQR(double x) { return x * x; }
+template <class Real>
+MDG_HD Real dot(V3T<Real> a, V3T<Real> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class Real>
+MDG_HD V3T<Real> cross(V3T<Real> a, V3T<Real> b)
+{
+  return v3r<Real>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class Real>
+MDG_HD Real norm2(V3T<Real> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+template <class Real>
+MDG_HD Real SQR(Real x) { return x * x; }
 
 // Periodic box: only uniform per-axis periodicity (every atom shares the
 // array's PBC, as AtomsArray::PBC sets it, mdtk/AtomsContainer.cxx:43-54).
@@ -87,7 +154,8 @@ MDG_HD V3 depos(const Box& b, V3 a1, V3 a2)
 
 // Cosine cutoff of AtomsPair (AtomsPair.hpp:137-158): f = 1 below R1,
 // (1 + cos(pi (r-R1)/(R2-R1)))/2 on [R1, R2), 0 beyond; df = df/dr.
-MDG_HD void cutoff(double r, double R1, double R2, double& f, double& df)
+template <class Real>
+MDG_HD void cutoff(Real r, double R1, double R2, Real& f, Real& df)
 {
   if (r < R1) { f = 1.0; df = 0.0; return; }
   if (r < R2) {
@@ -100,13 +168,15 @@ MDG_HD void cutoff(double r, double R1, double R2, double& f, double& df)
 }
 
 // Sprime / dSprime (REBO.cxx:67-106): 1 below min, 0 above max, cosine between.
-MDG_HD double Sprime(double arg, double amin, double amax)
+template <class Real>
+MDG_HD Real Sprime(Real arg, double amin, double amax)
 {
   if (arg < amin) return 1.0;
   if (arg > amax) return 0.0;
   return (1.0 + cos(kPi * (arg - amin) / (amax - amin))) / 2.0;
 }
-MDG_HD double dSprime(double arg, double amin, double amax)
+template <class Real>
+MDG_HD Real dSprime(Real arg, double amin, double amax)
 {
   if (arg < amin) return 0.0;
   if (arg > amax) return 0.0;

@@ -12,62 +12,63 @@
 
 namespace mdg {
 
-template <class S>
-MDG_HD double etors_bond(const Rebo& R, const TorsParams& TP, int i, int j, const PairG& p, S& sink)
+template <class Real, class TB, class S>
+MDG_HD Real etors_bond(const ReboT<Real, TB>& R, const TorsParams& TP, int i, int j, const PairGT<Real>& p,
+                        S& sink)
 {
   if (R.type(i) != kC || R.type(j) != kC) return 0.0;
   const BondList& B = R.B;
-  const V3 a = p.rv;
-  const double wij = p.f;
-  double E = 0.0;
+  const V3T<Real> a = p.rv;
+  const Real wij = p.f;
+  Real E = 0.0;
   const int nbi = B.nb[i], nbj = B.nb[j];
   for (int si = 0; si < nbi; si++) {
     const int qi = i * B.mb + si;
     const int k = B.bj[qi];
     if (k == j) continue;
     double4 rk = B.brv[qi], uk = B.bu[qi];
-    const V3 b = v3(rk.x, rk.y, rk.z);  // x_i - x_k
-    const double wki = uk.w;
+    const V3T<Real> b = xyz<Real>(rk);  // x_i - x_k
+    const Real wki = uk.w;
     for (int sj = 0; sj < nbj; sj++) {
       const int qj = j * B.mb + sj;
       const int l = B.bj[qj];
       if (l == i || l == k) continue;
-      double sin_ki = sqrt(norm2(cross(a, -b))) / (p.r * rk.w);
+      Real sin_ki = sqrt(norm2(cross(a, -b))) / (p.r * rk.w);
       if (fabs(sin_ki) < 0.1) continue;
       double4 rl = B.brv[qj], ul = B.bu[qj];
-      const V3 c = v3(rl.x, rl.y, rl.z);  // x_j - x_l
-      double sin_jl = sqrt(norm2(cross(a, c))) / (p.r * rl.w);
+      const V3T<Real> c = xyz<Real>(rl);  // x_j - x_l
+      Real sin_jl = sqrt(norm2(cross(a, c))) / (p.r * rl.w);
       if (fabs(sin_jl) < 0.1) continue;
-      const double wjl = ul.w;
-      const double eps = TP.eps[R.type(k)][R.type(l)];
-      V3 u = cross(-a, b);
-      V3 w = cross(a, c);
-      double e1 = dot(u, w);
-      double uu = norm2(u), ww = norm2(w);
-      double e2 = sqrt(uu) * sqrt(ww);
-      double cosd = (e2 == 0.0) ? 0.0 : e1 / e2;
+      const Real wjl = ul.w;
+      const Real eps = TP.eps[R.type(k)][R.type(l)];
+      V3T<Real> u = cross(-a, b);
+      V3T<Real> w = cross(a, c);
+      Real e1 = dot(u, w);
+      Real uu = norm2(u), ww = norm2(w);
+      Real e2 = sqrt(uu) * sqrt(ww);
+      Real cosd = (e2 == 0.0) ? 0.0 : e1 / e2;
       if (cosd < -1.0) cosd = -1.0;
       if (cosd > 1.0) cosd = 1.0;
-      double cdh = -cosd;
-      double val = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0) - 0.1 * eps;
-      double V = wki * wij * wjl;  // seed of Vtors (AIREBO_ETors.cxx:78)
+      Real cdh = -cosd;
+      Real val = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0) - 0.1 * eps;
+      Real V = wki * wij * wjl;  // seed of Vtors (AIREBO_ETors.cxx:78)
       if (val != 0.0) {
-        double der = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0 - 1.0) * 0.5;
-        double Vd = -1.0 * der * V;
+        Real der = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0 - 1.0) * 0.5;
+        Real Vd = -1.0 * der * V;
         if (Vd != 0.0 && e2 != 0.0) {
-          double cr = e1 / e2;
-          V3 U = w / e2 - u * (cr / uu);
-          V3 Wv = u / e2 - w * (cr / ww);
+          Real cr = e1 / e2;
+          V3T<Real> U = w / e2 - u * (cr / uu);
+          V3T<Real> Wv = u / e2 - w * (cr / ww);
           sink.pair(i, j, (cross(U, b) + cross(c, Wv)) * Vd);
           sink.cbond(i, si, cross(a, U) * Vd);
           sink.cbond(j, sj, cross(Wv, a) * Vd);
         }
       }
       // ki.f / ij.f / jl.f seeds (AIREBO_ETors.cxx:80-85)
-      double dfk = B.bd[qi].x, dfl = B.bd[qj].x;
-      if (dfk != 0.0) sink.cbond(i, si, v3(uk.x, uk.y, uk.z) * ((wij * wjl * val) * dfk));
+      Real dfk = B.bd[qi].x, dfl = B.bd[qj].x;
+      if (dfk != 0.0) sink.cbond(i, si, xyz<Real>(uk) * ((wij * wjl * val) * dfk));
       if (p.df != 0.0) sink.pair(i, j, p.u * ((wki * wjl * val) * p.df));
-      if (dfl != 0.0) sink.cbond(j, sj, v3(ul.x, ul.y, ul.z) * ((wki * wij * val) * dfl));
+      if (dfl != 0.0) sink.cbond(j, sj, xyz<Real>(ul) * ((wki * wij * val) * dfl));
       E += wki * wij * wjl * val;
     }
   }

@@ -159,57 +159,63 @@ MDG_HD int cij_find(const CijTable& T, int i, int j)
 }
 
 // S(t) switch (AIREBO::S / dS, AIREBO_LJ.cxx:116-156).
-MDG_HD double Slj(double arg, double amin, double amax)
+template <class Real>
+MDG_HD Real Slj(Real arg, double amin, double amax)
 {
   if (arg < amin) return 1.0;
   if (arg > amax) return 0.0;
-  double t = (arg - amin) / (amax - amin);
+  Real t = (arg - amin) / (amax - amin);
   return 1.0 - t * t * (3.0 - 2.0 * t);
 }
-MDG_HD double dSlj(double arg, double amin, double amax)
+template <class Real>
+MDG_HD Real dSlj(Real arg, double amin, double amax)
 {
   if (arg < amin) return 0.0;
   if (arg > amax) return 0.0;
-  double t = (arg - amin) / (amax - amin);
+  Real t = (arg - amin) / (amax - amin);
   return (-2.0 * t * (3.0 - 2.0 * t) + 2.0 * t * t) / (amax - amin);
 }
 
 // VLJ (AIREBO_LJ.cxx:158-189): f^LJ * 4 eps [(s/r)^12 - (s/r)^6]; with
 // V != 0 routes V * d/dr to the pair i-j.  Returns f*Val in `lj`, Val in `val`.
-template <class S>
-MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairG& pl, double V, S& sink, double& lj,
+// The powers of s/r are taken in double from the double length on every path
+// (a float length would carry 12 x its rounding into (s/r)^12).
+template <class Real, class S>
+MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairGT<Real>& pl, Real V, S& sink, double& lj,
                 double& val)
 {
-  const double fv = pl.f;
+  const Real fv = pl.f;
   lj = 0.0;
   val = 0.0;
   if (fv == 0.0) return;
-  const double r = pl.r;
+  const double r = pl.rd;
   const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
   const double sdr = sigma / r;
   double s6 = sdr;
   for (int q = 2; q <= 6; q++) s6 *= sdr;
   const double s12 = s6 * s6;
-  val = 4.0 * zeta * (s12 - s6);
+  const double vd = 4.0 * zeta * (s12 - s6);
+  val = vd;
   if (V != 0.0) {
-    double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
-    sink.pair(i, j, pl.u * (der * fv * V));
-    if (pl.df != 0.0) sink.pair(i, j, pl.u * ((val * V) * pl.df));
+    const double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
+    sink.pair(i, j, pl.u * Real(der * dbl(fv) * dbl(V)));
+    if (pl.df != 0.0) sink.pair(i, j, pl.u * Real((vd * dbl(V)) * dbl(pl.df)));
   }
-  lj = fv * val;
+  lj = dbl(fv) * vd;
 }
 
-struct LJ {
+template <class Real, class TB>
+struct LJT {
   const LJParams& P;
-  const Rebo& R;
+  const ReboT<Real, TB>& R;
   const CijTable& T;
 
   // b*_ij: REBO's b_ij average for the pair with r_alter = R1 of REBO
   // (AIREBO::BijAsterix, AIREBO_LJ.cxx:191-202).
   template <class S>
-  MDG_HD double bstar(int i, int j, const PairG& pl, double V, S& sink) const
+  MDG_HD Real bstar(int i, int j, const PairGT<Real>& pl, Real V, S& sink) const
   {
-    PairG p = pl;
+    PairGT<Real> p = pl;
     const int ti = R.type(i), tj = R.type(j);
     cutoff(p.r, R.P.R[ti][tj][0], R.P.R[ti][tj][1], p.f, p.df);
     p.alter = 1;
@@ -222,7 +228,7 @@ struct LJ {
   // energy; the middle bond of a 3-bond path is recorded through `mid` when
   // non-null (the i end passes it).
   template <class S>
-  MDG_HD double pair(int i, int j, const PairG& pl, S& sink, MidOut* mid, unsigned int* status) const
+  MDG_HD Real pair(int i, int j, const PairGT<Real>& pl, S& sink, MidOut* mid, unsigned int* status) const
   {
     // connectivity (AIREBO::Cij, AIREBO_LJ.cxx:381-408)
     int e = cij_find(T, i, j);
@@ -232,45 +238,49 @@ struct LJ {
       w = T.w[(long)i * T.cap + e];
       path = T.ent[(long)i * T.cap + e];
     }
+    // C_ij, the switches and their products are per-pair scalars, kept in
+    // double on every path: 1 - w and 1 - S(t_r) cancel to ~1e-3 here, which
+    // float would turn into 1e-5 relative errors of the pair force.  Only b*
+    // and the vectors handed to the sink use the arithmetic type.
     const double C = 1 - w;
     if (!(C > 0.0)) return 0.0;
     const int ti = R.type(i), tj = R.type(j);
-    const double r = pl.r;
+    const double r = pl.rd;
     // StrStb value (AIREBO_LJ.cxx:79-114)
     const double rmin = P.RLJ[ti][tj][0], rmax = P.RLJ[ti][tj][1];
     const double Str = Slj(r, rmin, rmax);
     double Stb = 0.0, bij = 0.0, SrSb = 1.0;
-    Sink dummy;
+    SinkT<Real> dummy;
     if (Str != 0.0) {
-      bij = bstar(i, j, pl, 0.0, dummy);
+      bij = dbl(bstar(i, j, pl, Real(0.0), dummy));
       Stb = Slj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
       SrSb += Str * Stb - Str;
     }
     // VLJ with seed SrSb*C
     if (pl.f == 0.0) return 0.0;
     double LJv, val;
-    vlj(P, ti, tj, i, j, pl, SrSb * C, sink, LJv, val);
+    vlj(P, ti, tj, i, j, pl, Real(SrSb * C), sink, LJv, val);
     // StrStb gradient with seed C*LJ
     const double V2 = C * LJv;
     if (Str != 0.0 && V2 != 0.0) {
-      double dStr = dSlj(r, rmin, rmax);
-      if (dStr != 0.0) sink.pair(i, j, pl.u * (-dStr * V2));
-      double dStb = dSlj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
-      if (dStr != 0.0 && Stb != 0.0) sink.pair(i, j, pl.u * (dStr * Stb * V2));
-      if (dStb != 0.0) bstar(i, j, pl, Str * dStb * V2, sink);
+      const double dStr = dSlj(r, rmin, rmax);
+      if (dStr != 0.0) sink.pair(i, j, pl.u * Real(-dStr * V2));
+      const double dStb = dSlj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
+      if (dStr != 0.0 && Stb != 0.0) sink.pair(i, j, pl.u * Real(dStr * Stb * V2));
+      if (dStb != 0.0) bstar(i, j, pl, Real(Str * dStb * V2), sink);
     }
-    // Cij gradient with seed SrSb*LJ: -V * (product of the other cutoffs) * df
-    const double V3 = SrSb * LJv;
-    if (e >= 0 && V3 != 0.0 && path.y > 0) {
+    // Cij gradient with seed Vc3 = SrSb*LJ: -V * (product of the other cutoffs) * df
+    const double Vc3 = SrSb * LJv;
+    if (e >= 0 && Vc3 != 0.0 && path.y > 0) {
       const BondList& B = R.B;
       if (path.y == 1) {
         int s = bond_slot(B, i, j);
         if (s >= 0) {
           const int q = i * B.mb + s;
-          double df = B.bd[q].x;
+          const double df = B.bd[q].x;
           if (df != 0.0) {
             double4 u = B.bu[q];
-            sink.pair(i, j, v3(u.x, u.y, u.z) * ((-1.0 * V3) * df));
+            sink.pair(i, j, xyz<Real>(u) * Real((-1.0 * Vc3) * df));
           }
         }
       } else {
@@ -292,30 +302,32 @@ struct LJ {
           dfmid = B.bd[qm].x;
         }
         // products in path order (AIREBO_LJ.cxx:396-402)
-        double m1 = (path.y == 2) ? 1.0 * fl : 1.0 * fmid * fl;
-        double ml = (path.y == 2) ? 1.0 * f1 : 1.0 * f1 * fmid;
-        double df1 = B.bd[q1].x, dfl = B.bd[qj].x;
+        const double m1 = (path.y == 2) ? 1.0 * fl : 1.0 * fmid * fl;
+        const double ml = (path.y == 2) ? 1.0 * f1 : 1.0 * f1 * fmid;
+        const double df1 = B.bd[q1].x, dfl = B.bd[qj].x;
         if (df1 != 0.0) {
           double4 u = B.bu[q1];
-          sink.cbond(i, s1, v3(u.x, u.y, u.z) * ((-m1 * V3) * df1));
+          sink.cbond(i, s1, xyz<Real>(u) * Real((-m1 * Vc3) * df1));
         }
         if (dfl != 0.0) {
           double4 u = B.bu[qj];
-          sink.cbond(j, sj, v3(u.x, u.y, u.z) * ((-ml * V3) * dfl));
+          sink.cbond(j, sj, xyz<Real>(u) * Real((-ml * Vc3) * dfl));
         }
         if (path.y == 3 && dfmid != 0.0 && mid) {
-          double mm = 1.0 * f1 * fl;
+          const double mm = 1.0 * f1 * fl;
           mid->k = k;
           mid->sm = sm;
           mid->m = m;
           mid->valid = 1;
-          mid->c = (-mm * V3) * dfmid;
+          mid->c = (-mm * Vc3) * dfmid;
         }
       }
     }
-    return SrSb * C * LJv;
+    return Real(SrSb * C * LJv);
   }
 };
+
+typedef LJT<double, ReboTables> LJ;
 
 // Special LJ pairs (those needing b*_ij or a connectivity gradient) are
 // evaluated one task per (atom, pair); each task writes its own record and a
@@ -342,7 +354,7 @@ MDG_HD int rec_size(int nb) { return 4 + 4 * nb; }
 // Classifies one LJ pair seen from atom a: returns 0 (skip), 1 (plain: C = 1
 // and S(t_r) = 0, so E = VLJ) or 2 (special).  For plain pairs adds the own
 // gradient and, at the lower end, the energy.
-template <class S>
+template <class Real, class S>
 MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, int a, int b, V3 xa, int ta,
                          S& sink, double& e)
 {
@@ -359,18 +371,21 @@ MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, 
   const double w = ei >= 0 ? T.w[(long)lo * T.cap + ei] : 0.0;
   const double C = 1 - w;
   if (!(C > 0.0)) return 0;
-  PairG p;
-  p.rv = rv;
-  p.r = sqrt(d2);
-  const double Str = Slj(p.r, P.RLJ[ta][tb][0], P.RLJ[ta][tb][1]);
+  const double r = sqrt(d2);
+  const double Str = Slj(r, P.RLJ[ta][tb][0], P.RLJ[ta][tb][1]);
   if (Str != 0.0 || w != 0.0) return 2;
-  p.u = rv / p.r;
+  // the pair term itself in the arithmetic type
+  PairGT<Real> p;
+  p.rv = cvt3<Real>(rv);
+  p.r = r;
+  p.rd = r;
+  p.u = cvt3<Real>(rv / r);
   cutoff(p.r, R1, R2, p.f, p.df);
   p.alter = 0;
   p.ralt = 0.0;
   double LJv, val;
   const int tlo = lo == a ? ta : tb, thi = lo == a ? tb : ta;
-  vlj(P, tlo, thi, lo, hi, p, 1.0 * C, sink, LJv, val);
+  vlj(P, tlo, thi, lo, hi, p, Real(1.0 * C), sink, LJv, val);
   if (a == lo) e += 1.0 * C * LJv;
   return 1;
 }
@@ -409,7 +424,8 @@ MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
 }
 
 // Records one special task: the full pair term from end a with a private sink.
-MDG_HD void lj_special_task(const LJ& X, const State& St, SpecialTasks& Tk, int t, unsigned int* status)
+template <class Real, class TB>
+MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTasks& Tk, int t, unsigned int* status)
 {
   const int2 ap = Tk.flat[t];
   const int a = ap.x, b = ap.y;
@@ -417,7 +433,7 @@ MDG_HD void lj_special_task(const LJ& X, const State& St, SpecialTasks& Tk, int 
   const long ro = Tk.trec[t];
   if (ro < 0) return;  // beyond the record capacity (already flagged)
   double* rec = Tk.rec + ro;
-  Sink sink;
+  SinkT<Real> sink;
   sink.a = a;
   sink.g = v3(0, 0, 0);
   sink.A = rec + 4;
@@ -432,20 +448,22 @@ MDG_HD void lj_special_task(const LJ& X, const State& St, SpecialTasks& Tk, int 
   if (a < b) rv = depos(St.box, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z));
   else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), v3(pa.x, pa.y, pa.z)); }
   const int tlo = (int)St.pos[lo].w, thi = (int)St.pos[hi].w;
-  PairG p;
-  p.rv = rv;
-  p.r = sqrt(norm2(rv));
-  p.u = rv / p.r;
+  const double r = sqrt(norm2(rv));
+  PairGT<Real> p;
+  p.rv = cvt3<Real>(rv);
+  p.r = r;
+  p.rd = r;
+  p.u = cvt3<Real>(rv / r);
   cutoff(p.r, X.P.R[tlo][thi][0], X.P.R[tlo][thi][1], p.f, p.df);
   p.alter = 0;
   p.ralt = 0.0;
   MidOut mo;
   mo.valid = 0;
-  double E = X.pair(lo, hi, p, sink, (a == lo) ? &mo : nullptr, status);
+  const Real E = X.pair(lo, hi, p, sink, (a == lo) ? &mo : nullptr, status);
   rec[0] = sink.g.x;
   rec[1] = sink.g.y;
   rec[2] = sink.g.z;
-  rec[3] = (a == lo) ? E : 0.0;
+  rec[3] = (a == lo) ? dbl(E) : 0.0;
   Tk.mid[t] = make_int4(mo.k, mo.sm, mo.m, mo.valid);
   Tk.midc[t] = mo.valid ? mo.c : 0.0;
 }

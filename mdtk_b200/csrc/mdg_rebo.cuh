@@ -34,50 +34,60 @@ struct BondList {
 };
 
 // A pair vector as AtomsPair holds it (AtomsPair.hpp:35-160): rv = x_1 - x_2.
-struct PairG {
-  V3 rv, u;        // vector and unit vector
-  double r, f, df; // length and REBO cosine cutoff (R cutoffs of the pair types)
-  double ralt;     // r_alter (b*_ij uses R1 of the pair, AIREBO_LJ.cxx:196-198)
+// Real is the arithmetic type (double, or f32 on the mixed-precision path).
+template <class Real>
+struct PairGT {
+  V3T<Real> rv, u;    // vector and unit vector
+  Real r, f, df;      // length and REBO cosine cutoff (R cutoffs of the pair types)
+  double rd;          // the length in double (the pair terms V_R, V_A use it on every path)
+  Real ralt;          // r_alter (b*_ij uses R1 of the pair, AIREBO_LJ.cxx:196-198)
   int alter;
 };
+typedef PairGT<double> PairG;
 
-MDG_HD PairG pair_reverse(const PairG& p)
+template <class Real>
+MDG_HD PairGT<Real> pair_reverse(const PairGT<Real>& p)
 {
-  PairG q = p;
+  PairGT<Real> q = p;
   q.rv = -p.rv;
   q.u = -p.u;
   return q;
 }
 
-// Gradient routing for one evaluating atom.
-struct Sink {
+// Gradient routing for one evaluating atom.  Contributions arrive in the
+// arithmetic type and are accumulated in double.
+template <class Real>
+struct SinkT {
   int a;           // evaluating atom
   V3 g;            // dE/dx_a accumulated here
   double* A;       // [mb*3] this atom's bond slots: gradient owed to each partner
   double* W;       // [mb]   third-shell coefficients of this atom's bond slots
-  MDG_HD void pair(int p, int q, V3 v)
+  MDG_HD void pair(int p, int q, V3T<Real> v)
   {
-    if (p == a) g += v;
-    else if (q == a) g -= v;
+    if (p == a) g += to_d(v);
+    else if (q == a) g -= to_d(v);
   }
-  MDG_HD void cbond(int c, int s, V3 v)
+  MDG_HD void cbond(int c, int s, V3T<Real> v)
   {
     if (c == a) {
-      g += v;
-      A[3 * s + 0] -= v.x;
-      A[3 * s + 1] -= v.y;
-      A[3 * s + 2] -= v.z;
+      const V3 d = to_d(v);
+      g += d;
+      A[3 * s + 0] -= d.x;
+      A[3 * s + 1] -= d.y;
+      A[3 * s + 2] -= d.z;
     }
   }
-  MDG_HD void wt(int c, int s, double w)
+  MDG_HD void wt(int c, int s, Real w)
   {
-    if (c == a) W[s] += w;
+    if (c == a) W[s] += dbl(w);
   }
 };
+typedef SinkT<double> Sink;
 
-struct Rebo {
+template <class Real, class TB>
+struct ReboT {
   const ReboParams& P;
-  const ReboTables& T;
+  const TB& T;
   const BondList& B;
   unsigned int* status;
 
@@ -86,14 +96,14 @@ struct Rebo {
 
   // ---- coordination numbers (REBO::Nt/NH/NC, REBO.cxx:423-502) ----
   // which: 0 = all neighbours (Nt), 1 = H only (NH), 2 = C only (NC).
-  MDG_HD double Nval(int c, int o, const PairG& p, int which) const
+  MDG_HD Real Nval(int c, int o, const PairGT<Real>& p, int which) const
   {
     double4 n = B.nco[c];
-    double N = which == 0 ? n.x : (which == 1 ? n.z : n.y);
+    Real N = which == 0 ? n.x : (which == 1 ? n.z : n.y);
     int to = type(o);
     bool sub = (which == 0) || (which == 1 && to == kH) || (which == 2 && to == kC);
     if (sub && p.r < R2(type(c), to)) N -= p.f;
-    if (!(N > -1e-15)) *status |= ST_N_NEGATIVE;
+    if (!(N > -n_neg_tol(N))) *status |= ST_N_NEGATIVE;
     if (N < 0) N = 0;
     return N;
   }
@@ -101,7 +111,7 @@ struct Rebo {
   // dfThem (REBO.cxx:409-421): V * df_ck along every switching-region bond
   // c-k (k != o) of the chosen neighbour class.
   template <class S>
-  MDG_HD void dfthem(int c, int o, double V, int which, S& sink) const
+  MDG_HD void dfthem(int c, int o, Real V, int which, S& sink) const
   {
     if (V == 0.0) return;
     const int nb = B.nb[c];
@@ -114,10 +124,10 @@ struct Rebo {
         if (which == 1 && tk != kH) continue;
         if (which == 2 && tk != kC) continue;
       }
-      double df = B.bd[q].x;
+      Real df = B.bd[q].x;
       if (df != 0.0) {
         double4 u = B.bu[q];
-        sink.cbond(c, s, v3(u.x, u.y, u.z) * (V * df));
+        sink.cbond(c, s, xyz<Real>(u) * (V * df));
       }
     }
   }
@@ -126,40 +136,40 @@ struct Rebo {
   // Returns G; with V != 0 routes V * dG to the pair c-o, the bond c-k and
   // (carbon centre) through N_co to c's switching bonds.
   template <class S>
-  MDG_HD double G(int c, int o, const PairG& p, int s_k, V3 bk_rv, double bk_r, V3 bk_u, double Nco,
-                  double V, S& sink) const
+  MDG_HD Real G(int c, int o, const PairGT<Real>& p, int s_k, V3T<Real> bk_rv, Real bk_r, V3T<Real> bk_u, Real Nco,
+                  Real V, S& sink) const
   {
-    double e1 = dot(p.rv, bk_rv);
-    double e2 = p.r * bk_r;
-    double cost = e1 / e2;
+    Real e1 = dot(p.rv, bk_rv);
+    Real e2 = p.r * bk_r;
+    Real cost = e1 / e2;
     if (!(cost >= -1.0 - 1e-7 && cost <= 1.0 + 1e-7)) *status |= ST_COS_RANGE;
     if (cost < -1.0) cost = -1.0;
     if (cost > 1.0) cost = 1.0;
-    double Vc = 0.0, val;
+    Real Vc = 0.0, val;
     if (type(c) == kC) {
-      double Sp = Sprime(Nco, P.Ntot[0], P.Ntot[1]);
-      double g1 = g_eval(T.G[0], cost, 0);
-      double g2 = g_eval(T.G[1], cost, 0);
+      Real Sp = Sprime(Nco, P.Ntot[0], P.Ntot[1]);
+      Real g1 = g_eval(T.G[0], cost, 0);
+      Real g2 = g_eval(T.G[1], cost, 0);
       if (V != 0.0) {
-        double SpDer = dSprime(Nco, P.Ntot[0], P.Ntot[1]);
-        double g1d = g_eval(T.G[0], cost, 1);
-        double g2d = g_eval(T.G[1], cost, 1);
+        Real SpDer = dSprime(Nco, P.Ntot[0], P.Ntot[1]);
+        Real g1d = g_eval(T.G[0], cost, 1);
+        Real g2d = g_eval(T.G[1], cost, 1);
         if (g2d != 0.0 || g1d != 0.0) Vc = g2d * V + g1d * Sp * V + (-g2d * Sp * V);
         if ((g2 != 0.0 || g1 != 0.0) && SpDer != 0.0) dfthem(c, o, g1 * SpDer * V + (-g2 * SpDer * V), 0, sink);
       }
       val = g2 + Sp * (g1 - g2);
     } else {
       if (V != 0.0) {
-        double ghd = g_eval(T.G[2], cost, 1);
+        Real ghd = g_eval(T.G[2], cost, 1);
         if (ghd != 0.0) Vc = ghd * V;
       }
       val = g_eval(T.G[2], cost, 0);
     }
     if (Vc != 0.0) {
       // d cos(theta_ock) / d(x_c - x_o) and d/d(x_c - x_k) (FGeneral.hpp:152-178)
-      double e2s = SQR(e2);
-      V3 dpa = (bk_rv * e2 - p.u * (bk_r * e1)) / e2s;
-      V3 dpb = (p.rv * e2 - bk_u * (p.r * e1)) / e2s;
+      Real e2s = SQR(e2);
+      V3T<Real> dpa = (bk_rv * e2 - p.u * (bk_r * e1)) / e2s;
+      V3T<Real> dpb = (p.rv * e2 - bk_u * (p.r * e1)) / e2s;
       sink.pair(c, o, dpa * Vc);
       sink.cbond(c, s_k, dpb * Vc);
     }
@@ -167,20 +177,20 @@ struct Rebo {
   }
 
   // ExpTerm (REBO.cxx:213-233): 1 unless the centre is H.
-  MDG_HD double expterm(int c, int o, const PairG& p, int k, double bk_r) const
+  MDG_HD Real expterm(int c, int o, const PairGT<Real>& p, int k, Real bk_r) const
   {
     if (type(c) != kH) return 1.0;
     int tc = type(c), to = type(o), tk = type(k);
-    double rij = p.alter ? p.ralt : p.r;
+    Real rij = p.alter ? p.ralt : p.r;
     return exp(4.0 * ((P.rho[tc][tk] - bk_r) - (P.rho[tc][to] - rij)));
   }
 
   // D_co = 1 + sum_k G f_ck lambda + P_co (REBO::D, REBO.cxx:235-265), value.
-  MDG_HD double D_value(int c, int o, const PairG& p) const
+  MDG_HD Real D_value(int c, int o, const PairGT<Real>& p) const
   {
-    Sink dummy;
-    double Dij = 1.0;
-    double Nco = Nval(c, o, p, 0);
+    SinkT<Real> dummy;
+    Real Dij = 1.0;
+    Real Nco = Nval(c, o, p, 0);
     const int nb = B.nb[c];
     for (int s = 0; s < nb; s++) {
       const int q = c * B.mb + s;
@@ -188,9 +198,9 @@ struct Rebo {
       if (k == o) continue;
       double4 rv = B.brv[q];
       double4 u = B.bu[q];
-      double ex = expterm(c, o, p, k, rv.w);
+      Real ex = expterm(c, o, p, k, rv.w);
       if (ex != 0.0) {
-        double gv = G(c, o, p, s, v3(rv.x, rv.y, rv.z), rv.w, v3(u.x, u.y, u.z), Nco, 0.0, dummy);
+        Real gv = G(c, o, p, s, xyz<Real>(rv), rv.w, xyz<Real>(u), Nco, 0.0, dummy);
         Dij += gv * u.w * ex;
       }
     }
@@ -200,9 +210,9 @@ struct Rebo {
 
   // D_co gradient pass with seed V.
   template <class S>
-  MDG_HD void D_grad(int c, int o, const PairG& p, double V, S& sink) const
+  MDG_HD void D_grad(int c, int o, const PairGT<Real>& p, Real V, S& sink) const
   {
-    double Nco = Nval(c, o, p, 0);
+    Real Nco = Nval(c, o, p, 0);
     const int nb = B.nb[c];
     const bool hcen = type(c) == kH;
     for (int s = 0; s < nb; s++) {
@@ -211,19 +221,19 @@ struct Rebo {
       if (k == o) continue;
       double4 rv = B.brv[q];
       double4 u = B.bu[q];
-      V3 brv = v3(rv.x, rv.y, rv.z), bu3 = v3(u.x, u.y, u.z);
-      double ex = expterm(c, o, p, k, rv.w);
+      V3T<Real> brv = xyz<Real>(rv), bu3 = xyz<Real>(u);
+      Real ex = expterm(c, o, p, k, rv.w);
       if (ex == 0.0) continue;
-      Sink dummy;
-      double gv = G(c, o, p, s, brv, rv.w, bu3, Nco, 0.0, dummy);
-      double fv = u.w;
+      SinkT<Real> dummy;
+      Real gv = G(c, o, p, s, brv, rv.w, bu3, Nco, 0.0, dummy);
+      Real fv = u.w;
       G(c, o, p, s, brv, rv.w, bu3, Nco, fv * ex * V, sink);
-      double df = B.bd[q].x;
+      Real df = B.bd[q].x;
       if (df != 0.0) sink.cbond(c, s, bu3 * ((gv * ex * V) * df));
       if (hcen) {
-        double Vx = gv * fv * V;
+        Real Vx = gv * fv * V;
         if (Vx != 0.0) {
-          double dert = ex * 4.0;
+          Real dert = ex * 4.0;
           sink.pair(c, o, p.u * (dert * Vx));
           sink.cbond(c, s, bu3 * (-dert * Vx));
         }
@@ -234,14 +244,14 @@ struct Rebo {
 
   // P_co (REBO::P, REBO.cxx:626-657): bicubic in (N^H, N^C) for a carbon centre.
   template <class S>
-  MDG_HD double P_term(int c, int o, const PairG& p, double V, S& sink) const
+  MDG_HD Real P_term(int c, int o, const PairGT<Real>& p, Real V, S& sink) const
   {
     if (type(c) != kC) return 0.0;
     int fam = type(o) == kC ? 0 : 1;
-    double nh = Nval(c, o, p, 1);
-    double nc = Nval(c, o, p, 2);
+    Real nh = Nval(c, o, p, 1);
+    Real nc = Nval(c, o, p, 2);
     if (V == 0.0) return p_value(T, fam, nh, nc);
-    double v, dh, dc;
+    Real v, dh, dc;
     p_eval(T, fam, nh, nc, v, dh, dc, status);
     dfthem(c, o, dh * V, 1, sink);
     dfthem(c, o, dc * V, 2, sink);
@@ -250,11 +260,11 @@ struct Rebo {
 
   // p^{sigma pi}_co = D^-1/2 (REBO::p_sigma_pi, REBO.cxx:267-278).
   template <class S>
-  MDG_HD double p_sigma_pi(int c, int o, const PairG& p, double V, S& sink) const
+  MDG_HD Real p_sigma_pi(int c, int o, const PairGT<Real>& p, Real V, S& sink) const
   {
-    double DVal = D_value(c, o, p);
+    Real DVal = D_value(c, o, p);
     if (V != 0.0) {
-      double Der = -0.5 * pow(DVal, -0.5 - 1.0);
+      Real Der = -0.5 * pow(DVal, -0.5 - 1.0);
       D_grad(c, o, p, Der * V, sink);
     }
     return pow(DVal, -0.5);
@@ -262,33 +272,33 @@ struct Rebo {
 
   // N_conj halves (REBO::NconjSum1/2, REBO.cxx:540-606): sum over C
   // neighbours k of c (k != o) of f_ck * S'(N_kc).
-  MDG_HD double nconj_sum(int c, int o) const
+  MDG_HD Real nconj_sum(int c, int o) const
   {
-    double sum = 0.0;
+    Real sum = 0.0;
     const int nb = B.nb[c];
     for (int s = 0; s < nb; s++) {
       const int q = c * B.mb + s;
       const int k = B.bj[q];
       if (k == o || type(k) != kC) continue;
-      double f = B.bu[q].w;
-      double N = Nk_excl(k, B.brv[q].w, f, c);
+      Real f = B.bu[q].w;
+      Real N = Nk_excl(k, B.brv[q].w, f, c);
       sum += f * Sprime(N, P.Ntot[0], P.Ntot[1]);
     }
     return sum;
   }
 
   // N_kc = Nt_k - f_kc (the pair k-c seen from k), clamped at 0.
-  MDG_HD double Nk_excl(int k, double r, double f, int c) const
+  MDG_HD Real Nk_excl(int k, Real r, Real f, int c) const
   {
-    double N = B.nco[k].x;
+    Real N = B.nco[k].x;
     if (r < R2(type(k), type(c))) N -= f;
-    if (!(N > -1e-15)) *status |= ST_N_NEGATIVE;
+    if (!(N > -n_neg_tol(N))) *status |= ST_N_NEGATIVE;
     if (N < 0) N = 0;
     return N;
   }
 
   template <class S>
-  MDG_HD void nconj_sum_grad(int c, int o, double V, S& sink) const
+  MDG_HD void nconj_sum_grad(int c, int o, Real V, S& sink) const
   {
     const int nb = B.nb[c];
     for (int s = 0; s < nb; s++) {
@@ -296,28 +306,28 @@ struct Rebo {
       const int k = B.bj[q];
       if (k == o || type(k) != kC) continue;
       double4 u = B.bu[q];
-      double f = u.w;
-      double N = Nk_excl(k, B.brv[q].w, f, c);
-      double Sp = Sprime(N, P.Ntot[0], P.Ntot[1]);
-      double df = B.bd[q].x;
-      if (df != 0.0) sink.cbond(c, s, v3(u.x, u.y, u.z) * ((Sp * V) * df));
-      double w = f * dSprime(N, P.Ntot[0], P.Ntot[1]) * V;
+      Real f = u.w;
+      Real N = Nk_excl(k, B.brv[q].w, f, c);
+      Real Sp = Sprime(N, P.Ntot[0], P.Ntot[1]);
+      Real df = B.bd[q].x;
+      if (df != 0.0) sink.cbond(c, s, xyz<Real>(u) * ((Sp * V) * df));
+      Real w = f * dSprime(N, P.Ntot[0], P.Ntot[1]) * V;
       if (w != 0.0) sink.wt(c, s, w);
     }
   }
 
   // N_conj = 1 + sum1^2 + sum2^2 (REBO::Nconj, REBO.cxx:608-624).
-  MDG_HD double nconj(int i, int j, double& s1, double& s2) const
+  MDG_HD Real nconj(int i, int j, Real& s1, Real& s2) const
   {
     s1 = nconj_sum(i, j);
     s2 = nconj_sum(j, i);
-    double N = 1.0;
+    Real N = 1.0;
     N += SQR(s1);
     N += SQR(s2);
     return N;
   }
   template <class S>
-  MDG_HD void nconj_grad(int i, int j, double s1, double s2, double V, S& sink) const
+  MDG_HD void nconj_grad(int i, int j, Real s1, Real s2, Real V, S& sink) const
   {
     if (V == 0.0) return;
     if (s1 != 0.0) nconj_sum_grad(i, j, 2.0 * s1 * V, sink);
@@ -326,64 +336,64 @@ struct Rebo {
 
   // ---- dihedral sum (REBO::pi_dh_sum, REBO.cxx:716-759) ----
   template <class S>
-  MDG_HD double dh_sum(int i, int j, const PairG& p, double V, S& sink) const
+  MDG_HD Real dh_sum(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
   {
-    double tsum = 0.0;
+    Real tsum = 0.0;
     const int nbi = B.nb[i], nbj = B.nb[j];
-    const V3 a = p.rv;
+    const V3T<Real> a = p.rv;
     for (int si = 0; si < nbi; si++) {
       const int qi = i * B.mb + si;
       const int k = B.bj[qi];
       if (k == j) continue;
       double4 rk = B.brv[qi];
-      const V3 b = v3(rk.x, rk.y, rk.z);  // x_i - x_k
+      const V3T<Real> b = xyz<Real>(rk);  // x_i - x_k
       for (int sj = 0; sj < nbj; sj++) {
         const int qj = j * B.mb + sj;
         const int l = B.bj[qj];
         if (l == i) continue;
         if (k == l) continue;
-        double sin_ik = sqrt(norm2(cross(a, -b))) / (p.r * rk.w);
+        Real sin_ik = sqrt(norm2(cross(a, -b))) / (p.r * rk.w);
         if (fabs(sin_ik) < 0.1) continue;
         double4 rl = B.brv[qj];
-        const V3 cc = v3(rl.x, rl.y, rl.z);  // x_j - x_l
-        double sin_jl = sqrt(norm2(cross(a, -cc))) / (p.r * rl.w);
+        const V3T<Real> cc = xyz<Real>(rl);  // x_j - x_l
+        Real sin_jl = sqrt(norm2(cross(a, -cc))) / (p.r * rl.w);
         if (fabs(sin_jl) < 0.1) continue;
         int ti = type(i), tk = type(k), tj = type(j), tl = type(l);
-        double fik = Sprime(rk.w, P.Rp[ti][tk][0], P.Rp[ti][tk][1]);
-        double fjl = Sprime(rl.w, P.Rp[tj][tl][0], P.Rp[tj][tl][1]);
+        Real fik = Sprime(Real(rk.w), P.Rp[ti][tk][0], P.Rp[ti][tk][1]);
+        Real fjl = Sprime(Real(rl.w), P.Rp[tj][tl][0], P.Rp[tj][tl][1]);
         // cos of the dihedral (FGeneral::CosDihedral, FGeneral.hpp:197-305)
-        V3 u = cross(-a, b);
-        V3 w = cross(a, cc);
-        double e1 = dot(u, w);
-        double uu = norm2(u), ww = norm2(w);
-        double e21 = sqrt(uu), e22 = sqrt(ww);
-        double e2 = e21 * e22;
-        double cosd = (e2 == 0.0) ? 0.0 : e1 / e2;
+        V3T<Real> u = cross(-a, b);
+        V3T<Real> w = cross(a, cc);
+        Real e1 = dot(u, w);
+        Real uu = norm2(u), ww = norm2(w);
+        Real e21 = sqrt(uu), e22 = sqrt(ww);
+        Real e2 = e21 * e22;
+        Real cosd = (e2 == 0.0) ? 0.0 : e1 / e2;
         if (cosd < -1.0) cosd = -1.0;
         if (cosd > 1.0) cosd = 1.0;
-        double cdh = -cosd;
+        Real cdh = -cosd;
         if (V != 0.0) {
-          double Vd = 2.0 * cdh * fik * fjl * V;
+          Real Vd = 2.0 * cdh * fik * fjl * V;
           if (Vd != 0.0 && e2 != 0.0) {
-            double cr = e1 / e2;
-            V3 U = w / e2 - u * (cr / uu);
-            V3 Wv = u / e2 - w * (cr / ww);
-            V3 da = cross(U, b) + cross(cc, Wv);
-            V3 db = cross(a, U);
-            V3 dc = cross(Wv, a);
+            Real cr = e1 / e2;
+            V3T<Real> U = w / e2 - u * (cr / uu);
+            V3T<Real> Wv = u / e2 - w * (cr / ww);
+            V3T<Real> da = cross(U, b) + cross(cc, Wv);
+            V3T<Real> db = cross(a, U);
+            V3T<Real> dc = cross(Wv, a);
             sink.pair(i, j, da * Vd);
             sink.cbond(i, si, db * Vd);
             sink.cbond(j, sj, dc * Vd);
           }
-          double vk = (1.0 - SQR(cdh)) * fjl * V;
+          Real vk = (1.0 - SQR(cdh)) * fjl * V;
           if (vk != 0.0 && rk.w >= P.Rp[ti][tk][0] && rk.w <= P.Rp[ti][tk][1]) {
             double4 uk = B.bu[qi];
-            sink.cbond(i, si, v3(uk.x, uk.y, uk.z) * (dSprime(rk.w, P.Rp[ti][tk][0], P.Rp[ti][tk][1]) * vk));
+            sink.cbond(i, si, xyz<Real>(uk) * (dSprime(Real(rk.w), P.Rp[ti][tk][0], P.Rp[ti][tk][1]) * vk));
           }
-          double vl = (1.0 - SQR(cdh)) * fik * V;
+          Real vl = (1.0 - SQR(cdh)) * fik * V;
           if (vl != 0.0 && rl.w >= P.Rp[tj][tl][0] && rl.w <= P.Rp[tj][tl][1]) {
             double4 ul = B.bu[qj];
-            sink.cbond(j, sj, v3(ul.x, ul.y, ul.z) * (dSprime(rl.w, P.Rp[tj][tl][0], P.Rp[tj][tl][1]) * vl));
+            sink.cbond(j, sj, xyz<Real>(ul) * (dSprime(Real(rl.w), P.Rp[tj][tl][0], P.Rp[tj][tl][1]) * vl));
           }
         }
         tsum += (1.0 - SQR(cdh)) * fik * fjl;
@@ -395,30 +405,30 @@ struct Rebo {
   // ---- b_ij average (REBO::Baver, REBO.cxx:200-211) with seed V ----
   // i < j in the reference's loop order; p = pair i->j.
   template <class S>
-  MDG_HD double baver(int i, int j, const PairG& p, double V, S& sink) const
+  MDG_HD Real baver(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
   {
-    const PairG q = pair_reverse(p);
-    const double half = V / 2.0;
-    double pij = p_sigma_pi(i, j, p, half, sink);
-    double pji = p_sigma_pi(j, i, q, half, sink);
-    double val = (pij + pji) / 2.0;
+    const PairGT<Real> q = pair_reverse(p);
+    const Real half = V / 2.0;
+    Real pij = p_sigma_pi(i, j, p, half, sink);
+    Real pji = p_sigma_pi(j, i, q, half, sink);
+    Real val = (pij + pji) / 2.0;
 
     const int ti = type(i), tj = type(j);
     // pi_rc (REBO.cxx:659-714): the H-C order evaluates as C-H with i and j swapped
     int ci = i, cj = j;
-    const PairG* pc = &p;
-    const PairG* qc = &q;
+    const PairGT<Real>* pc = &p;
+    const PairGT<Real>* qc = &q;
     if (ti == kH && tj == kC) { ci = j; cj = i; pc = &q; qc = &p; }
     const int tci = type(ci), tcj = type(cj);
     int fam = (tci == kC && tcj == kC) ? 0 : ((tci == kC && tcj == kH) ? 1 : 2);
-    double Nti = Nval(ci, cj, *pc, 0);
-    double Ntj = Nval(cj, ci, *qc, 0);
-    double s1, s2;
-    double Nconj = nconj(ci, cj, s1, s2);
-    double F[4];
+    Real Nti = Nval(ci, cj, *pc, 0);
+    Real Ntj = Nval(cj, ci, *qc, 0);
+    Real s1, s2;
+    Real Nconj = nconj(ci, cj, s1, s2);
+    Real F[4];
     t_eval(T, fam, Nti, Ntj, Nconj, F, status);
     val += F[0];
-    double cNti = 0.0, cNtj = 0.0, cNconj = 0.0;
+    Real cNti = 0.0, cNtj = 0.0, cNconj = 0.0;
     if (V != 0.0) {
       cNti = F[1] * V;
       cNtj = F[2] * V;
@@ -427,14 +437,14 @@ struct Rebo {
     // pi_dh (REBO.cxx:761-814): C-C only, T_ij nonzero only near (2,2,.)
     if (ti == kC && tj == kC) {
       // here (ci,cj) == (i,j)
-      double Tv[4];
+      Real Tv[4];
       t_eval(T, 3, Nti, Ntj, Nconj, Tv, status);
       if (Tv[0] != 0.0) {
-        double ts = dh_sum(i, j, p, 0.0, sink);
+        Real ts = dh_sum(i, j, p, 0.0, sink);
         val += Tv[0] * ts;
         if (V != 0.0) {
           if (ts != 0.0) {
-            double Vt = ts * V;
+            Real Vt = ts * V;
             cNti += Tv[1] * Vt;
             cNtj += Tv[2] * Vt;
             cNconj += Tv[3] * Vt;
@@ -453,64 +463,71 @@ struct Rebo {
 
   // ---- repulsive / attractive pair terms (REBO.cxx:134-198) ----
   // Return f*V_R and -f*V_A; with V != 0 route V * d/d(r_ij) to the pair.
+  // Evaluated in double from the double length on every path: their
+  // exponentials are the largest, most cancelling terms of the bond energy,
+  // and a float length alone would put ~alpha*r*eps_f of relative error into
+  // them.
   template <class S>
-  MDG_HD double VR(int i, int j, const PairG& p, double V, S& sink) const
+  MDG_HD Real VR(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
   {
-    double f = p.f;
+    const Real f = p.f;
     if (f == 0.0) return 0.0;
     int ti = type(i), tj = type(j);
-    double r = p.r, Q = P.Q[ti][tj], A = P.A[ti][tj], al = P.alpha[ti][tj];
-    double t1 = A * exp(-al * r);
-    double val = (1 + Q / r) * t1;
+    const double r = p.rd, Q = P.Q[ti][tj], A = P.A[ti][tj], al = P.alpha[ti][tj];
+    const double t1 = A * exp(-al * r);
+    const double val = (1 + Q / r) * t1;
     if (V != 0.0) {
-      double der = -t1 * (Q + al * r * r + al * r * Q) / (r * r);
-      sink.pair(i, j, p.u * (der * f * V));
-      if (p.df != 0.0) sink.pair(i, j, p.u * ((val * V) * p.df));
+      const double der = -t1 * (Q + al * r * r + al * r * Q) / (r * r);
+      sink.pair(i, j, p.u * Real(der * dbl(f) * dbl(V)));
+      if (p.df != 0.0) sink.pair(i, j, p.u * Real((val * dbl(V)) * dbl(p.df)));
     }
-    return f * val;
+    return Real(dbl(f) * val);
   }
   template <class S>
-  MDG_HD double VA(int i, int j, const PairG& p, double V, S& sink) const
+  MDG_HD Real VA(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
   {
-    double f = p.f;
+    const Real f = p.f;
     if (f == 0.0) return 0.0;
     int ti = type(i), tj = type(j);
-    double r = p.r;
-    double t1 = P.B[0][ti][tj] * exp(-P.beta[0][ti][tj] * r);
-    double t2 = P.B[1][ti][tj] * exp(-P.beta[1][ti][tj] * r);
-    double t3 = P.B[2][ti][tj] * exp(-P.beta[2][ti][tj] * r);
-    double val = t1 + t2 + t3;
+    const double r = p.rd;
+    const double t1 = P.B[0][ti][tj] * exp(-P.beta[0][ti][tj] * r);
+    const double t2 = P.B[1][ti][tj] * exp(-P.beta[1][ti][tj] * r);
+    const double t3 = P.B[2][ti][tj] * exp(-P.beta[2][ti][tj] * r);
+    const double val = t1 + t2 + t3;
     if (V != 0.0) {
-      double der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
-      sink.pair(i, j, p.u * (-der * f * V));
-      if (p.df != 0.0) sink.pair(i, j, p.u * ((-val * V) * p.df));
+      const double der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
+      sink.pair(i, j, p.u * Real(-der * dbl(f) * dbl(V)));
+      if (p.df != 0.0) sink.pair(i, j, p.u * Real((-val * dbl(V)) * dbl(p.df)));
     }
-    return -f * val;
+    return Real(-dbl(f) * val);
   }
 
   // One REBO bond i < j (REBO::operator(), REBO.cxx:43-59): returns its energy.
   template <class S>
-  MDG_HD double bond(int i, int j, const PairG& p, S& sink) const
+  MDG_HD Real bond(int i, int j, const PairGT<Real>& p, S& sink) const
   {
-    Sink dummy;
-    double vav = VA(i, j, p, 0.0, dummy);
-    double E = VR(i, j, p, 1.0, sink);
+    SinkT<Real> dummy;
+    Real vav = VA(i, j, p, 0.0, dummy);
+    Real E = VR(i, j, p, 1.0, sink);
     if (vav != 0.0) {
-      double bav = baver(i, j, p, vav, sink);
+      Real bav = baver(i, j, p, vav, sink);
       E += bav * VA(i, j, p, bav, sink);
     }
     return E;
   }
 };
+typedef ReboT<double, ReboTables> Rebo;
 
 // Pair record of bond slot q of atom c (the pair c -> partner).
-MDG_HD PairG pair_from_slot(const BondList& B, int q)
+template <class Real = double>
+MDG_HD PairGT<Real> pair_from_slot(const BondList& B, int q)
 {
-  PairG p;
+  PairGT<Real> p;
   double4 rv = B.brv[q], u = B.bu[q], d = B.bd[q];
-  p.rv = v3(rv.x, rv.y, rv.z);
-  p.u = v3(u.x, u.y, u.z);
+  p.rv = xyz<Real>(rv);
+  p.u = xyz<Real>(u);
   p.r = rv.w;
+  p.rd = rv.w;
   p.f = u.w;
   p.df = d.x;
   p.ralt = 0.0;

@@ -41,7 +41,8 @@ MDG_HD double ipow(double a, int n)
 struct GSpline {
   int npieces;
   int pad;
-  double x2[4];
+  double x1[4];   // lower knot of each piece
+  double x2[4];   // upper knot
   double f[4][6];
   double df[4][6];
 };
@@ -175,6 +176,124 @@ MDG_HD double t_value(const ReboTables& tb, int fam, double i, double j, double 
   int ii = (int)i, jj = (int)j, kk = (int)k;
   if ((double)ii == i && (double)jj == j && (double)kk == k) return tb.Tint[fam][ii][jj][kk][0];
   return poly3(tb.T[fam][ii][jj][kk][0], i, j, k, 0);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 tables of the mixed-precision path.  The FP64 tables above keep the
+// reference's monomials in absolute coordinates, whose terms cancel to ~1e-7
+// of their magnitude (sum |terms| ~3e6 in the pi_rc cells): float cannot
+// carry that.  Here every cell polynomial is re-expanded about the cell's
+// lower corner (a Taylor shift done in long double on the host) and evaluated
+// by Horner's rule in local coordinates u = x - corner, u in [0, 1) on the
+// bicubic/tricubic grids.  The functions are the same polynomials; only the
+// basis and the rounding differ.
+struct GSpline32 {
+  int npieces;
+  int pad;
+  float x1[4];    // expansion point of each piece (its lower knot)
+  float x2[4];    // upper knots
+  float f[4][6];  // value poly in u = x - x1, coefficient of u^t
+  float df[4][6]; // derivative poly in u
+};
+
+struct ReboTables32 {
+  GSpline32 G[3];
+  float P[2][4][4][3][16];      // cell [h][c], poly f/dH/dC: d[a + 4b] u^a v^b
+  float Pint[2][4][4][3];
+  float T[4][5][5][16][4][64];  // cell [i][j][k], poly f/di/dj/dk: d[a + 4b + 16c] u^a v^b w^c
+  float Tint[4][5][5][16][4];
+};
+
+MDG_HD float horner6(const float* c, float u)
+{
+  float v = c[5];
+  for (int t = 4; t >= 0; t--) v = fmaf(v, u, c[t]);
+  return v;
+}
+MDG_HD float horner4(const float* c, float u)
+{
+  return fmaf(fmaf(fmaf(c[3], u, c[2]), u, c[1]), u, c[0]);
+}
+MDG_HD float local2(const float* d, float u, float v)
+{
+  return horner4(d + 12, u) * v * v * v + horner4(d + 8, u) * v * v + horner4(d + 4, u) * v + horner4(d, u);
+}
+MDG_HD float local3(const float* d, float u, float v, float w)
+{
+  float r = 0.0f;
+  for (int c = 3; c >= 0; c--) {
+    const float* e = d + 16 * c;
+    float s = fmaf(fmaf(fmaf(horner4(e + 12, u), v, horner4(e + 8, u)), v, horner4(e + 4, u)), v, horner4(e, u));
+    r = fmaf(r, w, s);
+  }
+  return r;
+}
+
+MDG_HD f32 g_eval(const GSpline32& g, f32 cost, int deriv)
+{
+  int p = 0;
+  for (p = 0; p < g.npieces; p++)
+    if (cost.v <= g.x2[p]) break;
+  if (p >= g.npieces) p = g.npieces - 1;
+  return mkf(horner6(deriv ? g.df[p] : g.f[p], cost.v - g.x1[p]));
+}
+
+MDG_HD void p_eval(const ReboTables32& tb, int fam, f32 h, f32 c, f32& v, f32& dh, f32& dc, unsigned int* status)
+{
+  v = dh = dc = 0.0;
+  if (!(h.v >= 0 && c.v >= 0)) { if (status) *status |= ST_SPLINE_DOMAIN; return; }
+  if (h.v >= 4 || c.v >= 4) return;
+  int hi = (int)h.v, ci = (int)c.v;
+  if ((float)hi == h.v && (float)ci == c.v) {
+    v = tb.Pint[fam][hi][ci][0];
+    dh = tb.Pint[fam][hi][ci][1];
+    dc = tb.Pint[fam][hi][ci][2];
+    return;
+  }
+  const float* cell = tb.P[fam][hi][ci][0];
+  const float u = h.v - hi, w = c.v - ci;
+  v = mkf(local2(cell, u, w));
+  dh = mkf(local2(cell + 16, u, w));
+  dc = mkf(local2(cell + 32, u, w));
+}
+
+MDG_HD f32 p_value(const ReboTables32& tb, int fam, f32 h, f32 c)
+{
+  if (!(h.v >= 0 && c.v >= 0)) return 0.0;
+  if (h.v >= 4 || c.v >= 4) return 0.0;
+  int hi = (int)h.v, ci = (int)c.v;
+  if ((float)hi == h.v && (float)ci == c.v) return tb.Pint[fam][hi][ci][0];
+  return mkf(local2(tb.P[fam][hi][ci][0], h.v - hi, c.v - ci));
+}
+
+MDG_HD void t_eval(const ReboTables32& tb, int fam, f32 i, f32 j, f32 k, f32* out, unsigned int* status)
+{
+  out[0] = out[1] = out[2] = out[3] = 0.0;
+  if (!(i.v >= 0 && j.v >= 0 && k.v >= 1)) { if (status) *status |= ST_SPLINE_DOMAIN; return; }
+  if (i.v >= 4 || j.v >= 4) return;
+  float kc = k.v > 15 ? 15.0f : k.v;
+  int ii = (int)i.v, jj = (int)j.v, kk = (int)kc;
+  if ((float)ii == i.v && (float)jj == j.v && (float)kk == kc) {
+    const float* t = tb.Tint[fam][ii][jj][kk];
+    out[0] = t[0]; out[1] = t[1]; out[2] = t[2]; out[3] = t[3];
+    return;
+  }
+  const float* cell = tb.T[fam][ii][jj][kk][0];
+  const float u = i.v - ii, v = j.v - jj, w = kc - kk;
+  out[0] = mkf(local3(cell, u, v, w));
+  out[1] = mkf(local3(cell + 64, u, v, w));
+  out[2] = mkf(local3(cell + 128, u, v, w));
+  out[3] = mkf(local3(cell + 192, u, v, w));
+}
+
+MDG_HD f32 t_value(const ReboTables32& tb, int fam, f32 i, f32 j, f32 k)
+{
+  if (!(i.v >= 0 && j.v >= 0 && k.v >= 1)) return 0.0;
+  if (i.v >= 4 || j.v >= 4) return 0.0;
+  float kc = k.v > 15 ? 15.0f : k.v;
+  int ii = (int)i.v, jj = (int)j.v, kk = (int)kc;
+  if ((float)ii == i.v && (float)jj == j.v && (float)kk == kc) return tb.Tint[fam][ii][jj][kk][0];
+  return mkf(local3(tb.T[fam][ii][jj][kk][0], i.v - ii, j.v - jj, kc - kk));
 }
 
 }  // namespace mdg

@@ -275,11 +275,13 @@ struct BondTasks {
 
 MDG_HD int bond_rec_size(int nb) { return 5 + 4 * nb; }
 
-MDG_HD void rebo_task(const Rebo& R, const TorsParams& TP, int do_rebo, int do_tors, double* rec, int a, int s)
+template <class Real, class TB>
+MDG_HD void rebo_task(const ReboT<Real, TB>& R, const TorsParams& TP, int do_rebo, int do_tors, double* rec, int a,
+                      int s)
 {
   const BondList& B = R.B;
   const int nb = B.nb[a];
-  Sink sink;
+  SinkT<Real> sink;
   sink.a = a;
   sink.g = v3(0, 0, 0);
   sink.A = rec + 5;
@@ -287,17 +289,17 @@ MDG_HD void rebo_task(const Rebo& R, const TorsParams& TP, int do_rebo, int do_t
   for (int t = 0; t < 4 * nb; t++) sink.A[t] = 0.0;  // A and W are contiguous
   const int q = a * B.mb + s;
   const int b = B.bj[q];
-  PairG p = pair_from_slot(B, q);
+  PairGT<Real> p = pair_from_slot<Real>(B, q);
   int lo = a, hi = b;
   if (b < a) { lo = b; hi = a; p = pair_reverse(p); }
   double er = 0.0, et = 0.0;
   if (do_rebo) {
-    double E = R.bond(lo, hi, p, sink);
-    if (a == lo) er = E;
+    const Real E = R.bond(lo, hi, p, sink);
+    if (a == lo) er = dbl(E);
   }
   if (do_tors) {
-    double E = etors_bond(R, TP, lo, hi, p, sink);
-    if (a == lo) et = E;
+    const Real E = etors_bond(R, TP, lo, hi, p, sink);
+    if (a == lo) et = dbl(E);
   }
   rec[0] = sink.g.x;
   rec[1] = sink.g.y;

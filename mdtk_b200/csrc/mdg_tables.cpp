@@ -386,6 +386,7 @@ void put_g(const GKnot* kn, int nknots, GSpline& gs, std::vector<double>& flat)
       std::vector<double> f, df;
       emit(P, 0, f);
       emit(P, 1, df);
+      gs.x1[p] = x[0];
       gs.x2[p] = x[1];
       flat.push_back(x[0]);
       flat.push_back(x[1]);
@@ -575,6 +576,92 @@ void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out)
   put_t(kTij, sizeof(kTij) / sizeof(kTij[0]), tb->T[3], tb->Tint[3], flat, tint[3]);
   for (int f = 0; f < 4; f++) flat.insert(flat.end(), tint[f].begin(), tint[f].end());
   if (flat_out) *flat_out = flat;
+}
+
+// ---- FP32 local-basis tables (ReboTables32) ----
+namespace {
+
+long double binom(int n, int k)
+{
+  long double r = 1.0L;
+  for (int q = 1; q <= k; q++) r = r * (n - k + q) / q;
+  return r;
+}
+
+long double lpow(long double x, int n)
+{
+  long double r = 1.0L;
+  for (int q = 0; q < n; q++) r *= x;
+  return r;
+}
+
+// Taylor shift of sum_t c_t prod_d x_d^e_d(t) (the term enumeration of the
+// FP64 tables, x0 fastest; `deriv` lowers the exponent of that coordinate as
+// the derivative polynomials do) to local coordinates u_d = x_d - x0_d.
+void shift_poly(const double* c, int nterms, int ndim, int deriv, const double* x0, float* out)
+{
+  long double acc[64];
+  const int nout = ndim == 1 ? 6 : (ndim == 2 ? 16 : 64);
+  for (int i = 0; i < nout; i++) acc[i] = 0.0L;
+  for (int t = 0; t < nterms; t++) {
+    if (c[t] == 0.0) continue;
+    int e[3] = {0, 0, 0};
+    if (ndim == 1) e[0] = t;
+    else if (ndim == 2) { e[0] = t & 3; e[1] = t >> 2; }
+    else { e[0] = t & 3; e[1] = (t >> 2) & 3; e[2] = t >> 4; }
+    if (deriv) e[deriv - 1] -= 1;
+    if (e[0] < 0 || e[1] < 0 || e[2] < 0) continue;
+    for (int k0 = 0; k0 <= e[0]; k0++)
+      for (int k1 = 0; k1 <= e[1]; k1++)
+        for (int k2 = 0; k2 <= e[2]; k2++) {
+          long double w = (long double)c[t] * binom(e[0], k0) * lpow(x0[0], e[0] - k0);
+          if (ndim > 1) w *= binom(e[1], k1) * lpow(x0[1], e[1] - k1);
+          if (ndim > 2) w *= binom(e[2], k2) * lpow(x0[2], e[2] - k2);
+          const int idx = ndim == 1 ? k0 : (ndim == 2 ? k0 + 4 * k1 : k0 + 4 * k1 + 16 * k2);
+          acc[idx] += w;
+        }
+  }
+  for (int i = 0; i < nout; i++) out[i] = (float)acc[i];
+}
+
+}  // namespace
+
+void build_rebo_tables32(const ReboTables& d, ReboTables32* f)
+{
+  std::memset(f, 0, sizeof(*f));
+  for (int g = 0; g < 3; g++) {
+    const GSpline& a = d.G[g];
+    GSpline32& b = f->G[g];
+    b.npieces = a.npieces;
+    for (int p = 0; p < 4; p++) {
+      b.x1[p] = (float)a.x1[p];
+      b.x2[p] = (float)a.x2[p];
+      if (p >= a.npieces) continue;
+      // expand about the float-rounded knot, the point the device subtracts
+      const double x0 = (double)b.x1[p];
+      shift_poly(a.f[p], 6, 1, 0, &x0, b.f[p]);
+      shift_poly(a.df[p], 6, 1, 1, &x0, b.df[p]);
+    }
+  }
+  for (int fam = 0; fam < 2; fam++)
+    for (int h = 0; h < 4; h++)
+      for (int c = 0; c < 4; c++) {
+        const double x0[2] = {(double)h, (double)c};
+        for (int q = 0; q < 3; q++) {
+          shift_poly(d.P[fam][h][c][q], 16, 2, q, x0, f->P[fam][h][c][q]);
+          f->Pint[fam][h][c][q] = (float)d.Pint[fam][h][c][q];
+        }
+      }
+  for (int fam = 0; fam < 4; fam++)
+    for (int i = 0; i < 5; i++)
+      for (int j = 0; j < 5; j++)
+        for (int k = 0; k < 16; k++) {
+          const double x0[3] = {(double)i, (double)j, (double)k};
+          for (int q = 0; q < 4; q++) {
+            shift_poly(d.T[fam][i][j][k][q], 64, 3, q, x0, f->T[fam][i][j][k][q]);
+            f->Tint[fam][i][j][k][q] = (float)d.Tint[fam][i][j][k][q];
+          }
+        }
 }
 
 }  // namespace mdg

@@ -11,6 +11,10 @@ namespace mdg {
 // the tables flattened in the oracle's export order (for the bitwise check).
 void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out);
 
+// FP32 tables of the mixed-precision path: the same cell polynomials
+// re-expanded about each cell's lower corner, rounded to float.
+void build_rebo_tables32(const ReboTables& d, ReboTables32* f);
+
 struct BrennerTables;
 // Brenner H_CC / H_CH / F tables of parameter set 1 or 2, same layout rules.
 void build_brenner_tables(int set, BrennerTables* tb, std::vector<double>* flat_out);

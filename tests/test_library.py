@@ -62,6 +62,33 @@ def test_create_rejects_lj_without_rebo():
     assert e.value.code == -1
 
 
+def test_create_rejects_mixed_brenner():
+    # checked before any device work, so it runs without a GPU
+    with pytest.raises(M.MdgError) as e:
+        M.Context(potentials=M.POT_BRENNER, precision=M.PREC_FP32_MIXED)
+    assert e.value.code == -1
+
+
+@pytest.mark.parametrize("kind,nfam", [(0, 3), (1, 2), (2, 4)])
+def test_fp32_spline_tables_match_fp64(kind, nfam):
+    # The FP32 tables re-expand every cell about its corner; over the domain
+    # they agree with the FP64 (reference-order) evaluation to a few float ulps
+    # of each family's scale.
+    rng = np.random.default_rng(kind)
+    n = 4000
+    if kind == 0:
+        a = rng.uniform(-1, 1, (n, 1))
+    elif kind == 1:
+        a = rng.uniform(0, 4, (n, 2))
+    else:
+        a = np.column_stack([rng.uniform(0, 4, n), rng.uniform(0, 4, n), rng.uniform(1, 12, n)])
+    for fam in range(nfam):
+        d = M.debug_spline(M.PREC_FP64, kind, fam, a)
+        f = M.debug_spline(M.PREC_FP32_MIXED, kind, fam, a)
+        scale = np.maximum(np.abs(d).max(axis=0), 1e-30)
+        assert np.all(np.abs(f - d).max(axis=0) <= 5e-6 * scale), (kind, fam)
+
+
 def _has_gpu():
     try:
         import torch
