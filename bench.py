@@ -32,6 +32,8 @@ sys.path.insert(0, ROOT)
 METRIC = "atom-steps/s on 1 B200: FP64 plain vs FP32-mixed/batched at ≤1e-5 force err"
 N_MOL = 5461
 DT_FS = 0.25
+BATCH_SYSTEMS = 256
+BATCH_DT_FS = 0.2
 WORKLOAD = (f"FP64 AIREBO ethane liquid: {N_MOL} C2H6 ({8 * N_MOL} atoms), 0.55 g/cm^3, 300 K, "
             f"dt {DT_FS} fs, reference cutoffs and 0.44 Rcut skin")
 
@@ -306,6 +308,44 @@ def main():
                  "scope": "FP32 bond orders (REBO, torsion) and plain LJ pairs; FP64 pair exponentials, LJ "
                           "powers and switches, b* of close non-bonded pairs, accumulation, integration"}
 
+    # Batched variant: 256 independent cluster-impact systems of uneven size
+    # (AB graphite slabs of 800-6000 atoms, lateral PBC, open z, fixed bottom
+    # layer, a 13-atom C cluster at 10-100 eV), FP32-mixed AIREBO, dt 0.2 fs,
+    # all systems advanced by the same launches.
+    batched = None
+    if not args.no_variants:
+        from mdtk_b200 import builders as B
+        systems = B.impact_batch(BATCH_SYSTEMS, seed=1 + 1000 * rank)
+        bx = M.Context(potentials=M.POT_AIREBO, precision=M.PREC_FP32_MIXED, device=local)
+        bx.set_batch(systems)
+        bx.set_stream(stream.cuda_stream)
+        nb_atoms = bx.n
+        bx.run(max(args.warmup, 3), BATCH_DT_FS, energies=False)
+        bx.sync()
+        kb = min(args.steps, 50)
+        evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kb)]
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(kb):
+            flush.zero_()
+            evb[k][0].record(stream)
+            bx.run(1, BATCH_DT_FS, energies=False)
+            evb[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        b_ms = sum(a.elapsed_time(b) for a, b in evb)
+        if dist is not None:
+            t = torch.tensor([b_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            b_ms = float(t.item())
+        bx.sync()
+        batched = {"value": world * nb_atoms * kb / (b_ms * 1e-3), "unit": "atom-steps/s", "steps": kb,
+                   "ms_per_step": b_ms / kb, "systems": BATCH_SYSTEMS, "atoms": nb_atoms,
+                   "precision": "fp32-mixed", "dt_fs": BATCH_DT_FS,
+                   "workload": "cluster impacts: AB graphite slabs 800-6000 atoms (lateral PBC, open z, fixed "
+                               "bottom layer) + 13-atom C cluster at 10-100 eV, AIREBO"}
+        del bx
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
@@ -316,7 +356,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches, "clocks": clk, "kernels": kern, "roofline": roof, "e2e": e2e,
             "fp64_peak_tflops": fp64_peak,
-            "variants": {"fp32_mixed": mixed},
+            "variants": {"fp32_mixed": mixed, "batched": batched},
         }
         if world == 1 and not args.no_cpu_baseline:
             try:

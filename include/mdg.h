@@ -185,6 +185,25 @@ int mdg_pipe_peak(int device, int fp32, double* tflops);
 int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const double box[3], const int32_t pbc[3],
                              int with_torsion, double* energy, double* grad, void* stream);
 
+/* ---- Batched systems ----
+ * Many independent systems of uneven size in one context (the reference runs
+ * impacts one after another, mdtrajsim/main.cpp:295-345): atoms of system s
+ * are [first[s], first[s+1]) of the concatenated arrays, its box and
+ * periodicity are box[3s..3s+2] and pbc[3s..3s+2].  Every kernel of a step
+ * covers all systems in one launch; lists, bonds and forces never cross
+ * systems.  mdg_compute, mdg_run, mdg_get_state/mdg_set_state work on the
+ * concatenated arrays; the energies below are per system. */
+int mdg_set_batch(mdg_ctx* ctx, int nsys, const int64_t* first, const int32_t* z, const double* pos,
+                  const double* vel, const double* box, const int32_t* pbc, const uint8_t* fixed);
+
+/* Per-system energies at the current state: e_sys[4 s + {0,1,2,3}] = REBO,
+ * LJ, torsion, kinetic. */
+int mdg_batch_energies(mdg_ctx* ctx, double* e_sys);
+
+/* mdg_run for a batched context with per-system energies: epot/etot
+ * [nsteps * nsys] (step-major), either may be NULL. */
+int mdg_batch_run(mdg_ctx* ctx, int nsteps, double dt, double* epot, double* etot);
+
 /* Test hook: the REBO spline tables the library built on the host, flattened
  * in the oracle's export order; returns the number of doubles (writes at most
  * cap).  Host only; needs no device. */

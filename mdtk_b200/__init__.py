@@ -82,6 +82,10 @@ def lib():
         L.mdg_compute.argtypes = [vp, dp, dp, dp]
         L.mdg_nl_pairs.argtypes = [vp, ctypes.c_int, i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
         L.mdg_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
+        L.mdg_set_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), i32p, dp, dp, dp, i32p,
+                                    ctypes.POINTER(ctypes.c_uint8)]
+        L.mdg_batch_energies.argtypes = [vp, dp]
+        L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_sync.argtypes = [vp]
         L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
         L.mdg_launch_count.argtypes = [vp]
@@ -192,6 +196,36 @@ class Context:
             fx = fixed.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
         _check(lib().mdg_set_system(self.h, len(z), _ip(z), _dp(pos), _dp(vel), _dp(box), _ip(pbc), fx))
         self.n = len(z)
+
+    def set_batch(self, systems):
+        """Load independent systems (dicts as the builders return) into one
+        batched context; atoms are concatenated in list order."""
+        self.first = np.zeros(len(systems) + 1, dtype=np.int64)
+        self.first[1:] = np.cumsum([len(s["z"]) for s in systems])
+        z = np.ascontiguousarray(np.concatenate([s["z"] for s in systems]), dtype=np.int32)
+        pos = np.ascontiguousarray(np.concatenate([s["pos"] for s in systems]), dtype=np.float64)
+        vel = np.ascontiguousarray(np.concatenate([s["vel"] for s in systems]), dtype=np.float64)
+        box = np.ascontiguousarray(np.concatenate([np.asarray(s["box"], float) for s in systems]))
+        pbc = np.ascontiguousarray(np.concatenate([np.asarray(s["pbc"]) for s in systems]), dtype=np.int32)
+        fixed = np.ascontiguousarray(np.concatenate([s["fixed"] for s in systems]), dtype=np.uint8)
+        _check(lib().mdg_set_batch(self.h, len(systems), self.first.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                   _ip(z), _dp(pos), _dp(vel), _dp(box), _ip(pbc),
+                                   fixed.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        self.n = len(z)
+        self.nsys = len(systems)
+
+    def batch_energies(self) -> np.ndarray:
+        """[nsys, 4]: REBO, LJ, torsion, kinetic energy of each system."""
+        out = np.zeros((self.nsys, 4))
+        _check(lib().mdg_batch_energies(self.h, _dp(out)))
+        return out
+
+    def batch_run(self, nsteps: int, dt: float):
+        """Steps every system; returns (epot, etot) as [nsteps, nsys]."""
+        ep = np.zeros((nsteps, self.nsys))
+        et = np.zeros((nsteps, self.nsys))
+        _check(lib().mdg_batch_run(self.h, nsteps, dt, _dp(ep), _dp(et)))
+        return ep, et
 
     def set_state(self, pos, vel=None):
         pos = np.ascontiguousarray(pos, dtype=np.float64)

@@ -273,3 +273,53 @@ def graphite_slab(n_layers: int, nx: int, ny: int, cc: float = 1.42, interlayer:
     rng = np.random.default_rng(seed)
     vel = thermal_velocities(z, temp_k, rng, fixed)
     return _system(z, pos, vel, box, [1, 1, 0], fixed)
+
+
+def impact(seed: int, n_target: int = None, e_min_ev: float = 10.0, e_max_ev: float = 100.0,
+           temp_k: float = 0.0, cluster_atoms: int = 13) -> Dict[str, np.ndarray]:
+    """One cluster-impact system: an AB graphite slab of about n_target atoms
+    (uniform in [800, 6000] when not given; whole layers x lateral repeats,
+    lateral periods >= 11 A so that checkMIC(2 x 5.5 A) holds), z open,
+    bottom layer fixed, and a random C cluster (min separation 1.3 A) 8 A
+    above the top layer moving straight down with kinetic energy uniform in
+    [e_min_ev, e_max_ev] (AtomsArray::setTranslationalEnergy,
+    mdtk/AtomsContainer.cxx:313-323: every cluster atom gets the same
+    velocity)."""
+    rng = np.random.default_rng(seed)
+    if n_target is None:
+        n_target = int(rng.integers(800, 6001))
+    n_layers = int(rng.integers(2, 7))
+    cells = max(1.0, n_target / (4.0 * n_layers))
+    ny = max(3, int(round(math.sqrt(cells * 2.46 / 4.26))))
+    nx = max(5, int(round(cells / ny)))
+    slab = graphite_slab(n_layers, nx, ny, temp_k=temp_k, seed=seed)
+    box = slab["box"]
+    top = slab["pos"][:, 2].max()
+    # cluster: rejection sampling in a ball
+    cl = []
+    radius = 2.6
+    while len(cl) < cluster_atoms:
+        p = rng.uniform(-radius, radius, 3)
+        if np.linalg.norm(p) > radius:
+            continue
+        if all(np.linalg.norm(p - q) >= 1.3 for q in cl):
+            cl.append(p)
+    cl = np.array(cl)
+    centre = np.array([rng.uniform(0, box[0]), rng.uniform(0, box[1]), top + 8.0])
+    cl = cl - cl.mean(axis=0) + centre
+    cl[:, 2] = np.maximum(cl[:, 2], top + 8.0 - radius)
+    cl[:, 0] = np.mod(cl[:, 0], box[0])
+    cl[:, 1] = np.mod(cl[:, 1], box[1])
+    e_kin = rng.uniform(e_min_ev, e_max_ev)
+    m_tot = 12.0 * cluster_atoms
+    v = math.sqrt(2.0 * e_kin / m_tot * EV_PER_AMU_A2FS2)
+    z = np.concatenate([slab["z"], np.full(cluster_atoms, 6, np.int32)])
+    pos = np.concatenate([slab["pos"], cl])
+    vel = np.concatenate([slab["vel"], np.tile([0.0, 0.0, -v], (cluster_atoms, 1))])
+    fixed = np.concatenate([slab["fixed"], np.zeros(cluster_atoms, np.uint8)])
+    return _system(z, pos, vel, box, [1, 1, 0], fixed)
+
+
+def impact_batch(n_systems: int, seed: int = 0, **kw):
+    """n_systems independent impact systems of uneven size (seeds seed, seed+1, ...)."""
+    return [impact(seed + k, **kw) for k in range(n_systems)]

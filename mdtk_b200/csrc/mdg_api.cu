@@ -101,7 +101,7 @@ __global__ void k_cell_count(State S, Grid g, const int* need)
 {
   if (!*need) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < S.n) atomicAdd(&g.ccount[cell_of(g, S.box, S.pos[i])], 1);
+  if (i < S.n) atomicAdd(&g.ccount[cell_of(g, S, i)], 1);
 }
 
 // single-block exclusive scan of the cell counts
@@ -131,7 +131,7 @@ __global__ void k_cell_fill(State S, Grid g, const int* need)
   if (!*need) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
-  int c = cell_of(g, S.box, S.pos[i]);
+  int c = cell_of(g, S, i);
   int slot = atomicAdd(&g.ccursor[c], 1);
   g.catoms[g.cstart[c] + slot] = i;
 }
@@ -320,42 +320,73 @@ __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
 
-// Plain LJ pairs, one warp per atom: lanes stride the atom's LJ list;
-// pairs that need b*_ij or a connectivity gradient are compacted, in list
-// order, into the atom's special list.
+// Plain LJ pairs, one warp per atom.  Only ~1/4 of an LJ-list entry is
+// inside the pair's cutoff, so the warp first filters 32 entries at a time
+// (position load + distance) and appends the survivors, in list order, to a
+// per-warp queue in shared memory; every 32 queued pairs are then evaluated
+// with all lanes busy.  Pairs that need b*_ij or a connectivity gradient are
+// compacted, in list order, into the atom's special list.
 template <class Real>
-__global__ void k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* nbonds, ForceOut O,
-                           SpecialTasks Tk, unsigned int* status)
+__global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, State S, NList L,
+                                                       const int* nbonds, ForceOut O, SpecialTasks Tk,
+                                                       unsigned int* status)
 {
+  __shared__ int queue[kThreads / 32][64];
   const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (a >= S.n) return;
+  if (a >= S.n) return;  // whole warps
+  int* q = queue[threadIdx.x >> 5];
   const double4 pa = S.pos[a];
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
+  const Box& box = box_of(S, a);
   const int cnt = L.cnt[a];
   const int* lst = L.list + (long)a * L.cap;
+  const unsigned below = (1u << lane) - 1u;
   SinkT<Real> sk;
   sk.a = a;
   sk.g = v3(0, 0, 0);
   sk.A = nullptr;
   sk.W = nullptr;
   double e = 0.0;
-  int nsp = 0;
-  for (int base = 0; base < cnt; base += 32) {
-    const int s = base + lane;
+  int nsp = 0, qn = 0;
+  auto evaluate = [&](int nq) {
     int kind = 0, b = -1;
-    if (s < cnt) {
-      b = lst[s];
+    if (lane < nq) {
+      b = q[lane];
       kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
     }
     const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
     if (kind == 2) {
-      const int pos = nsp + __popc(m & ((1u << lane) - 1u));
+      const int pos = nsp + __popc(m & below);
       if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
     }
     nsp += __popc(m);
+  };
+  for (int base = 0; base < cnt; base += 32) {
+    const int s = base + lane;
+    bool in = false;
+    int b = -1;
+    if (s < cnt) {
+      b = lst[s];
+      const double4 pb = S.pos[b];
+      const double R2 = P.R[ta][(int)pb.w][1];
+      const V3 rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
+      in = !(norm2(rv) > R2 * R2);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (in) q[qn + __popc(m & below)] = b;
+    qn += __popc(m);
+    __syncwarp();
+    if (qn >= 32) {
+      evaluate(32);
+      __syncwarp();
+      if (lane < qn - 32) q[lane] = q[lane + 32];
+      __syncwarp();
+      qn -= 32;
+    }
   }
+  if (qn > 0) evaluate(qn);
   double gx = sk.g.x, gy = sk.g.y, gz = sk.g.z;
   for (int o = 16; o > 0; o >>= 1) {
     gx += __shfl_xor_sync(0xffffffffu, gx, o);
@@ -563,6 +594,36 @@ __global__ void k_reduce_final(const double* part, int nparts, int narr, double*
   if (!isfinite(s)) atomicOr(status, ST_NONFINITE);
 }
 
+// Per-system energy sums of a batched context: one block per system; each
+// thread sums a strided share of the system's atoms, then a fixed tree
+// (deterministic).  out[4 s + {0,1,2,3}] = REBO, LJ, torsion, kinetic.
+__global__ void k_sys_energy(const int64_t* first, const double* er, const double* el, const double* et,
+                             const double* ek, double* out, unsigned int* status)
+{
+  __shared__ double sh[4][kThreads];
+  const int sy = blockIdx.x;
+  const int64_t b = first[sy], e = first[sy + 1];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+    acc[0] += er[i];
+    acc[1] += el[i];
+    acc[2] += et[i];
+    acc[3] += ek[i];
+  }
+  for (int q = 0; q < 4; q++) sh[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int q = 0; q < 4; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) {
+    const double v = sh[threadIdx.x][0];
+    out[4 * sy + threadIdx.x] = v;
+    if (!isfinite(v)) atomicOr(status, ST_NONFINITE);
+  }
+}
+
 __global__ void k_finite(const double4* g, int n, unsigned int* status)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -626,6 +687,17 @@ struct mdg_ctx {
 
   int n = 0;
   Box box;
+  // batched context: nsys independent systems, atoms [first[s], first[s+1])
+  int nsys = 1;
+  std::vector<int64_t> h_first;
+  std::vector<Box> h_boxes;
+  std::vector<int> h_sys;
+  int* d_sys = nullptr;
+  Box* d_boxes = nullptr;
+  int64_t* d_first = nullptr;
+  int4* d_snc[2] = {nullptr, nullptr};
+  double4* d_slo[2] = {nullptr, nullptr};
+  double4* d_scs[2] = {nullptr, nullptr};
   double unit_len = 1.0, unit_vel = 1.0, unit_e = 1.0, unit_grad = 1.0;
 
   // state
@@ -652,7 +724,7 @@ struct mdg_ctx {
   double* d_red_part = nullptr;
   double* d_energy = nullptr;   // [4] rebo, lj, tors, kin of the last evaluation
   double* d_elog = nullptr;     // per-step energy log [cap * 4]
-  int elog_cap = 0;
+  int64_t elog_cap = 0;
 
   CijTable cij;
   SpecialTasks spc;
@@ -683,6 +755,8 @@ struct mdg_ctx {
     State s;
     s.n = n;
     s.box = box;
+    s.sys = nsys > 1 ? d_sys : nullptr;
+    s.boxes = nsys > 1 ? d_boxes : nullptr;
     s.pos = pos;
     s.vel = vel;
     s.acc = acc;
@@ -817,6 +891,18 @@ void free_system(mdg_ctx* c)
     if (p) cudaFree(p);
   std::memset(&c->cij, 0, sizeof(c->cij));
   std::memset(&c->spc, 0, sizeof(c->spc));
+  void* sq[] = {c->d_sys, c->d_boxes, c->d_first, c->d_snc[0], c->d_snc[1], c->d_slo[0], c->d_slo[1],
+                c->d_scs[0], c->d_scs[1]};
+  for (void* p : sq)
+    if (p) cudaFree(p);
+  c->d_sys = nullptr;
+  c->d_boxes = nullptr;
+  c->d_first = nullptr;
+  for (int l = 0; l < 2; l++) { c->d_snc[l] = nullptr; c->d_slo[l] = nullptr; c->d_scs[l] = nullptr; }
+  c->nsys = 1;
+  c->h_first.clear();
+  c->h_boxes.clear();
+  c->h_sys.clear();
   void* bq[] = {c->bt.q, c->bt.ctr, c->bt.rbase, c->bt.rec};
   for (void* p : bq)
     if (p) cudaFree(p);
@@ -872,6 +958,65 @@ int setup_grid(mdg_ctx* c, int l, const std::vector<double>& hpos)
   g.ccursor = dalloc<int>(nc);
   g.catoms = dalloc<int>(c->n);
   if (!g.ccount || !g.cstart || !g.ccursor || !g.catoms) return fail(MDG_ERR_CUDA, "cudaMalloc (cell grid)");
+  return MDG_OK;
+}
+
+// One cell grid per system of a batched context, laid out one after another
+// (non-periodic axes span the system's atoms at set-up plus two ranges, as
+// in the single-system grid; a periodic axis may have 1 or 2 cells).
+int setup_grid_batch(mdg_ctx* c, int l, const std::vector<double>& hpos)
+{
+  Grid& g = c->grid[l];
+  const double range = std::sqrt(c->nl[l].range2);
+  g.brute = 0;
+  g.nc[0] = g.nc[1] = g.nc[2] = 1;
+  std::vector<int4> snc(c->nsys);
+  std::vector<double4> slo(c->nsys), scs(c->nsys);
+  long total = 0;
+  for (int sy = 0; sy < c->nsys; sy++) {
+    const Box& b = c->h_boxes[sy];
+    int nc[3];
+    double lo[3], cs[3];
+    for (int ax = 0; ax < 3; ax++) {
+      if (b.pbc[ax]) {
+        nc[ax] = std::max(1, (int)std::floor(b.L[ax] / range));
+        lo[ax] = 0.0;
+        cs[ax] = b.L[ax] / nc[ax];
+      } else {
+        double mn = 1e300, mx = -1e300;
+        for (int64_t i = c->h_first[sy]; i < c->h_first[sy + 1]; i++) {
+          mn = std::fmin(mn, hpos[3 * i + ax]);
+          mx = std::fmax(mx, hpos[3 * i + ax]);
+        }
+        mn -= 2 * range;
+        mx += 2 * range;
+        nc[ax] = std::min(1024, std::max(1, (int)std::floor((mx - mn) / range)));
+        lo[ax] = mn;
+        cs[ax] = (mx - mn) / nc[ax];
+      }
+    }
+    snc[sy] = make_int4(nc[0], nc[1], nc[2], (int)total);
+    slo[sy] = make_double4(lo[0], lo[1], lo[2], 0.0);
+    scs[sy] = make_double4(cs[0], cs[1], cs[2], 0.0);
+    total += (long)nc[0] * nc[1] * nc[2];
+    if (total > (1L << 26)) return fail(MDG_ERR_ARG, "cell grids too large");
+  }
+  g.ncell = (int)total;
+  g.ccount = dalloc<int>(total);
+  g.cstart = dalloc<int>(total + 1);
+  g.ccursor = dalloc<int>(total);
+  g.catoms = dalloc<int>(c->n);
+  c->d_snc[l] = dalloc<int4>(c->nsys);
+  c->d_slo[l] = dalloc<double4>(c->nsys);
+  c->d_scs[l] = dalloc<double4>(c->nsys);
+  if (!g.ccount || !g.cstart || !g.ccursor || !g.catoms || !c->d_snc[l] || !c->d_slo[l] || !c->d_scs[l])
+    return fail(MDG_ERR_CUDA, "cudaMalloc (cell grids)");
+  CK(cudaMemcpy(c->d_snc[l], snc.data(), c->nsys * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_slo[l], slo.data(), c->nsys * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_scs[l], scs.data(), c->nsys * sizeof(double4), cudaMemcpyHostToDevice));
+  g.snc = c->d_snc[l];
+  g.slo = c->d_slo[l];
+  g.scs = c->d_scs[l];
   return MDG_OK;
 }
 
@@ -1132,17 +1277,34 @@ int mdg_set_stream(mdg_ctx* c, void* stream)
   return MDG_OK;
 }
 
-int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const double* vel,
-                   const double box[3], const int32_t pbc[3], const uint8_t* fixed)
+// Loads nsys independent systems (atoms [first[s], first[s+1]) with box
+// box[3s..3s+2] and periodicity pbc[3s..3s+2]); nsys = 1 is the ordinary
+// single-system context.
+static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t* z, const double* pos,
+                       const double* vel, const double* box, const int32_t* pbc, const uint8_t* fixed)
 {
-  if (!c || n <= 0 || !z || !pos || !box || !pbc) return fail(MDG_ERR_ARG, "bad argument");
+  if (!c || nsys <= 0 || !first || !z || !pos || !box || !pbc) return fail(MDG_ERR_ARG, "bad argument");
+  if (first[0] != 0) return fail(MDG_ERR_ARG, "first[0] must be 0");
+  for (int sy = 0; sy < nsys; sy++)
+    if (!(first[sy + 1] > first[sy])) return fail(MDG_ERR_ARG, "every system needs at least one atom");
+  if (first[nsys] > (1LL << 30)) return fail(MDG_ERR_ARG, "too many atoms");
+  const int n = (int)first[nsys];
   free_system(c);
   c->n = n;
-  for (int a = 0; a < 3; a++) {
-    c->box.pbc[a] = pbc[a] ? 1 : 0;
-    c->box.L[a] = c->box.pbc[a] ? box[a] * c->unit_len : 0.0;
-    if (c->box.pbc[a] && !(c->box.L[a] > 0)) return fail(MDG_ERR_ARG, "periodic axis with non-positive period");
+  c->nsys = nsys;
+  c->h_first.assign(first, first + nsys + 1);
+  c->h_boxes.resize(nsys);
+  c->h_sys.resize(n);
+  for (int sy = 0; sy < nsys; sy++) {
+    Box& b = c->h_boxes[sy];
+    for (int a = 0; a < 3; a++) {
+      b.pbc[a] = pbc[3 * sy + a] ? 1 : 0;
+      b.L[a] = b.pbc[a] ? box[3 * sy + a] * c->unit_len : 0.0;
+      if (b.pbc[a] && !(b.L[a] > 0)) return fail(MDG_ERR_ARG, "periodic axis with non-positive period");
+    }
+    for (int64_t i = first[sy]; i < first[sy + 1]; i++) c->h_sys[i] = sy;
   }
+  c->box = c->h_boxes[0];
   // host-side packing: species, wrap (Atom::applyPBC), masses (Atom.hpp:104-105)
   std::vector<double4> hp(n), hv(n), ha(n);
   std::vector<int4> him(n);
@@ -1156,10 +1318,11 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
     else return fail(MDG_ERR_ARG, "unknown element (REBO::e2i handles only H and C)");
     double x[3];
     int im[3] = {0, 0, 0};
+    const Box& bx = c->h_boxes[c->h_sys[i]];
     for (int a = 0; a < 3; a++) {
       x[a] = pos[3 * i + a] * c->unit_len;
       if (!std::isfinite(x[a])) return fail(MDG_ERR_NONFINITE, "non-finite coordinate");
-      if (c->box.pbc[a] && !wrap1(x[a], im[a], c->box.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
+      if (bx.pbc[a] && !wrap1(x[a], im[a], bx.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
       hpos[3 * i + a] = x[a];
     }
     hp[i] = make_double4(x[0], x[1], x[2], (double)t);
@@ -1176,9 +1339,19 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
   // minimum image needs every period above twice the largest cutoff
   // (SimLoop.cxx:239-245, AtomsArray::checkMIC)
   double rmax = (c->prm.potentials & MDG_POT_AIREBO_LJ) ? c->ljp.R[0][0][1] : 2.0;
-  for (int a = 0; a < 3; a++)
-    if (c->box.pbc[a] && !(c->box.L[a] > 2.0 * rmax))
-      return fail(MDG_ERR_ARG, "Rcutoff is too large for given PBC (AtomsArray::checkMIC)");
+  for (const Box& bx : c->h_boxes)
+    for (int a = 0; a < 3; a++)
+      if (bx.pbc[a] && !(bx.L[a] > 2.0 * rmax))
+        return fail(MDG_ERR_ARG, "Rcutoff is too large for given PBC (AtomsArray::checkMIC)");
+  if (nsys > 1) {
+    c->d_sys = dalloc<int>(n);
+    c->d_boxes = dalloc<Box>(nsys);
+    c->d_first = dalloc<int64_t>(nsys + 1);
+    if (!c->d_sys || !c->d_boxes || !c->d_first) return fail(MDG_ERR_CUDA, "cudaMalloc (systems)");
+    CK(cudaMemcpy(c->d_sys, c->h_sys.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_boxes, c->h_boxes.data(), nsys * sizeof(Box), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_first, first, (nsys + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
   c->pos = dalloc<double4>(n);
   c->vel = dalloc<double4>(n);
   c->acc = dalloc<double4>(n);
@@ -1213,7 +1386,7 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
     L.list = dalloc<int>((size_t)n * L.cap);
     L.pos0 = dalloc<double4>(n);
     if (!L.cnt || !L.list || !L.pos0) return fail(MDG_ERR_CUDA, "cudaMalloc (neighbour list)");
-    int rc = setup_grid(c, l, hpos);
+    int rc = nsys > 1 ? setup_grid_batch(c, l, hpos) : setup_grid(c, l, hpos);
     if (rc) return rc;
   }
   int one[2] = {1, 1};
@@ -1304,6 +1477,20 @@ int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const
   return MDG_OK;
 }
 
+int mdg_set_system(mdg_ctx* c, int n, const int32_t* z, const double* pos, const double* vel,
+                   const double box[3], const int32_t pbc[3], const uint8_t* fixed)
+{
+  if (n <= 0) return fail(MDG_ERR_ARG, "bad argument");
+  const int64_t first[2] = {0, n};
+  return set_systems(c, 1, first, z, pos, vel, box, pbc, fixed);
+}
+
+int mdg_set_batch(mdg_ctx* c, int nsys, const int64_t* first, const int32_t* z, const double* pos,
+                  const double* vel, const double* box, const int32_t* pbc, const uint8_t* fixed)
+{
+  return set_systems(c, nsys, first, z, pos, vel, box, pbc, fixed);
+}
+
 int mdg_set_positions(mdg_ctx* c, const double* pos)
 {
   return mdg_set_state(c, pos, nullptr);
@@ -1325,7 +1512,8 @@ int mdg_set_state(mdg_ctx* c, const double* pos, const double* vel)
     for (int a = 0; a < 3; a++) {
       x[a] = pos[3 * i + a] * c->unit_len;
       if (!std::isfinite(x[a])) return fail(MDG_ERR_NONFINITE, "non-finite coordinate");
-      if (c->box.pbc[a] && !wrap1(x[a], im[a], c->box.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
+      const Box& bx = c->h_boxes[c->h_sys[i]];
+      if (bx.pbc[a] && !wrap1(x[a], im[a], bx.L[a])) return fail(MDG_ERR_ARG, "coordinate too far outside the box");
     }
     hp[i] = make_double4(x[0], x[1], x[2], old[i].w);
     him[i] = make_int4(im[0], im[1], im[2], 0);
@@ -1419,11 +1607,11 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->acc_valid = true;
   }
   const bool log = epot || etot;
-  if (log && c->elog_cap < nsteps) {
+  if (log && c->elog_cap < (int64_t)nsteps * 4) {
     if (c->d_elog) cudaFree(c->d_elog);
     c->d_elog = dalloc<double>((size_t)nsteps * 4);
     if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
-    c->elog_cap = nsteps;
+    c->elog_cap = (int64_t)nsteps * 4;
   }
   // Without per-step energies (and without profiling) a step is replayed
   // from a CUDA graph: same kernels, same arguments, no host launch cost.
@@ -1477,6 +1665,79 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     return MDG_OK;
   }
   return launch_check(c);
+}
+
+int sys_energies(mdg_ctx* c, double* out_dev)
+{
+  LAUNCH(c, "sys_energy", k_sys_energy, c->nsys, kThreads, c->d_first ? c->d_first : nullptr, c->fo.e_rebo,
+         c->fo.e_lj, c->fo.e_tors, c->e_kin, out_dev, c->d_status);
+  return launch_check(c);
+}
+
+int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (c->nsys < 2 || !c->d_first) return fail(MDG_ERR_STATE, "not a batched context (mdg_set_batch)");
+  if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
+  if (!epot && !etot) return mdg_run(c, nsteps, dt, nullptr, nullptr);
+  const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
+  State S = c->S();
+  int rc;
+  if (!c->acc_valid) {
+    rc = evaluate(c);
+    if (rc) return rc;
+    LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
+    c->acc_valid = true;
+  }
+  const int64_t need = (int64_t)nsteps * c->nsys * 4;
+  if (c->elog_cap < need) {
+    if (c->d_elog) cudaFree(c->d_elog);
+    c->d_elog = dalloc<double>((size_t)need);
+    if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
+    c->elog_cap = need;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
+    rc = evaluate(c);
+    if (rc) return rc;
+    LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
+    rc = sys_energies(c, c->d_elog + (int64_t)s * c->nsys * 4);
+    if (rc) return rc;
+  }
+  std::vector<double> h((size_t)need);
+  CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  for (int64_t q = 0; q < (int64_t)nsteps * c->nsys; q++) {
+    const double ep = (h[4 * q] + h[4 * q + 1]) + h[4 * q + 2];
+    if (epot) epot[q] = ep * c->unit_e;
+    if (etot) etot[q] = (ep + h[4 * q + 3]) * c->unit_e;
+  }
+  return MDG_OK;
+}
+
+int mdg_batch_energies(mdg_ctx* c, double* e_sys)
+{
+  if (!c || !c->n || !e_sys) return fail(MDG_ERR_ARG, "bad argument");
+  if (c->nsys < 2 || !c->d_first) return fail(MDG_ERR_STATE, "not a batched context (mdg_set_batch)");
+  int rc = evaluate(c);
+  if (rc) return rc;
+  State S = c->S();
+  LAUNCH(c, "ekin", k_ekin, nblk(c->n), kThreads, S, c->e_kin);
+  if (c->elog_cap < (int64_t)c->nsys * 4) {
+    if (c->d_elog) cudaFree(c->d_elog);
+    c->d_elog = dalloc<double>((size_t)c->nsys * 4);
+    if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
+    c->elog_cap = (int64_t)c->nsys * 4;
+  }
+  rc = sys_energies(c, c->d_elog);
+  if (rc) return rc;
+  std::vector<double> h((size_t)c->nsys * 4);
+  CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  for (size_t q = 0; q < h.size(); q++) e_sys[q] = h[q] * c->unit_e;
+  return MDG_OK;
 }
 
 int mdg_sync(mdg_ctx* c)

@@ -362,8 +362,9 @@ MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, 
   const int tb = (int)pb.w;
   int lo = a, hi = b;
   V3 rv;
-  if (a < b) rv = depos(St.box, xa, v3(pb.x, pb.y, pb.z));
-  else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), xa); }
+  const Box& box = box_of(St, a);
+  if (a < b) rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
+  else { lo = b; hi = a; rv = depos(box, v3(pb.x, pb.y, pb.z), xa); }
   const double d2 = norm2(rv);
   const double R1 = P.R[ta][tb][0], R2 = P.R[ta][tb][1];
   if (d2 > R2 * R2) return 0;
@@ -445,8 +446,9 @@ MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTask
   const double4 pa = St.pos[a], pb = St.pos[b];
   int lo = a, hi = b;
   V3 rv;
-  if (a < b) rv = depos(St.box, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z));
-  else { lo = b; hi = a; rv = depos(St.box, v3(pb.x, pb.y, pb.z), v3(pa.x, pa.y, pa.z)); }
+  const Box& box = box_of(St, a);
+  if (a < b) rv = depos(box, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z));
+  else { lo = b; hi = a; rv = depos(box, v3(pb.x, pb.y, pb.z), v3(pa.x, pa.y, pa.z)); }
   const int tlo = (int)St.pos[lo].w, thi = (int)St.pos[hi].w;
   const double r = sqrt(norm2(rv));
   PairGT<Real> p;

@@ -21,21 +21,28 @@ struct NList {
   double4* pos0;      // positions at the last build
 };
 
-// Cell grid of one list.
+// Cell grid of one list.  A batched context (many independent systems in
+// one atom array) keeps one grid per system, laid out one after another:
+// per-system dimensions, origin, cell size and first cell in snc/slo/scs.
 struct Grid {
   int nc[3];
   double lo[3], cs[3];  // origin and cell size per axis
-  int ncell;
-  int brute;            // 1: O(N^2) scan (a periodic axis has fewer than 3 cells)
+  int ncell;            // all systems together
+  int brute;            // 1: O(N^2) scan (single system, a periodic axis has fewer than 3 cells)
   int* ccount;          // [ncell]
   int* cstart;          // [ncell + 1]
   int* ccursor;         // [ncell]
   int* catoms;          // [n]
+  const int4* snc;      // [nsys] x, y, z = cells per axis, w = first cell (batched only)
+  const double4* slo;   // [nsys] origin
+  const double4* scs;   // [nsys] cell size
 };
 
 struct State {
   int n;
-  Box box;
+  Box box;              // the box of a single-system context
+  const int* sys;       // [n] system of each atom in a batched context, else null
+  const Box* boxes;     // [nsys] boxes of a batched context
   double4* pos;         // x, y, z, w = species index (0 C, 1 H)
   double4* vel;         // w unused
   double4* acc;         // an (Angstrom/fs^2)
@@ -44,7 +51,34 @@ struct State {
   double* mass;         // amu
 };
 
-MDG_HD int cell_coord(const Grid& g, const Box& box, int ax, double x)
+// The periodic box atom a lives in.
+MDG_HD const Box& box_of(const State& S, int a) { return S.sys ? S.boxes[S.sys[a]] : S.box; }
+
+// The cell grid of atom a's system.
+struct GridView {
+  int nc[3];
+  double lo[3], cs[3];
+  int base;
+};
+MDG_HD GridView grid_view(const Grid& g, const State& S, int a)
+{
+  GridView v;
+  if (S.sys) {
+    const int s = S.sys[a];
+    const int4 n = g.snc[s];
+    const double4 lo = g.slo[s], cs = g.scs[s];
+    v.nc[0] = n.x; v.nc[1] = n.y; v.nc[2] = n.z;
+    v.lo[0] = lo.x; v.lo[1] = lo.y; v.lo[2] = lo.z;
+    v.cs[0] = cs.x; v.cs[1] = cs.y; v.cs[2] = cs.z;
+    v.base = n.w;
+  } else {
+    for (int ax = 0; ax < 3; ax++) { v.nc[ax] = g.nc[ax]; v.lo[ax] = g.lo[ax]; v.cs[ax] = g.cs[ax]; }
+    v.base = 0;
+  }
+  return v;
+}
+
+MDG_HD int cell_coord(const GridView& g, const Box& box, int ax, double x)
 {
   int c = (int)floor((x - g.lo[ax]) / g.cs[ax]);
   if (box.pbc[ax]) {
@@ -57,10 +91,13 @@ MDG_HD int cell_coord(const Grid& g, const Box& box, int ax, double x)
   return c;
 }
 
-MDG_HD int cell_of(const Grid& g, const Box& box, double4 p)
+MDG_HD int cell_of(const Grid& g, const State& S, int a)
 {
-  int cx = cell_coord(g, box, 0, p.x), cy = cell_coord(g, box, 1, p.y), cz = cell_coord(g, box, 2, p.z);
-  return (cz * g.nc[1] + cy) * g.nc[0] + cx;
+  const GridView v = grid_view(g, S, a);
+  const Box& box = box_of(S, a);
+  const double4 p = S.pos[a];
+  int cx = cell_coord(v, box, 0, p.x), cy = cell_coord(v, box, 1, p.y), cz = cell_coord(v, box, 2, p.z);
+  return v.base + (cz * v.nc[1] + cy) * v.nc[0] + cx;
 }
 
 // Insertion sort of a short int range (ascending).
@@ -75,43 +112,53 @@ MDG_HD void isort(int* v, int n)
 }
 
 // Build atom i's list from the cell grid (or by brute force); ascending order.
+// A periodic axis with fewer than 3 cells (batched systems only) visits each
+// of its cells once.
 MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsigned int* status)
 {
   const double4 pi = S.pos[i];
   const V3 xi = v3(pi.x, pi.y, pi.z);
+  const Box& box = box_of(S, i);
   int cnt = 0;
   int* out = L.list + (long)i * L.cap;
-  if (g.brute) {
+  if (g.brute && !S.sys) {
     for (int j = 0; j < S.n; j++) {
       if (j == i) continue;
       double4 pj = S.pos[j];
-      V3 d = depos(S.box, xi, v3(pj.x, pj.y, pj.z));
+      V3 d = depos(box, xi, v3(pj.x, pj.y, pj.z));
       if (norm2(d) < L.range2) {
         if (cnt < L.cap) out[cnt] = j;
         cnt++;
       }
     }
   } else {
-    int c0[3] = {cell_coord(g, S.box, 0, pi.x), cell_coord(g, S.box, 1, pi.y), cell_coord(g, S.box, 2, pi.z)};
-    for (int dz = -1; dz <= 1; dz++) {
+    const GridView v = grid_view(g, S, i);
+    int c0[3], dlo[3], dhi[3];
+    for (int ax = 0; ax < 3; ax++) {
+      c0[ax] = cell_coord(v, box, ax, ax == 0 ? pi.x : (ax == 1 ? pi.y : pi.z));
+      dlo[ax] = -1;
+      dhi[ax] = 1;
+      if (box.pbc[ax] && v.nc[ax] < 3) { dlo[ax] = 0; dhi[ax] = v.nc[ax] - 1; }
+    }
+    for (int dz = dlo[2]; dz <= dhi[2]; dz++) {
       int cz = c0[2] + dz;
-      if (S.box.pbc[2]) cz = (cz + g.nc[2]) % g.nc[2];
-      else if (cz < 0 || cz >= g.nc[2]) continue;
-      for (int dy = -1; dy <= 1; dy++) {
+      if (box.pbc[2]) cz = (cz + v.nc[2]) % v.nc[2];
+      else if (cz < 0 || cz >= v.nc[2]) continue;
+      for (int dy = dlo[1]; dy <= dhi[1]; dy++) {
         int cy = c0[1] + dy;
-        if (S.box.pbc[1]) cy = (cy + g.nc[1]) % g.nc[1];
-        else if (cy < 0 || cy >= g.nc[1]) continue;
-        for (int dx = -1; dx <= 1; dx++) {
+        if (box.pbc[1]) cy = (cy + v.nc[1]) % v.nc[1];
+        else if (cy < 0 || cy >= v.nc[1]) continue;
+        for (int dx = dlo[0]; dx <= dhi[0]; dx++) {
           int cx = c0[0] + dx;
-          if (S.box.pbc[0]) cx = (cx + g.nc[0]) % g.nc[0];
-          else if (cx < 0 || cx >= g.nc[0]) continue;
-          int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+          if (box.pbc[0]) cx = (cx + v.nc[0]) % v.nc[0];
+          else if (cx < 0 || cx >= v.nc[0]) continue;
+          int cell = v.base + (cz * v.nc[1] + cy) * v.nc[0] + cx;
           int b = g.cstart[cell], e = g.cstart[cell + 1];
           for (int q = b; q < e; q++) {
             int j = g.catoms[q];
             if (j == i) continue;
             double4 pj = S.pos[j];
-            V3 d = depos(S.box, xi, v3(pj.x, pj.y, pj.z));
+            V3 d = depos(box, xi, v3(pj.x, pj.y, pj.z));
             if (norm2(d) < L.range2) {
               if (cnt < L.cap) out[cnt] = j;
               cnt++;
@@ -134,7 +181,7 @@ MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsign
 MDG_HD double disp_atom(const State& S, const NList& L, int i)
 {
   double4 p = S.pos[i], q = L.pos0[i];
-  V3 d = depos(S.box, v3(p.x, p.y, p.z), v3(q.x, q.y, q.z));
+  V3 d = depos(box_of(S, i), v3(p.x, p.y, p.z), v3(q.x, q.y, q.z));
   return sqrt(norm2(d));
 }
 
@@ -167,7 +214,7 @@ MDG_HD void bonds_atom(const State& S, const NList& L, const ReboParams& P, Bond
     const int j = lst[s];
     const double4 pj = S.pos[j];
     const int tj = (int)pj.w;
-    V3 rv = depos(S.box, xa, v3(pj.x, pj.y, pj.z));
+    V3 rv = depos(box_of(S, a), xa, v3(pj.x, pj.y, pj.z));
     double d2 = norm2(rv);
     const double R1 = P.R[ta][tj][0], R2 = P.R[ta][tj][1];
     if (d2 > R2 * R2) continue;
@@ -392,9 +439,10 @@ MDG_HD void wrap_atom(State& S, int i, unsigned int* status)
   double4 p = S.pos[i];
   int4 im = S.image[i];
   bool ok = true;
-  if (S.box.pbc[0]) ok &= wrap1(p.x, im.x, S.box.L[0]);
-  if (S.box.pbc[1]) ok &= wrap1(p.y, im.y, S.box.L[1]);
-  if (S.box.pbc[2]) ok &= wrap1(p.z, im.z, S.box.L[2]);
+  const Box& box = box_of(S, i);
+  if (box.pbc[0]) ok &= wrap1(p.x, im.x, box.L[0]);
+  if (box.pbc[1]) ok &= wrap1(p.y, im.y, box.L[1]);
+  if (box.pbc[2]) ok &= wrap1(p.z, im.z, box.L[2]);
   if (!ok && status) *status |= ST_NONFINITE;
   S.pos[i] = p;
   S.image[i] = im;
