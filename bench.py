@@ -339,9 +339,18 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             b_ms = float(t.item())
         bx.sync()
+        bx.set_profiling(True)
+        for k in range(5):
+            flush.zero_()
+            bx.run(1, BATCH_DT_FS, energies=False)
+        bprof = bx.profile_read()
+        bx.set_profiling(False)
+        btot = sum(v[0] for v in bprof.values()) or 1.0
+        bkern = {k: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1], "share": v[0] / btot}
+                 for k, v in sorted(bprof.items(), key=lambda kv: -kv[1][0])[:10]}
         batched = {"value": world * nb_atoms * kb / (b_ms * 1e-3), "unit": "atom-steps/s", "steps": kb,
                    "ms_per_step": b_ms / kb, "systems": BATCH_SYSTEMS, "atoms": nb_atoms,
-                   "precision": "fp32-mixed", "dt_fs": BATCH_DT_FS,
+                   "precision": "fp32-mixed", "dt_fs": BATCH_DT_FS, "kernels": bkern,
                    "workload": "cluster impacts: AB graphite slabs 800-6000 atoms (lateral PBC, open z, fixed "
                                "bottom layer) + 13-atom C cluster at 10-100 eV, AIREBO"}
         del bx

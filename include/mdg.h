@@ -77,6 +77,10 @@ typedef struct mdg_params {
   int bond_rec_avg;   /* capacity of the per-bond REBO records over the whole system, doubles per
                          atom on average (a bond slot of an atom with b bonds takes 5 + 4b);
                          0 = default (174: six bonds per atom) */
+  int task_mode;      /* REBO work split: 1 = one task per directed bond (both ends evaluate each
+                         bond, shortest critical path), 2 = one task per bond writing both ends'
+                         records (half the work); 0 = timed once per system on the first mdg_run
+                         (the autotuner) and the faster kept.  Results are bitwise the same. */
 } mdg_params;
 
 /* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */
@@ -184,6 +188,10 @@ int mdg_pipe_peak(int device, int fp32, double* tflops);
  * calls that overlap on the GPU race.  No counterpart in the reference. */
 int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const double box[3], const int32_t pbc[3],
                              int with_torsion, double* energy, double* grad, void* stream);
+
+/* The REBO task mode in use (1 directed, 2 per bond) and, when the autotuner
+ * ran, its timings of one force evaluation in each mode (ms; 0 otherwise). */
+int mdg_task_mode(mdg_ctx* ctx, int* mode, float* ms_directed, float* ms_per_bond);
 
 /* ---- Batched systems ----
  * Many independent systems of uneven size in one context (the reference runs

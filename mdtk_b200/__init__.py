@@ -56,6 +56,7 @@ class Params(ctypes.Structure):
         ("special_avg", ctypes.c_int),
         ("device", ctypes.c_int),
         ("bond_rec_avg", ctypes.c_int),
+        ("task_mode", ctypes.c_int),
     ]
 
 
@@ -85,6 +86,8 @@ def lib():
         L.mdg_set_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), i32p, dp, dp, dp, i32p,
                                     ctypes.POINTER(ctypes.c_uint8)]
         L.mdg_batch_energies.argtypes = [vp, dp]
+        L.mdg_task_mode.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_float)]
         L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_sync.argtypes = [vp]
         L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
@@ -213,6 +216,15 @@ class Context:
                                    fixed.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
         self.n = len(z)
         self.nsys = len(systems)
+
+    def task_mode(self):
+        """(mode, ms_directed, ms_per_bond): REBO task mode in use (1 directed,
+        2 per bond) and the autotuner's timings (0 when it did not run)."""
+        m = ctypes.c_int()
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        _check(lib().mdg_task_mode(self.h, ctypes.byref(m), ctypes.byref(a), ctypes.byref(b)))
+        return m.value, a.value, b.value
 
     def batch_energies(self) -> np.ndarray:
         """[nsys, 4]: REBO, LJ, torsion, kinetic energy of each system."""

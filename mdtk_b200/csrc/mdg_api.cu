@@ -196,8 +196,18 @@ __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
   if (!K.ctr) return;  // uniform over the launch
   const unsigned long long need = ok ? (unsigned long long)nb * bond_rec_size(nb) : 0ull;
   const unsigned long long rb = warp_alloc(need, &K.ctr[2]);
-  const unsigned long long i0 = warp_alloc(ncc, &K.ctr[0]);
-  const unsigned long long i1 = warp_alloc(nb - ncc, &K.ctr[1]);
+  // queued slots: all (one task per directed slot) or those to higher
+  // partners (one task per bond)
+  int mcc = 0, mot = 0;
+  if (ok)
+    for (int s = 0; s < nb; s++) {
+      const int j = B.bj[a * B.mb + s];
+      if (K.pairs && j < a) continue;
+      if (ncc && (int)B.nco[j].w == kC) mcc++;
+      else mot++;
+    }
+  const unsigned long long i0 = warp_alloc(mcc, &K.ctr[0]);
+  const unsigned long long i1 = warp_alloc(mot, &K.ctr[1]);
   if (!ok) return;
   if ((long)(rb + need) > K.rec_cap) {
     K.rbase[a] = -1;
@@ -207,7 +217,9 @@ __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
   }
   int f = (int)i0, b = (int)i1;
   for (int s = 0; s < nb; s++) {
-    const bool cc = ncc && (int)B.nco[B.bj[a * B.mb + s]].w == kC;
+    const int j = B.bj[a * B.mb + s];
+    if (K.pairs && j < a) continue;
+    const bool cc = ncc && (int)B.nco[j].w == kC;
     if (cc) K.q[f++] = a * B.mb + s;
     else K.q[K.cap - 1 - (b++)] = a * B.mb + s;
   }
@@ -236,6 +248,25 @@ __global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const TB
     const long rb = K.rbase[a];
     if (rb < 0) continue;
     rebo_task(R, TP, do_rebo, do_tors, K.rec + rb + (long)s * bond_rec_size(B.nb[a]), a, s);
+  }
+}
+
+// REBO + torsion, one thread per bond (both ends' records), grid-stride.
+template <class Real, class TB>
+__global__ void __launch_bounds__(128) k_rebo_pair_task(const ReboParams* P, const TB* T, BondList B, TorsParams TP,
+                                                        int do_rebo, int do_tors, BondTasks K,
+                                                        unsigned int* status)
+{
+  const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
+  ReboT<Real, TB> R{*P, *T, B, status};
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
+    const int q = t < n0 ? K.q[t] : K.q[K.cap - 1 - (t - n0)];
+    const int lo = q / B.mb, s = q - lo * B.mb;
+    const int hi = B.bj[q], sh = B.brev[q];
+    const long rl = K.rbase[lo], rh = K.rbase[hi];
+    if (rl < 0 || rh < 0 || sh < 0) continue;  // already flagged
+    rebo_pair_task(R, TP, do_rebo, do_tors, K.rec + rl + (long)s * bond_rec_size(B.nb[lo]),
+                   K.rec + rh + (long)sh * bond_rec_size(B.nb[hi]), lo, s, hi);
   }
 }
 
@@ -332,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
                                                        unsigned int* status)
 {
   __shared__ int queue[kThreads / 32][64];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
   const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (a >= S.n) return;  // whole warps
@@ -487,22 +519,48 @@ __global__ void k_scan_add(ScanPair P)
   if (i < P.n && blockIdx.x > 0) P.out[y][i] += P.tile[y][blockIdx.x];
 }
 
-__global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, unsigned int* status)
+// Flat task list (atom, partner) and record offsets; with `pairs`, also the
+// work list of tasks owned by the lower index of their pair and, for each,
+// the partner's task of the same pair (a linear search in its special list).
+__global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, int pairs, unsigned int* status)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
-  const int c = Tk.cnt[a], o = Tk.off[a];
-  const int rs = rec_size(nbonds[a]);
+  const bool ok = a < n;
+  int c = 0, o = 0, nhi = 0;
+  if (ok) {
+    c = Tk.cnt[a];
+    o = Tk.off[a];
+    const int rs = rec_size(nbonds[a]);
+    for (int q = 0; q < c; q++) {
+      const int t = o + q;
+      const long ro = (long)Tk.roff[a] + (long)q * rs;
+      const int b = Tk.part[(long)a * Tk.cap + q];
+      if (t < Tk.task_cap) {
+        Tk.flat[t] = make_int2(a, b);
+        if (ro + rs <= Tk.rec_cap) Tk.trec[t] = ro;
+        else { Tk.trec[t] = -1; atomicOr(status, ST_RECORD_OVERFLOW); }
+        nhi += (b > a);
+      } else {
+        atomicOr(status, ST_RECORD_OVERFLOW);
+      }
+    }
+  }
+  if (!pairs) return;  // uniform over the launch
+  const unsigned long long w0 = warp_alloc(nhi, Tk.wcnt);
+  if (!ok) return;
+  int w = (int)w0;
   for (int q = 0; q < c; q++) {
     const int t = o + q;
-    const long ro = (long)Tk.roff[a] + (long)q * rs;
-    if (t < Tk.task_cap) {
-      Tk.flat[t] = make_int2(a, Tk.part[(long)a * Tk.cap + q]);
-      if (ro + rs <= Tk.rec_cap) Tk.trec[t] = ro;
-      else { Tk.trec[t] = -1; atomicOr(status, ST_RECORD_OVERFLOW); }
-    } else {
-      atomicOr(status, ST_RECORD_OVERFLOW);
-    }
+    if (t >= Tk.task_cap) break;
+    const int b = Tk.part[(long)a * Tk.cap + q];
+    if (b < a) continue;
+    int t2 = -1;
+    const int cb = Tk.cnt[b], ob = Tk.off[b];
+    for (int u = 0; u < cb; u++)
+      if (Tk.part[(long)b * Tk.cap + u] == a) { t2 = ob + u; break; }
+    if (t2 >= Tk.task_cap) t2 = -1;
+    Tk.wrev[t] = t2;
+    Tk.work[w++] = t;
   }
 }
 
@@ -516,6 +574,22 @@ __global__ void k_lj_special(const ReboParams* P, const TB* Tb, LJParams LP, Bon
   LJT<Real, TB> X{LP, R, T};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
     lj_special_task(X, S, Tk, t, status);
+}
+
+// Special LJ pairs, one thread per pair (both ends' records).
+template <class Real, class TB>
+__global__ void k_lj_special_pair(const ReboParams* P, const TB* Tb, LJParams LP, BondList B, CijTable T, State S,
+                                  SpecialTasks Tk, unsigned int* status)
+{
+  const long total = (long)*Tk.wcnt;
+  ReboT<Real, TB> R{*P, *Tb, B, status};
+  LJT<Real, TB> X{LP, R, T};
+  for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < total; w += (long)gridDim.x * blockDim.x) {
+    const int t = Tk.work[w];
+    const int t2 = Tk.wrev[t];
+    if (t2 < 0) { atomicOr(status, ST_RECORD_OVERFLOW); continue; }
+    lj_special_pair_task(X, S, Tk, t, t2, status);
+  }
 }
 
 __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad)
@@ -730,6 +804,8 @@ struct mdg_ctx {
   SpecialTasks spc;
   BondTasks bt;
   int rebo_task_blocks = 0;
+  bool tuned = false;        // the autotuner ran for this system
+  float tune_ms[2] = {0, 0};  // its timings of one force evaluation per task mode
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
@@ -883,7 +959,8 @@ void free_system(mdg_ctx* c)
     c->has_list[l] = false;
   }
   void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
-                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->scan_tiles};
+                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work, c->spc.wrev,
+                c->spc.wcnt, c->scan_tiles};
   c->scan_tiles = nullptr;
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   c->step_graph = nullptr;
@@ -900,6 +977,7 @@ void free_system(mdg_ctx* c)
   c->d_first = nullptr;
   for (int l = 0; l < 2; l++) { c->d_snc[l] = nullptr; c->d_slo[l] = nullptr; c->d_scs[l] = nullptr; }
   c->nsys = 1;
+  c->tuned = false;
   c->h_first.clear();
   c->h_boxes.clear();
   c->h_sys.clear();
@@ -1070,14 +1148,25 @@ int evaluate(mdg_ctx* c)
   LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
   const bool f32p = c->prm.precision == MDG_PREC_FP32_MIXED;
-  if (tasks && f32p) {
-    auto kern = k_rebo_task<f32, ReboTables32>;
-    LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, rebo ? 1 : 0,
-           tors ? 1 : 0, c->bt, c->d_status);
-  } else if (tasks) {
-    auto kern = k_rebo_task<double, ReboTables>;
-    LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
-           tors ? 1 : 0, c->bt, c->d_status);
+  if (tasks) {
+    const int ir = rebo ? 1 : 0, it = tors ? 1 : 0;
+    if (f32p && c->bt.pairs) {
+      auto kern = k_rebo_pair_task<f32, ReboTables32>;
+      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
+             c->d_status);
+    } else if (f32p) {
+      auto kern = k_rebo_task<f32, ReboTables32>;
+      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
+             c->d_status);
+    } else if (c->bt.pairs) {
+      auto kern = k_rebo_pair_task<double, ReboTables>;
+      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
+             c->d_status);
+    } else {
+      auto kern = k_rebo_task<double, ReboTables>;
+      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
+             c->d_status);
+    }
   }
   else
     LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
@@ -1104,11 +1193,16 @@ int evaluate(mdg_ctx* c)
     LAUNCH(c, "lj_scan_tiles", k_scan_tiles, dim3(sp.ntiles, 2), kScanTile, sp);
     LAUNCH(c, "lj_scan_top", k_scan_top, dim3(1, 2), 32, sp);
     LAUNCH(c, "lj_scan_add", k_scan_add, dim3(sp.ntiles, 2), kScanTile, sp);
-    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, c->d_status);
+    const int pairs = (c->bt.ctr && c->bt.pairs) ? 1 : 0;
+    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, pairs, c->d_status);
     // b*_ij of close non-bonded pairs stays FP64 in the mixed mode too: the
     // S(t_b) window (0.04 wide for C-C) multiplies an error of b* by up to
     // 1/0.04^2 in the pair force, beyond what float b* can carry.
-    {
+    if (pairs) {
+      auto kern = k_lj_special_pair<double, ReboTables>;
+      LAUNCH(c, "lj_special", kern, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
+             c->spc, c->d_status);
+    } else {
       auto kern = k_lj_special<double, ReboTables>;
       LAUNCH(c, "lj_special", kern, c->special_blocks, kThreads, c->d_rp, c->d_tables, c->ljp, B, c->cij, S,
              c->spc, c->d_status);
@@ -1382,6 +1476,10 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     L.range2 = range * range;
     L.trigger = c->prm.nl_skin_mode == 0 ? 0.44 * c->rcut[l] : c->prm.nl_skin;
     L.cap = (l == 0) ? c->prm.cap_rebo_list : c->prm.cap_lj_list;
+    // The REBO list keeps the reference's ascending order (it fixes the bond
+    // slot order, hence every bond-order sum).  The LJ list only orders pair
+    // sums, so it stays in (deterministic) cell order and skips the sort.
+    L.sorted = (l == 0) ? 1 : 0;
     L.cnt = dalloc<int>(n);
     L.list = dalloc<int>((size_t)n * L.cap);
     L.pos0 = dalloc<double4>(n);
@@ -1423,6 +1521,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   if (c->prm.potentials & (MDG_POT_REBO | MDG_POT_ETORS) && !(c->prm.potentials & MDG_POT_BRENNER)) {
     BondTasks& K = c->bt;
     K.cap = n * mb;
+    K.pairs = c->prm.task_mode == 2 ? 1 : 0;
     K.rec_cap = (long)n * c->prm.bond_rec_avg;
     K.q = dalloc<int>((size_t)K.cap);
     K.ctr = dalloc<unsigned long long>(4);
@@ -1459,6 +1558,11 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     X.rec = dalloc<double>(X.rec_cap);
     X.mid = dalloc<int4>(X.task_cap);
     X.midc = dalloc<double>(X.task_cap);
+    X.work = dalloc<int>(X.task_cap);
+    X.wrev = dalloc<int>(X.task_cap);
+    X.wcnt = dalloc<unsigned long long>(1);
+    if (!X.work || !X.wrev || !X.wcnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ work list)");
+    CK(cudaMemset(X.wcnt, 0, sizeof(unsigned long long)));
     if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
         !X.trec || !X.rec || !X.mid || !X.midc)
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
@@ -1593,6 +1697,41 @@ int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* 
   return MDG_OK;
 }
 
+// The autotuner: with task_mode 0, times one force evaluation in each REBO
+// task mode (after one untimed evaluation each; best of three) on the first
+// run of a system and keeps the faster.  Both modes give bitwise the same
+// forces, so the choice changes only the speed.
+static int autotune(mdg_ctx* c)
+{
+  if (c->tuned || !c->bt.ctr) return MDG_OK;
+  c->tuned = true;
+  if (c->prm.task_mode != 0) return MDG_OK;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int mode = 0; mode < 2; mode++) {
+    c->bt.pairs = mode;
+    int rc = evaluate(c);
+    if (rc) return rc;
+    float best = 1e30f;
+    for (int r = 0; r < 3; r++) {
+      CK(cudaEventRecord(e0, c->stream));
+      rc = evaluate(c);
+      if (rc) return rc;
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      best = std::min(best, ms);
+    }
+    c->tune_ms[mode] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->bt.pairs = c->tune_ms[1] < c->tune_ms[0] ? 1 : 0;
+  return read_status(c);
+}
+
 int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
@@ -1606,6 +1745,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
     c->acc_valid = true;
   }
+  rc = autotune(c);
+  if (rc) return rc;
   const bool log = epot || etot;
   if (log && c->elog_cap < (int64_t)nsteps * 4) {
     if (c->d_elog) cudaFree(c->d_elog);
@@ -1689,6 +1830,8 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
     c->acc_valid = true;
   }
+  rc = autotune(c);
+  if (rc) return rc;
   const int64_t need = (int64_t)nsteps * c->nsys * 4;
   if (c->elog_cap < need) {
     if (c->d_elog) cudaFree(c->d_elog);
@@ -1737,6 +1880,15 @@ int mdg_batch_energies(mdg_ctx* c, double* e_sys)
   rc = read_status(c);
   if (rc) return rc;
   for (size_t q = 0; q < h.size(); q++) e_sys[q] = h[q] * c->unit_e;
+  return MDG_OK;
+}
+
+int mdg_task_mode(mdg_ctx* c, int* mode, float* ms_directed, float* ms_per_bond)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  if (mode) *mode = c->bt.pairs ? 2 : 1;
+  if (ms_directed) *ms_directed = c->tune_ms[0];
+  if (ms_per_bond) *ms_per_bond = c->tune_ms[1];
   return MDG_OK;
 }
 

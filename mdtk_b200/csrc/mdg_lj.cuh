@@ -346,6 +346,10 @@ struct SpecialTasks {
   double* rec;      // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]
   int4* mid;        // [task_cap] middle-bond output (k, slot of m in k, m, valid)
   double* midc;     // [task_cap]
+  // one evaluation per pair (the lower-index end's task writes both records):
+  int* work;        // [task_cap] tasks whose owner is the lower index
+  int* wrev;        // [task_cap] the partner's task of the same pair (-1: none)
+  unsigned long long* wcnt;  // number of work items
 };
 
 // Record size of a task owned by an atom with nb bonds.
@@ -468,6 +472,59 @@ MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTask
   rec[3] = (a == lo) ? dbl(E) : 0.0;
   Tk.mid[t] = make_int4(mo.k, mo.sm, mo.m, mo.valid);
   Tk.midc[t] = mo.valid ? mo.c : 0.0;
+}
+
+// One special pair (a < b) from task t of a and task t2 of b, written into
+// both records by a PairSink: the same additions as the two single-end tasks.
+template <class Real, class TB>
+MDG_HD void lj_special_pair_task(const LJT<Real, TB>& X, const State& St, SpecialTasks& Tk, int t, int t2,
+                                 unsigned int* status)
+{
+  const int2 ap = Tk.flat[t];
+  const int a = ap.x, b = ap.y;
+  const long ro = Tk.trec[t], ro2 = Tk.trec[t2];
+  if (ro < 0 || ro2 < 0) return;  // beyond the record capacity (already flagged)
+  const int na = X.R.B.nb[a], nb = X.R.B.nb[b];
+  double* ra = Tk.rec + ro;
+  double* rb = Tk.rec + ro2;
+  PairSinkT<Real> sink;
+  sink.a = a;
+  sink.b = b;
+  sink.ga = v3(0, 0, 0);
+  sink.gb = v3(0, 0, 0);
+  sink.Aa = ra + 4;
+  sink.Wa = ra + 4 + 3 * na;
+  sink.Ab = rb + 4;
+  sink.Wb = rb + 4 + 3 * nb;
+  for (int q = 0; q < 4 * na; q++) sink.Aa[q] = 0.0;
+  for (int q = 0; q < 4 * nb; q++) sink.Ab[q] = 0.0;
+  const double4 pa = St.pos[a], pb = St.pos[b];
+  const V3 rv = depos(box_of(St, a), v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z));
+  const int ta = (int)pa.w, tb = (int)pb.w;
+  const double r = sqrt(norm2(rv));
+  PairGT<Real> p;
+  p.rv = cvt3<Real>(rv);
+  p.r = r;
+  p.rd = r;
+  p.u = cvt3<Real>(rv / r);
+  cutoff(p.r, X.P.R[ta][tb][0], X.P.R[ta][tb][1], p.f, p.df);
+  p.alter = 0;
+  p.ralt = 0.0;
+  MidOut mo;
+  mo.valid = 0;
+  const Real E = X.pair(a, b, p, sink, &mo, status);
+  ra[0] = sink.ga.x;
+  ra[1] = sink.ga.y;
+  ra[2] = sink.ga.z;
+  ra[3] = dbl(E);
+  rb[0] = sink.gb.x;
+  rb[1] = sink.gb.y;
+  rb[2] = sink.gb.z;
+  rb[3] = 0.0;
+  Tk.mid[t] = make_int4(mo.k, mo.sm, mo.m, mo.valid);
+  Tk.midc[t] = mo.valid ? mo.c : 0.0;
+  Tk.mid[t2] = make_int4(0, 0, 0, 0);
+  Tk.midc[t2] = 0.0;
 }
 
 // Sums atom a's special-task records (in list order) into its accumulators.

@@ -84,6 +84,44 @@ struct SinkT {
 };
 typedef SinkT<double> Sink;
 
+// Both ends of a bond (lo, hi) at once: contributions are routed to each
+// end's record exactly as two single-end Sinks would route them (the same
+// additions in the same order), so one evaluation of the bond replaces two.
+template <class Real>
+struct PairSinkT {
+  int a, b;          // lo, hi
+  V3 ga, gb;
+  double *Aa, *Wa, *Ab, *Wb;
+  MDG_HD void pair(int p, int q, V3T<Real> v)
+  {
+    const V3 d = to_d(v);
+    if (p == a) ga += d;
+    else if (q == a) ga -= d;
+    if (p == b) gb += d;
+    else if (q == b) gb -= d;
+  }
+  MDG_HD void cbond(int c, int s, V3T<Real> v)
+  {
+    const V3 d = to_d(v);
+    if (c == a) {
+      ga += d;
+      Aa[3 * s + 0] -= d.x;
+      Aa[3 * s + 1] -= d.y;
+      Aa[3 * s + 2] -= d.z;
+    } else if (c == b) {
+      gb += d;
+      Ab[3 * s + 0] -= d.x;
+      Ab[3 * s + 1] -= d.y;
+      Ab[3 * s + 2] -= d.z;
+    }
+  }
+  MDG_HD void wt(int c, int s, Real w)
+  {
+    if (c == a) Wa[s] += dbl(w);
+    else if (c == b) Wb[s] += dbl(w);
+  }
+};
+
 template <class Real, class TB>
 struct ReboT {
   const ReboParams& P;

@@ -14,6 +14,7 @@ namespace mdg {
 // list[i * cap + s], s < cnt[i].
 struct NList {
   int cap;
+  int sorted;         // 1: ascending partner order (the reference's); 0: cell order (deterministic)
   int* cnt;
   int* list;
   double range2;      // ((1 + 0.44) * Rcutoff)^2
@@ -167,7 +168,7 @@ MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsign
         }
       }
     }
-    if (cnt <= L.cap) isort(out, cnt);
+    if (L.sorted && cnt <= L.cap) isort(out, cnt);
   }
   if (cnt > L.cap) {
     *status |= ST_NL_OVERFLOW;
@@ -313,6 +314,7 @@ MDG_HD void rebo_atom(const Rebo& R, const TorsParams& TP, int do_rebo, int do_t
 // longest serial chain from all of a carbon's bonds to one bond.
 struct BondTasks {
   int cap;                  // queue capacity (n * mb)
+  int pairs;                // 0: one task per directed slot; 1: one task per bond (slots to higher partners)
   int* q;                   // slots a*mb+s: C-C bonds from the front, the rest from the back
   unsigned long long* ctr;  // [0] C-C tasks, [1] other tasks, [2] record doubles handed out
   long* rbase;              // [n] first record double of atom a (-1: over capacity, flagged)
@@ -353,6 +355,41 @@ MDG_HD void rebo_task(const ReboT<Real, TB>& R, const TorsParams& TP, int do_reb
   rec[2] = sink.g.z;
   rec[3] = er;
   rec[4] = et;
+}
+
+// REBO (+ torsion) of bond slot s of atom lo (partner hi > lo, slot sh in
+// hi's list) into both ends' records.
+template <class Real, class TB>
+MDG_HD void rebo_pair_task(const ReboT<Real, TB>& R, const TorsParams& TP, int do_rebo, int do_tors, double* rlo,
+                           double* rhi, int lo, int s, int hi)
+{
+  const BondList& B = R.B;
+  const int na = B.nb[lo], nb = B.nb[hi];
+  PairSinkT<Real> sink;
+  sink.a = lo;
+  sink.b = hi;
+  sink.ga = v3(0, 0, 0);
+  sink.gb = v3(0, 0, 0);
+  sink.Aa = rlo + 5;
+  sink.Wa = rlo + 5 + 3 * na;
+  sink.Ab = rhi + 5;
+  sink.Wb = rhi + 5 + 3 * nb;
+  for (int t = 0; t < 4 * na; t++) sink.Aa[t] = 0.0;
+  for (int t = 0; t < 4 * nb; t++) sink.Ab[t] = 0.0;
+  const PairGT<Real> p = pair_from_slot<Real>(B, lo * B.mb + s);
+  double er = 0.0, et = 0.0;
+  if (do_rebo) er = dbl(R.bond(lo, hi, p, sink));
+  if (do_tors) et = dbl(etors_bond(R, TP, lo, hi, p, sink));
+  rlo[0] = sink.ga.x;
+  rlo[1] = sink.ga.y;
+  rlo[2] = sink.ga.z;
+  rlo[3] = er;
+  rlo[4] = et;
+  rhi[0] = sink.gb.x;
+  rhi[1] = sink.gb.y;
+  rhi[2] = sink.gb.z;
+  rhi[3] = 0.0;
+  rhi[4] = 0.0;
 }
 
 // Total dE/dx_a: own parts, what bond partners owe a, and the third-shell

@@ -1,0 +1,57 @@
+"""REBO work split and the autotuner: one task per directed bond and one
+task per bond route the same additions into the same records, so forces,
+energies and trajectories are bitwise the same in both modes; the
+autotuner only picks the faster."""
+import numpy as np
+import pytest
+
+import mdtk_b200 as M
+from mdtk_b200 import builders as B
+
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = {
+    "ethane30": lambda: B.ethane_liquid(30, seed=61, min_dist=1.6, jitter=0.4),
+    "diamond4_disp": lambda: B.diamond(4, disp_sigma=0.1, seed=62),
+    "ach300": lambda: B.amorphous_carbon(300, h_fraction=0.25, seed=63),
+    "impact": lambda: B.impact(64, n_target=900),
+}
+
+
+def _ctx(s, mode, precision=M.PREC_FP64, pot=M.POT_AIREBO):
+    c = M.Context(potentials=pot, precision=precision, task_mode=mode)
+    c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    return c
+
+
+@pytest.mark.parametrize("precision", [M.PREC_FP64, M.PREC_FP32_MIXED])
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_task_modes_bitwise_equal(name, precision):
+    s = SYSTEMS[name]()
+    e1, t1, g1 = _ctx(s, 1, precision).compute()
+    e2, t2, g2 = _ctx(s, 2, precision).compute()
+    assert np.array_equal(g1, g2)
+    assert np.array_equal(t1, t2) and e1 == e2
+
+
+def test_task_modes_same_trajectory():
+    s = SYSTEMS["diamond4_disp"]()
+    a, b = _ctx(s, 1), _ctx(s, 2)
+    ea = a.run(20, 0.5)
+    eb = b.run(20, 0.5)
+    assert np.array_equal(ea[1], eb[1])
+    assert np.array_equal(a.get_state()[0], b.get_state()[0])
+
+
+def test_autotuner_picks_a_mode():
+    s = SYSTEMS["ach300"]()
+    c = _ctx(s, 0)
+    assert c.task_mode()[0] == 1          # before the first run: directed
+    c.run(2, 0.25, energies=False)
+    mode, t1, t2 = c.task_mode()
+    assert mode in (1, 2) and t1 > 0 and t2 > 0
+    assert mode == (2 if t2 < t1 else 1)
+    # the tuned context still reproduces a fixed-mode run bitwise
+    d = _ctx(s, mode)
+    d.run(2, 0.25, energies=False)
+    assert np.array_equal(c.get_state()[0], d.get_state()[0])
