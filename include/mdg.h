@@ -80,7 +80,9 @@ typedef struct mdg_params {
   int task_mode;      /* REBO work split: 1 = one task per directed bond (both ends evaluate each
                          bond, shortest critical path), 2 = one task per bond writing both ends'
                          records (half the work); 0 = timed once per system on the first mdg_run
-                         (the autotuner) and the faster kept.  Results are bitwise the same. */
+                         (the autotuner) and the faster kept.  Both route the same terms into the
+                         same records; results agree to rounding (the two kernels may contract
+                         multiply-adds differently). */
 } mdg_params;
 
 /* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */

@@ -1699,8 +1699,8 @@ int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* 
 
 // The autotuner: with task_mode 0, times one force evaluation in each REBO
 // task mode (after one untimed evaluation each; best of three) on the first
-// run of a system and keeps the faster.  Both modes give bitwise the same
-// forces, so the choice changes only the speed.
+// run of a system and keeps the faster.  Both modes compute the same terms
+// (equal to rounding), so the choice changes only the speed.
 static int autotune(mdg_ctx* c)
 {
   if (c->tuned || !c->bt.ctr) return MDG_OK;

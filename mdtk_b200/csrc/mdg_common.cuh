@@ -127,6 +127,19 @@ MDG_HD V3T<Real> cross(V3T<Real> a, V3T<Real> b)
 }
 template <class Real>
 MDG_HD Real norm2(V3T<Real> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+// Squared length in double with every product and sum rounded on its own (no
+// FMA contraction): a distance computed in two kernels is then the same
+// number, so a cutoff f_ij subtracted from a coordination sum N_i cancels it
+// exactly (the reference's check N > -1e-15, REBO.cxx:434), and it equals the
+// reference's own x*x + y*y + z*z.
+MDG_HD double norm2(V3 a)
+{
+#if defined(__CUDA_ARCH__)
+  return __dadd_rn(__dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y)), __dmul_rn(a.z, a.z));
+#else
+  return a.x * a.x + a.y * a.y + a.z * a.z;
+#endif
+}
 template <class Real>
 MDG_HD Real SQR(Real x) { return x * x; }
 

@@ -87,6 +87,8 @@ typedef SinkT<double> Sink;
 // Both ends of a bond (lo, hi) at once: contributions are routed to each
 // end's record exactly as two single-end Sinks would route them (the same
 // additions in the same order), so one evaluation of the bond replaces two.
+// (Compiled into a different kernel, the arithmetic upstream may contract
+// multiply-adds differently, so the two modes agree to rounding.)
 template <class Real>
 struct PairSinkT {
   int a, b;          // lo, hi
