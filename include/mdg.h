@@ -173,6 +173,57 @@ int mdg_profile_read(mdg_ctx* ctx, int max, char* names, double* ms, int64_t* co
  * the bond-order kernels.  No reference counterpart. */
 int mdg_pipe_peak(int device, int fp32, double* tflops);
 
+/* ---- Parameters and the adjoint ----
+ * The adjoint differentiates a velocity-Verlet trajectory (the step of
+ * mdg_run) with respect to the initial positions and velocities and to the
+ * C-C pair parameters below; derived C-H / H-H parameters follow them as
+ * AIREBO::setupPotential derives them (AIREBO_LJ.cxx:229-247).  No
+ * counterpart in the reference (which has no gradients of trajectories);
+ * the parameters are those of REBO::setupPotential1 (REBO.cxx:859-938) and
+ * AIREBO::setupPotential (AIREBO_LJ.cxx:229-236), in Angstrom / eV. */
+#define MDG_PARAM_LJ_EPS_CC 0      /* AIREBO zeta_[C][C] (eV) */
+#define MDG_PARAM_LJ_SIGMA_CC 1    /* AIREBO sigma_[C][C] (Angstrom) */
+#define MDG_PARAM_REBO_A_CC 2      /* REBO A_[C][C] (eV) */
+#define MDG_PARAM_REBO_B1_CC 3     /* REBO B_[0][C][C] (eV) */
+#define MDG_PARAM_REBO_ALPHA_CC 4  /* REBO alpha_[C][C] (1/Angstrom) */
+#define MDG_PARAM_REBO_BETA1_CC 5  /* REBO beta_[0][C][C] (1/Angstrom) */
+#define MDG_NPARAM 6
+
+/* Set / read one parameter (Angstrom / eV).  Setting invalidates the stored
+ * accelerations and the captured step.  In the 3-sigma cutoff mode sigma_CC
+ * also sets the LJ list range and must be set before mdg_set_system. */
+int mdg_set_param(mdg_ctx* ctx, int id, double value);
+int mdg_get_param(mdg_ctx* ctx, int id, double* value);
+
+/* Products of the force field's derivatives at the current positions, for a
+ * direction u [n*3]: ju = J^T u (transpose != 0, what the adjoint uses) or
+ * J u (transpose = 0, the tangent-linear product) with J = d(grad)/dx the
+ * Jacobian of the gradient mdg_compute returns; grad = the exact gradient of
+ * the energy (it differs from mdg_compute's only by the reference's torsion
+ * derivative, AIREBO_ETors.cxx:110), de_dparam [MDG_NPARAM] = dE/dtheta and
+ * dprod_dparam [MDG_NPARAM] = d(u . grad)/dtheta.  Any output may be NULL.
+ * FP64 single-system REBO (+LJ) (+torsion) contexts in Angstrom/eV/fs. */
+int mdg_force_product(mdg_ctx* ctx, const double* u, int transpose, double* ju, double* grad, double* de_dparam,
+                      double* dprod_dparam);
+
+/* Forward run of the adjoint: nsteps velocity-Verlet steps of dt from the
+ * current state (the accelerations are recomputed from the positions first),
+ * keeping the state every checkpoint_every steps on the device.  Outputs (any
+ * may be NULL): pos [n*3] final positions UNWRAPPED (box position plus image
+ * count times the period), vel [n*3], epot = E_pot(x_N).  The context ends at
+ * the final state. */
+int mdg_adjoint_forward(mdg_ctx* ctx, int nsteps, double dt, int checkpoint_every, double* pos, double* vel,
+                        double* epot);
+
+/* Backward run for a loss L(x_N, v_N, E_pot(x_N)) of the last forward run:
+ * seeds dL/dx_N [n*3] and dL/dv_N [n*3] (NULL = zero) and dL/dE_pot.
+ * Outputs (any may be NULL): grad_params [MDG_NPARAM] = dL/dtheta,
+ * grad_pos0 = dL/dx_0, grad_vel0 = dL/dv_0.  Each segment between
+ * checkpoints is recomputed from its checkpoint; the context ends at the
+ * forward run's final state. */
+int mdg_adjoint_backward(mdg_ctx* ctx, const double* seed_pos, const double* seed_vel, double seed_epot,
+                         double* grad_params, double* grad_pos0, double* grad_vel0);
+
 /* REBO energy and gradient (plus the torsion term when with_torsion != 0)
  * for callers that cannot allocate device memory: hosts whose device memory
  * is all owned by their own allocator, which forbids driver allocations by

@@ -27,6 +27,16 @@ POT_ETORS = 4
 POT_BRENNER = 8
 POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
 
+# parameters the adjoint differentiates (include/mdg.h MDG_PARAM_*)
+PARAM_LJ_EPS_CC = 0
+PARAM_LJ_SIGMA_CC = 1
+PARAM_REBO_A_CC = 2
+PARAM_REBO_B1_CC = 3
+PARAM_REBO_ALPHA_CC = 4
+PARAM_REBO_BETA1_CC = 5
+NPARAM = 6
+PARAM_NAMES = ("eps_CC", "sigma_CC", "A_CC", "B1_CC", "alpha_CC", "beta1_CC")
+
 UNITS_AEVFS = 0
 UNITS_CGS = 1
 PREC_FP64 = 0
@@ -101,6 +111,11 @@ def lib():
         L.mdg_debug_brenner_tables.argtypes = [ctypes.c_int, dp, ctypes.c_int64]
         L.mdg_debug_brenner_tables.restype = ctypes.c_int64
         L.mdg_debug_spline.argtypes = [ctypes.c_int] * 4 + [dp, dp]
+        L.mdg_set_param.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.mdg_get_param.argtypes = [vp, ctypes.c_int, dp]
+        L.mdg_force_product.argtypes = [vp, dp, ctypes.c_int, dp, dp, dp, dp]
+        L.mdg_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+        L.mdg_adjoint_backward.argtypes = [vp, dp, dp, ctypes.c_double, dp, dp, dp]
         L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
         L.mdg_debug_rebo_tables.restype = ctypes.c_int64
         _lib = L
@@ -286,6 +301,47 @@ class Context:
         et = np.zeros(nsteps)
         _check(lib().mdg_step_host(self.h, nsteps, dt, _dp(pos), _dp(vel), _dp(ep), _dp(et)))
         return ep, et
+
+    # ---- parameters and the adjoint ----
+    def set_param(self, pid: int, value: float):
+        _check(lib().mdg_set_param(self.h, pid, float(value)))
+
+    def get_param(self, pid: int) -> float:
+        out = np.zeros(1)
+        _check(lib().mdg_get_param(self.h, pid, _dp(out)))
+        return float(out[0])
+
+    def force_product(self, u, transpose: bool = True) -> dict:
+        """At the current positions, for a direction u [n, 3]: J^T u (or J u
+        with transpose=False; J the Jacobian of the gradient) as "ju", the
+        exact energy gradient, dE/dtheta and d(u . grad)/dtheta."""
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
+        ju = np.zeros((self.n, 3))
+        g = np.zeros((self.n, 3))
+        de = np.zeros(NPARAM)
+        dp = np.zeros(NPARAM)
+        _check(lib().mdg_force_product(self.h, _dp(u), 1 if transpose else 0, _dp(ju), _dp(g), _dp(de), _dp(dp)))
+        return {"ju": ju, "grad": g, "de_dparam": de, "dprod_dparam": dp}
+
+    def adjoint_forward(self, nsteps: int, dt: float, checkpoint_every: int = 20):
+        """Forward run with checkpoints; returns (unwrapped final positions,
+        final velocities, E_pot at the final positions)."""
+        pos = np.zeros((self.n, 3))
+        vel = np.zeros((self.n, 3))
+        ep = np.zeros(1)
+        _check(lib().mdg_adjoint_forward(self.h, nsteps, dt, checkpoint_every, _dp(pos), _dp(vel), _dp(ep)))
+        return pos, vel, float(ep[0])
+
+    def adjoint_backward(self, seed_pos=None, seed_vel=None, seed_epot: float = 0.0):
+        """Gradients of a loss of the last forward run's final state:
+        returns (dL/dtheta [NPARAM], dL/dx0 [n, 3], dL/dv0 [n, 3])."""
+        sp = None if seed_pos is None else np.ascontiguousarray(seed_pos, dtype=np.float64).reshape(-1, 3)
+        sv = None if seed_vel is None else np.ascontiguousarray(seed_vel, dtype=np.float64).reshape(-1, 3)
+        gp = np.zeros(NPARAM)
+        gx = np.zeros((self.n, 3))
+        gv = np.zeros((self.n, 3))
+        _check(lib().mdg_adjoint_backward(self.h, _dp(sp), _dp(sv), float(seed_epot), _dp(gp), _dp(gx), _dp(gv)))
+        return gp, gx, gv
 
     def set_profiling(self, on: bool):
         _check(lib().mdg_set_profiling(self.h, 1 if on else 0))

@@ -323,3 +323,30 @@ def impact(seed: int, n_target: int = None, e_min_ev: float = 10.0, e_max_ev: fl
 def impact_batch(n_systems: int, seed: int = 0, **kw):
     """n_systems independent impact systems of uneven size (seeds seed, seed+1, ...)."""
     return [impact(seed + k, **kw) for k in range(n_systems)]
+
+
+def relax_hot(s: Dict[str, np.ndarray], steps: int, temp_k: float, dt: float, potentials: int,
+              seed: int = 0, device: int = 0) -> Dict[str, np.ndarray]:
+    """Pre-relaxation of a random packing: `steps` velocity-Verlet steps on
+    the GPU (mdg) with the velocities rescaled to temp_k after every step (a
+    seeded Maxwell-Boltzmann start).  Returns a copy of s with the relaxed,
+    wrapped positions and the final velocities."""
+    from mdtk_b200 import Context
+
+    rng = np.random.default_rng(seed)
+    out = dict(s)
+    vel = thermal_velocities(s["z"], temp_k, rng, s.get("fixed"))
+    ctx = Context(potentials=potentials, device=device)
+    ctx.set_system(s["z"], s["pos"], vel, s["box"], s["pbc"], s.get("fixed"))
+    for _ in range(steps):
+        ctx.run(1, dt, energies=False)
+        pos, v, _ = ctx.get_state()
+        t_now = temperature(s["z"], v, s.get("fixed"))
+        if t_now > 0:
+            v = v * math.sqrt(temp_k / t_now)
+        ctx.set_state(pos, v)
+    pos, v, _ = ctx.get_state()
+    ctx.close()
+    out["pos"] = pos
+    out["vel"] = v
+    return out

@@ -745,6 +745,10 @@ T* dalloc(size_t count)
 
 // ---------------------------------------------------------------- context
 
+namespace {
+struct AdjWs;  // adjoint-path buffers (mdg_adjoint.cuh)
+}
+
 struct mdg_ctx {
   mdg_params prm;
   ReboParams rp;
@@ -825,6 +829,7 @@ struct mdg_ctx {
   // host staging for mdg_step_host
   double4* h_stage = nullptr;
   std::vector<int> h_type;
+  AdjWs* adj = nullptr;       // adjoint path, allocated on first use
 
   State S() const
   {
@@ -941,8 +946,11 @@ int status_to_code(unsigned int st, std::string& msg)
   return code;
 }
 
+void adj_free(mdg_ctx* c);
+
 void free_system(mdg_ctx* c)
 {
+  adj_free(c);
   void* ptrs[] = {c->pos, c->vel, c->acc, c->grad, c->image, c->fixed, c->mass,
                   c->bb.nb, c->bb.bj, c->bb.brev, c->bb.brv, c->bb.bu, c->bb.bd, c->bb.nco,
                   c->fo.A, c->fo.W, c->fo.gown, c->fo.glj, c->fo.e_rebo, c->fo.e_tors, c->fo.e_lj,
@@ -1246,6 +1254,8 @@ int read_status(mdg_ctx* c)
 }
 
 }  // namespace
+
+#include "mdg_adjoint.cuh"
 
 // Lets the library's other translation units report through mdg_last_error().
 __attribute__((visibility("hidden"))) void mdg_set_last_error_internal(const char* msg) { g_err = msg; }

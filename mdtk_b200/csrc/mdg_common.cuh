@@ -84,6 +84,67 @@ MDG_HD double n_neg_tol(double) { return 1e-15; }
 MDG_HD double n_neg_tol(f32) { return 1e-5; }
 MDG_HD double dbl(f32 x) { return (double)x.v; }
 
+// Forward-mode dual number (value, tangent) of the adjoint path: the force
+// code run on duals whose position tangents are u gives, in the tangent of
+// every output, its derivative along u (the tangent of the gradient is the
+// Jacobian product J u).  Ordering compares values; equality compares value
+// and tangent, so a "skip when zero" test never drops a nonzero tangent.
+struct dual {
+  double v, d;
+  dual() = default;
+  MDG_HD dual(double x) : v(x), d(0.0) {}
+  MDG_HD dual(double x, double t) : v(x), d(t) {}
+  friend MDG_HD dual exp(dual a) { const double e = exp(a.v); return dual(e, e * a.d); }
+  friend MDG_HD dual sqrt(dual a) { const double s = sqrt(a.v); return dual(s, a.d / (2.0 * s)); }
+  friend MDG_HD dual cos(dual a) { return dual(cos(a.v), -sin(a.v) * a.d); }
+  friend MDG_HD dual sin(dual a) { return dual(sin(a.v), cos(a.v) * a.d); }
+  friend MDG_HD dual fabs(dual a) { return a.v < 0 ? dual(-a.v, -a.d) : a; }
+  friend MDG_HD dual pow(dual a, double b) { return dual(pow(a.v, b), b * pow(a.v, b - 1.0) * a.d); }
+};
+MDG_HD dual operator+(dual a, dual b) { return dual(a.v + b.v, a.d + b.d); }
+MDG_HD dual operator-(dual a, dual b) { return dual(a.v - b.v, a.d - b.d); }
+MDG_HD dual operator*(dual a, dual b) { return dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+MDG_HD dual operator/(dual a, dual b) { const double q = a.v / b.v; return dual(q, (a.d - q * b.d) / b.v); }
+MDG_HD dual operator-(dual a) { return dual(-a.v, -a.d); }
+MDG_HD dual& operator+=(dual& a, dual b) { a.v += b.v; a.d += b.d; return a; }
+MDG_HD dual& operator-=(dual& a, dual b) { a.v -= b.v; a.d -= b.d; return a; }
+MDG_HD dual& operator*=(dual& a, dual b) { a = a * b; return a; }
+MDG_HD bool operator<(dual a, dual b) { return a.v < b.v; }
+MDG_HD bool operator>(dual a, dual b) { return a.v > b.v; }
+MDG_HD bool operator<=(dual a, dual b) { return a.v <= b.v; }
+MDG_HD bool operator>=(dual a, dual b) { return a.v >= b.v; }
+MDG_HD bool operator==(dual a, dual b) { return a.v == b.v && a.d == b.d; }
+MDG_HD bool operator!=(dual a, dual b) { return !(a == b); }
+MDG_HD dual dbl(dual x) { return x; }
+MDG_HD double n_neg_tol(dual) { return 1e-15; }
+// value of a scalar (for indices and types stored in floating-point fields)
+MDG_HD double val(double x) { return x; }
+MDG_HD double val(dual x) { return x.v; }
+
+// A dual vector's values with zero tangents.
+template <class Real>
+MDG_HD Real value_only(Real x) { return Real(val(x)); }
+
+// The wide type of an arithmetic type: what its results are stored and
+// accumulated in (double for the FP64 and FP32-mixed paths, dual on the
+// adjoint path).
+template <class Real> struct Wide { typedef double T; };
+template <> struct Wide<dual> { typedef dual T; };
+
+template <class T> struct IsDual { static constexpr bool v = false; };
+template <> struct IsDual<dual> { static constexpr bool v = true; };
+
+// Four wide scalars (x, y, z, w) of a stored record: double4 on the FP64 and
+// mixed paths.
+struct dual4 {
+  dual x, y, z, w;
+};
+template <class W> struct Q4T { typedef double4 T; };
+template <> struct Q4T<dual> { typedef dual4 T; };
+MDG_HD dual4 make_dual4(dual x, dual y, dual z, dual w) { dual4 r; r.x = x; r.y = y; r.z = z; r.w = w; return r; }
+MDG_HD double4 make_q4(double x, double y, double z, double w) { return make_double4(x, y, z, w); }
+MDG_HD dual4 make_q4(dual x, dual y, dual z, dual w) { return make_dual4(x, y, z, w); }
+
 template <class T> struct Id { typedef T type; };
 
 template <class Real>
@@ -98,9 +159,14 @@ MDG_HD V3T<Real> v3r(Real x, Real y, Real z) { V3T<Real> r; r.x = x; r.y = y; r.
 template <class Real>
 MDG_HD V3T<Real> xyz(double4 q) { return v3r<Real>(Real(q.x), Real(q.y), Real(q.z)); }
 template <class Real>
+MDG_HD V3T<Real> xyz(const dual4& q) { return v3r<Real>(Real(q.x), Real(q.y), Real(q.z)); }
+template <class Real>
 MDG_HD V3T<Real> cvt3(V3 a) { return v3r<Real>(Real(a.x), Real(a.y), Real(a.z)); }
 template <class Real>
-MDG_HD V3 to_d(V3T<Real> a) { return v3(dbl(a.x), dbl(a.y), dbl(a.z)); }
+MDG_HD V3T<typename Wide<Real>::T> to_d(V3T<Real> a)
+{
+  return v3r<typename Wide<Real>::T>(dbl(a.x), dbl(a.y), dbl(a.z));
+}
 template <class Real>
 MDG_HD V3T<Real> operator+(V3T<Real> a, V3T<Real> b) { return v3r<Real>(a.x + b.x, a.y + b.y, a.z + b.z); }
 template <class Real>
@@ -142,6 +208,21 @@ MDG_HD double norm2(V3 a)
 }
 template <class Real>
 MDG_HD Real SQR(Real x) { return x * x; }
+template <class Real>
+MDG_HD V3T<Real> values_of(V3T<Real> a) { return v3r<Real>(value_only(a.x), value_only(a.y), value_only(a.z)); }
+
+// Parameters the adjoint differentiates (their order in gradients), the
+// C-C pair parameters of the LJ term (AIREBO_LJ.cxx:229-247) and of REBO's
+// V_R / V_A (REBO.cxx:859-938).
+enum ParamId : int {
+  kParLJEps = 0,      // epsilon_CC (AIREBO's zeta_)
+  kParLJSigma = 1,    // sigma_CC
+  kParReboA = 2,      // A_CC
+  kParReboB1 = 3,     // B1_CC
+  kParReboAlpha = 4,  // alpha_CC
+  kParReboBeta1 = 5,  // beta1_CC
+  kNParam = 6
+};
 
 // Periodic box: only uniform per-axis periodicity (every atom shares the
 // array's PBC, as AtomsArray::PBC sets it, mdtk/AtomsContainer.cxx:43-54).
@@ -212,6 +293,11 @@ struct LJParams {
   double RLJ[2][2][2];    // S(t_r) window: [sigma, 2^(1/6) sigma]
   double R[2][2][2];      // LJ cosine cutoff window
   double b[2][2][2];      // S(t_b) window on b*_ij
+  // chain factors of the adjoint's parameters: d sigma_ab / d sigma_CC,
+  // d eps_ab / d eps_CC (sigma_CH is the mean, eps_CH the geometric mean),
+  // and d R_ab / d sigma_ab of the cutoff window (3 in the 3-sigma mode)
+  double dsig[2][2], deps[2][2];
+  double dcut;
 };
 
 // ETors parameters (ETors::setupPotential, AIREBO_ETors.cxx:125-133).

@@ -4,9 +4,11 @@
 // with its first-order adjoint.
 #pragma once
 
-#include "mdg_rebo.cuh"
+#include "mdg_step.cuh"
 
 namespace mdg {
+
+inline void set_lj_chain(LJParams& p, int lj_cut_mode);
 
 // AIREBO::setupPotential (AIREBO_LJ.cxx:219-287), A / eV.  lj_cut_mode 1
 // replaces the cosine cutoff window by [3 sigma - 0.5, 3 sigma].
@@ -41,27 +43,72 @@ inline void set_lj_params(LJParams& p, int lj_cut_mode)
   p.b[C][C][1] = 0.81;
   p.b[H][H][1] = 0.42;
   p.b[C][H][1] = p.b[H][C][1] = 0.90;
+  set_lj_chain(p, lj_cut_mode);
+}
+
+// Chain factors of the derived C-H / H-H parameters by sigma_CC and eps_CC
+// (sigma_CH = (sigma_CC + sigma_HH)/2, eps_CH = sqrt(eps_CC eps_HH),
+// AIREBO_LJ.cxx:229-247), and of the 3-sigma cutoff window.
+inline void set_lj_chain(LJParams& p, int lj_cut_mode)
+{
+  const int C = kC, H = kH;
+  p.dsig[C][C] = 1.0;
+  p.dsig[C][H] = p.dsig[H][C] = 0.5;
+  p.dsig[H][H] = 0.0;
+  p.deps[C][C] = 1.0;
+  p.deps[C][H] = p.deps[H][C] = p.eps[C][H] / (2.0 * p.eps[C][C]);
+  p.deps[H][H] = 0.0;
+  p.dcut = lj_cut_mode == 1 ? 3.0 : 0.0;
+}
+
+// Sets sigma_CC or eps_CC and re-derives what depends on them as
+// AIREBO::setupPotential does (AIREBO_LJ.cxx:229-262).
+inline void set_lj_cc(LJParams& p, int lj_cut_mode, double sigma_cc, double eps_cc)
+{
+  const int C = kC, H = kH;
+  p.sigma[C][C] = sigma_cc;
+  p.sigma[C][H] = p.sigma[H][C] = 0.5 * (p.sigma[C][C] + p.sigma[H][H]);
+  p.eps[C][C] = eps_cc;
+  p.eps[C][H] = p.eps[H][C] = sqrt(p.eps[C][C] * p.eps[H][H]);
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      p.RLJ[a][b][0] = p.sigma[a][b];
+      p.RLJ[a][b][1] = p.sigma[a][b] * pow(2.0, 1.0 / 6.0);
+    }
+  if (lj_cut_mode == 1)
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++) {
+        p.R[a][b][1] = 3.0 * p.sigma[a][b];
+        p.R[a][b][0] = p.R[a][b][1] - 0.5;
+      }
+  set_lj_chain(p, lj_cut_mode);
 }
 
 // Connectivity table of atom i: every atom reachable over at most three REBO
 // bonds with the largest product of bond cutoffs w and the path that gives
 // it (AIREBO::fill_Cij, AIREBO_LJ.cxx:289-367), sorted by target.
-struct CijTable {
+// W: double, or dual on the adjoint path (the same entries, w with its tangent).
+template <class W>
+struct CijTableT {
   int cap;
   int* cnt;        // [n]
   int4* ent;       // [n * cap] x = target, y = path length, z = k, w = m
-  double* w;       // [n * cap]
+  W* w;            // [n * cap]
 };
+typedef CijTableT<double> CijTable;
 
 // The middle bond k-m of a 3-bond connectivity path i-k-m-j belongs to
 // neither end of the LJ pair; its gradient is returned with the pair's task
 // (written by the lower-index end) and gathered later by k and m.
-struct MidOut {
+template <class W>
+struct MidOutT {
   int k, sm, m, valid;  // sm = slot of m in k's bond list
-  double c;             // dE/dr of the bond k-m
+  W c;                  // dE/dr of the bond k-m
 };
+typedef MidOutT<double> MidOut;
 
-MDG_HD int bond_slot(const BondList& B, int c, int k)
+template <class W>
+MDG_HD int bond_slot(const BondListT<W>& B, int c, int k)
 {
   const int nb = B.nb[c];
   for (int s = 0; s < nb; s++)
@@ -144,7 +191,8 @@ MDG_HD void cij_build_atom(const BondList& B, CijTable& T, int i, unsigned int* 
 
 // Lookup of target j in the table of i (binary search).  Returns the entry
 // index or -1.
-MDG_HD int cij_find(const CijTable& T, int i, int j)
+template <class W>
+MDG_HD int cij_find(const CijTableT<W>& T, int i, int j)
 {
   int lo = 0, hi = T.cnt[i] - 1;
   const int4* e = T.ent + (long)i * T.cap;
@@ -181,34 +229,59 @@ MDG_HD Real dSlj(Real arg, double amin, double amax)
 // The powers of s/r are taken in double from the double length on every path
 // (a float length would carry 12 x its rounding into (s/r)^12).
 template <class Real, class S>
-MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairGT<Real>& pl, Real V, S& sink, double& lj,
-                double& val)
+MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairGT<Real>& pl, Real V, S& sink,
+                typename Wide<Real>::T& lj, typename Wide<Real>::T& val)
 {
+  typedef typename Wide<Real>::T Wd;
   const Real fv = pl.f;
   lj = 0.0;
   val = 0.0;
   if (fv == 0.0) return;
-  const double r = pl.rd;
+  const Wd r = pl.rd;
   const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
-  const double sdr = sigma / r;
-  double s6 = sdr;
+  const Wd sdr = sigma / r;
+  Wd s6 = sdr;
   for (int q = 2; q <= 6; q++) s6 *= sdr;
-  const double s12 = s6 * s6;
-  const double vd = 4.0 * zeta * (s12 - s6);
+  const Wd s12 = s6 * s6;
+  const Wd vd = 4.0 * zeta * (s12 - s6);
   val = vd;
   if (V != 0.0) {
-    const double der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
+    const Wd der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
     sink.pair(i, j, pl.u * Real(der * dbl(fv) * dbl(V)));
     if (pl.df != 0.0) sink.pair(i, j, pl.u * Real((vd * dbl(V)) * dbl(pl.df)));
   }
   lj = dbl(fv) * vd;
 }
 
+// Derivatives of one LJ pair energy E = C SrSb f vd by eps_CC and sigma_CC
+// (adjoint path): E is linear in eps; sigma enters vd = 4 eps ((s/r)^12 -
+// (s/r)^6), the S(t_r) window [sigma, 2^(1/6) sigma] (d Str / d sigma =
+// -dS/dr r / sigma) and, in the 3-sigma mode, the cutoff window
+// (d f / d sigma = -3 df/dr).
+template <class Real, class S, class Wd>
+MDG_HD void lj_par(const LJParams& P, int ti, int tj, int lo, const PairGT<Real>& pl, Wd C, Wd SrSb, Wd dSrSb_ds,
+                   Wd vd, S& sink)
+{
+  const double fs = P.dsig[ti][tj], fe = P.deps[ti][tj];
+  if (fs == 0.0 && fe == 0.0) return;
+  const Wd r = pl.rd, f = dbl(pl.f), df = dbl(pl.df);
+  const double sigma = P.sigma[ti][tj], eps = P.eps[ti][tj];
+  const Wd sdr = sigma / r;
+  Wd s6 = sdr;
+  for (int q = 2; q <= 6; q++) s6 *= sdr;
+  const Wd s12 = s6 * s6;
+  const Wd dvd = 4.0 * eps * (12.0 * s12 - 6.0 * s6) / sigma;
+  const Wd dLJ = f * dvd - P.dcut * df * vd;
+  sink.par(lo, kParLJEps, fe * (C * SrSb * f * vd / eps));
+  sink.par(lo, kParLJSigma, fs * (C * (SrSb * dLJ + f * vd * dSrSb_ds)));
+}
+
 template <class Real, class TB>
 struct LJT {
+  typedef typename Wide<Real>::T Wd;
   const LJParams& P;
   const ReboT<Real, TB>& R;
-  const CijTable& T;
+  const CijTableT<Wd>& T;
 
   // b*_ij: REBO's b_ij average for the pair with r_alter = R1 of REBO
   // (AIREBO::BijAsterix, AIREBO_LJ.cxx:191-202).
@@ -228,11 +301,11 @@ struct LJT {
   // energy; the middle bond of a 3-bond path is recorded through `mid` when
   // non-null (the i end passes it).
   template <class S>
-  MDG_HD Real pair(int i, int j, const PairGT<Real>& pl, S& sink, MidOut* mid, unsigned int* status) const
+  MDG_HD Real pair(int i, int j, const PairGT<Real>& pl, S& sink, MidOutT<Wd>* mid, unsigned int* status) const
   {
     // connectivity (AIREBO::Cij, AIREBO_LJ.cxx:381-408)
     int e = cij_find(T, i, j);
-    double w = 0.0;
+    Wd w = 0.0;
     int4 path = make_int4(j, 0, -1, -1);
     if (e >= 0) {
       w = T.w[(long)i * T.cap + e];
@@ -242,14 +315,14 @@ struct LJT {
     // double on every path: 1 - w and 1 - S(t_r) cancel to ~1e-3 here, which
     // float would turn into 1e-5 relative errors of the pair force.  Only b*
     // and the vectors handed to the sink use the arithmetic type.
-    const double C = 1 - w;
+    const Wd C = 1 - w;
     if (!(C > 0.0)) return 0.0;
     const int ti = R.type(i), tj = R.type(j);
-    const double r = pl.rd;
+    const Wd r = pl.rd;
     // StrStb value (AIREBO_LJ.cxx:79-114)
     const double rmin = P.RLJ[ti][tj][0], rmax = P.RLJ[ti][tj][1];
-    const double Str = Slj(r, rmin, rmax);
-    double Stb = 0.0, bij = 0.0, SrSb = 1.0;
+    const Wd Str = Slj(r, rmin, rmax);
+    Wd Stb = 0.0, bij = 0.0, SrSb = 1.0;
     SinkT<Real> dummy;
     if (Str != 0.0) {
       bij = dbl(bstar(i, j, pl, Real(0.0), dummy));
@@ -258,28 +331,32 @@ struct LJT {
     }
     // VLJ with seed SrSb*C
     if (pl.f == 0.0) return 0.0;
-    double LJv, val;
+    Wd LJv, val;
     vlj(P, ti, tj, i, j, pl, Real(SrSb * C), sink, LJv, val);
+    if constexpr (S::kAdj) {
+      const Wd dSrSb = (Str != 0.0) ? dSlj(r, rmin, rmax) * (r / P.sigma[ti][tj]) * (1.0 - Stb) : Wd(0.0);
+      lj_par(P, ti, tj, i, pl, C, SrSb, dSrSb, val, sink);
+    }
     // StrStb gradient with seed C*LJ
-    const double V2 = C * LJv;
+    const Wd V2 = C * LJv;
     if (Str != 0.0 && V2 != 0.0) {
-      const double dStr = dSlj(r, rmin, rmax);
+      const Wd dStr = dSlj(r, rmin, rmax);
       if (dStr != 0.0) sink.pair(i, j, pl.u * Real(-dStr * V2));
-      const double dStb = dSlj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
+      const Wd dStb = dSlj(bij, P.b[ti][tj][0], P.b[ti][tj][1]);
       if (dStr != 0.0 && Stb != 0.0) sink.pair(i, j, pl.u * Real(dStr * Stb * V2));
       if (dStb != 0.0) bstar(i, j, pl, Real(Str * dStb * V2), sink);
     }
     // Cij gradient with seed Vc3 = SrSb*LJ: -V * (product of the other cutoffs) * df
-    const double Vc3 = SrSb * LJv;
+    const Wd Vc3 = SrSb * LJv;
     if (e >= 0 && Vc3 != 0.0 && path.y > 0) {
-      const BondList& B = R.B;
+      const auto& B = R.B;
       if (path.y == 1) {
         int s = bond_slot(B, i, j);
         if (s >= 0) {
           const int q = i * B.mb + s;
-          const double df = B.bd[q].x;
+          const Wd df = B.bd[q].x;
           if (df != 0.0) {
-            double4 u = B.bu[q];
+            const auto u = B.bu[q];
             sink.pair(i, j, xyz<Real>(u) * Real((-1.0 * Vc3) * df));
           }
         }
@@ -291,8 +368,8 @@ struct LJT {
         const int sj = bond_slot(B, j, last);
         if (s1 < 0 || sj < 0) { *status |= ST_CIJ_OVERFLOW; return 0.0; }
         const int q1 = i * B.mb + s1, qj = j * B.mb + sj;
-        const double f1 = B.bu[q1].w, fl = B.bu[qj].w;
-        double fmid = 1.0, dfmid = 0.0;
+        const Wd f1 = B.bu[q1].w, fl = B.bu[qj].w;
+        Wd fmid = 1.0, dfmid = 0.0;
         int sm = -1, qm = -1;
         if (path.y == 3) {
           sm = bond_slot(B, k, m);
@@ -302,19 +379,19 @@ struct LJT {
           dfmid = B.bd[qm].x;
         }
         // products in path order (AIREBO_LJ.cxx:396-402)
-        const double m1 = (path.y == 2) ? 1.0 * fl : 1.0 * fmid * fl;
-        const double ml = (path.y == 2) ? 1.0 * f1 : 1.0 * f1 * fmid;
-        const double df1 = B.bd[q1].x, dfl = B.bd[qj].x;
+        const Wd m1 = (path.y == 2) ? 1.0 * fl : 1.0 * fmid * fl;
+        const Wd ml = (path.y == 2) ? 1.0 * f1 : 1.0 * f1 * fmid;
+        const Wd df1 = B.bd[q1].x, dfl = B.bd[qj].x;
         if (df1 != 0.0) {
-          double4 u = B.bu[q1];
+          const auto u = B.bu[q1];
           sink.cbond(i, s1, xyz<Real>(u) * Real((-m1 * Vc3) * df1));
         }
         if (dfl != 0.0) {
-          double4 u = B.bu[qj];
+          const auto u = B.bu[qj];
           sink.cbond(j, sj, xyz<Real>(u) * Real((-ml * Vc3) * dfl));
         }
         if (path.y == 3 && dfmid != 0.0 && mid) {
-          const double mm = 1.0 * f1 * fl;
+          const Wd mm = 1.0 * f1 * fl;
           mid->k = k;
           mid->sm = sm;
           mid->m = m;
@@ -332,7 +409,8 @@ typedef LJT<double, ReboTables> LJ;
 // Special LJ pairs (those needing b*_ij or a connectivity gradient) are
 // evaluated one task per (atom, pair); each task writes its own record and a
 // per-atom pass sums an atom's records in list order.
-struct SpecialTasks {
+template <class W>
+struct SpecialTasksT {
   int cap;          // special pairs per atom
   int task_cap;     // total tasks
   long rec_cap;     // total record doubles
@@ -343,24 +421,53 @@ struct SpecialTasks {
   int* roff;        // [n + 1] exclusive prefix of rsz
   int2* flat;       // [task_cap] (atom, partner)
   long* trec;       // [task_cap] record offset of each task
-  double* rec;      // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]
+  W* rec;           // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]
   int4* mid;        // [task_cap] middle-bond output (k, slot of m in k, m, valid)
-  double* midc;     // [task_cap]
+  W* midc;          // [task_cap]
+  W* dp;            // [task_cap * kNParam] energy derivatives by parameter (adjoint path only)
   // one evaluation per pair (the lower-index end's task writes both records):
   int* work;        // [task_cap] tasks whose owner is the lower index
   int* wrev;        // [task_cap] the partner's task of the same pair (-1: none)
   unsigned long long* wcnt;  // number of work items
 };
+typedef SpecialTasksT<double> SpecialTasks;
 
 // Record size of a task owned by an atom with nb bonds.
 MDG_HD int rec_size(int nb) { return 4 + 4 * nb; }
 
+// Geometry of a pair lo -> hi (rv = x_lo - x_hi, r = |rv| as the FP64 path
+// computes them) in the arithmetic type; on the adjoint path with the
+// tangents of rv and r along the position tangents tan.
+template <class Real>
+MDG_HD PairGT<Real> pair_geom(V3 rv, double r, const double4* tan, int lo, int hi)
+{
+  PairGT<Real> p;
+  if constexpr (IsDual<Real>::v) {
+    const double4 tl = tan[lo], th = tan[hi];
+    const V3 dv = v3(tl.x - th.x, tl.y - th.y, tl.z - th.z);
+    const dual rr(r, (rv.x * dv.x + rv.y * dv.y + rv.z * dv.z) / r);
+    p.rv = v3r<dual>(dual(rv.x, dv.x), dual(rv.y, dv.y), dual(rv.z, dv.z));
+    p.r = rr;
+    p.rd = rr;
+    p.u = p.rv / rr;
+  } else {
+    p.rv = cvt3<Real>(rv);
+    p.r = r;
+    p.rd = r;
+    p.u = cvt3<Real>(rv / r);
+  }
+  p.alter = 0;
+  p.ralt = 0.0;
+  return p;
+}
+
 // Classifies one LJ pair seen from atom a: returns 0 (skip), 1 (plain: C = 1
 // and S(t_r) = 0, so E = VLJ) or 2 (special).  For plain pairs adds the own
-// gradient and, at the lower end, the energy.
-template <class Real, class S>
-MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, int a, int b, V3 xa, int ta,
-                         S& sink, double& e)
+// gradient and, at the lower end, the energy.  The classification is made in
+// double on every path (the adjoint path's pairs are the FP64 path's).
+template <class Real, class S, class W>
+MDG_HD int lj_plain_pair(const LJParams& P, const CijTableT<W>& T, const State& St, int a, int b, V3 xa, int ta,
+                         S& sink, W& e, const double4* tan = nullptr)
 {
   const double4 pb = St.pos[b];
   const int tb = (int)pb.w;
@@ -373,33 +480,29 @@ MDG_HD int lj_plain_pair(const LJParams& P, const CijTable& T, const State& St, 
   const double R1 = P.R[ta][tb][0], R2 = P.R[ta][tb][1];
   if (d2 > R2 * R2) return 0;
   const int ei = cij_find(T, lo, hi);
-  const double w = ei >= 0 ? T.w[(long)lo * T.cap + ei] : 0.0;
+  const double w = ei >= 0 ? val(T.w[(long)lo * T.cap + ei]) : 0.0;
   const double C = 1 - w;
   if (!(C > 0.0)) return 0;
   const double r = sqrt(d2);
   const double Str = Slj(r, P.RLJ[ta][tb][0], P.RLJ[ta][tb][1]);
   if (Str != 0.0 || w != 0.0) return 2;
   // the pair term itself in the arithmetic type
-  PairGT<Real> p;
-  p.rv = cvt3<Real>(rv);
-  p.r = r;
-  p.rd = r;
-  p.u = cvt3<Real>(rv / r);
+  PairGT<Real> p = pair_geom<Real>(rv, r, tan, lo, hi);
   cutoff(p.r, R1, R2, p.f, p.df);
-  p.alter = 0;
-  p.ralt = 0.0;
-  double LJv, val;
+  W LJv, val;
   const int tlo = lo == a ? ta : tb, thi = lo == a ? tb : ta;
   vlj(P, tlo, thi, lo, hi, p, Real(1.0 * C), sink, LJv, val);
+  if constexpr (S::kAdj) lj_par(P, tlo, thi, lo, p, W(C), W(1.0), W(0.0), val, sink);
   if (a == lo) e += 1.0 * C * LJv;
   return 1;
 }
 
 // Gradient owed to atom a by middle bonds k-m of connectivity paths (a as k
 // or as m); the tasks of every bond partner lo of k are scanned in order.
-MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
+template <class W>
+MDG_HD V3T<W> mid_gather_atom(const BondListT<W>& B, const SpecialTasksT<W>& X, int a)
 {
-  V3 g = v3(0, 0, 0);
+  V3T<W> g = v3r<W>(0.0, 0.0, 0.0);
   const int nb = B.nb[a];
   for (int s = 0; s < nb; s++) {
     const int lo = B.bj[a * B.mb + s];
@@ -407,13 +510,13 @@ MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
     for (int t = t0; t < t1; t++) {
       int4 e = X.mid[t];
       if (!e.w || e.x != a) continue;
-      double4 u = B.bu[a * B.mb + e.y];
-      g += v3(u.x, u.y, u.z) * X.midc[t];
+      const auto u = B.bu[a * B.mb + e.y];
+      g += v3r<W>(u.x, u.y, u.z) * X.midc[t];
     }
   }
   for (int s = 0; s < nb; s++) {
     const int k = B.bj[a * B.mb + s];
-    double4 ua = B.bu[a * B.mb + s];
+    const auto ua = B.bu[a * B.mb + s];
     const int nbk = B.nb[k];
     for (int q = 0; q < nbk; q++) {
       const int lo = B.bj[k * B.mb + q];
@@ -421,7 +524,7 @@ MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
       for (int t = t0; t < t1; t++) {
         int4 e = X.mid[t];
         if (!e.w || e.x != k || e.z != a) continue;
-        g += v3(ua.x, ua.y, ua.z) * X.midc[t];
+        g += v3r<W>(ua.x, ua.y, ua.z) * X.midc[t];
       }
     }
   }
@@ -429,20 +532,33 @@ MDG_HD V3 mid_gather_atom(const BondList& B, const SpecialTasks& X, int a)
 }
 
 // Records one special task: the full pair term from end a with a private sink.
-template <class Real, class TB>
-MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTasks& Tk, int t, unsigned int* status)
+// ADJ: the adjoint path (duals with position tangents tan; the task's
+// parameter derivatives go to Tk.dp).
+template <bool ADJ = false, class Real, class TB>
+MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTasksT<typename Wide<Real>::T>& Tk, int t,
+                            unsigned int* status, const double4* tan = nullptr)
 {
+  typedef typename Wide<Real>::T Wd;
   const int2 ap = Tk.flat[t];
   const int a = ap.x, b = ap.y;
   const int nba = X.R.B.nb[a];
   const long ro = Tk.trec[t];
-  if (ro < 0) return;  // beyond the record capacity (already flagged)
-  double* rec = Tk.rec + ro;
-  SinkT<Real> sink;
+  if (ro < 0) {  // beyond the record capacity (already flagged): no middle bond either
+    Tk.mid[t] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  Wd* rec = Tk.rec + ro;
+  SinkT<Real, ADJ> sink;
   sink.a = a;
-  sink.g = v3(0, 0, 0);
+  sink.g = v3r<Wd>(0.0, 0.0, 0.0);
   sink.A = rec + 4;
   sink.W = rec + 4 + 3 * nba;
+  sink.dp = nullptr;
+  sink.jt = 1;
+  if constexpr (ADJ) {
+    sink.dp = Tk.dp + (long)t * kNParam;
+    for (int k = 0; k < kNParam; k++) sink.dp[k] = 0.0;
+  }
   for (int s = 0; s < nba; s++) {
     sink.A[3 * s] = sink.A[3 * s + 1] = sink.A[3 * s + 2] = 0.0;
     sink.W[s] = 0.0;
@@ -455,23 +571,17 @@ MDG_HD void lj_special_task(const LJT<Real, TB>& X, const State& St, SpecialTask
   else { lo = b; hi = a; rv = depos(box, v3(pb.x, pb.y, pb.z), v3(pa.x, pa.y, pa.z)); }
   const int tlo = (int)St.pos[lo].w, thi = (int)St.pos[hi].w;
   const double r = sqrt(norm2(rv));
-  PairGT<Real> p;
-  p.rv = cvt3<Real>(rv);
-  p.r = r;
-  p.rd = r;
-  p.u = cvt3<Real>(rv / r);
+  PairGT<Real> p = pair_geom<Real>(rv, r, tan, lo, hi);
   cutoff(p.r, X.P.R[tlo][thi][0], X.P.R[tlo][thi][1], p.f, p.df);
-  p.alter = 0;
-  p.ralt = 0.0;
-  MidOut mo;
+  MidOutT<Wd> mo;
   mo.valid = 0;
   const Real E = X.pair(lo, hi, p, sink, (a == lo) ? &mo : nullptr, status);
   rec[0] = sink.g.x;
   rec[1] = sink.g.y;
   rec[2] = sink.g.z;
-  rec[3] = (a == lo) ? dbl(E) : 0.0;
+  rec[3] = (a == lo) ? dbl(E) : Wd(0.0);
   Tk.mid[t] = make_int4(mo.k, mo.sm, mo.m, mo.valid);
-  Tk.midc[t] = mo.valid ? mo.c : 0.0;
+  Tk.midc[t] = mo.valid ? mo.c : Wd(0.0);
 }
 
 // One special pair (a < b) from task t of a and task t2 of b, written into
@@ -527,21 +637,25 @@ MDG_HD void lj_special_pair_task(const LJT<Real, TB>& X, const State& St, Specia
   Tk.midc[t2] = 0.0;
 }
 
-// Sums atom a's special-task records (in list order) into its accumulators.
-MDG_HD void lj_reduce_atom(const BondList& B, const SpecialTasks& Tk, ForceOut& O, int a)
+// Sums atom a's special-task records (in list order) into its accumulators
+// (and, on the adjoint path, the tasks' parameter derivatives).
+template <class Wd>
+MDG_HD void lj_reduce_atom(const BondListT<Wd>& B, const SpecialTasksT<Wd>& Tk, ForceOutT<Wd>& O, int a)
 {
   const int nb = B.nb[a];
-  double4 g0 = O.glj[a];
-  V3 g = v3(g0.x, g0.y, g0.z);
-  double e = O.e_lj[a];
-  double* A = O.A + (long)a * O.mb * 3;
-  double* W = O.W + (long)a * O.mb;
+  const auto g0 = O.glj[a];
+  V3T<Wd> g = v3r<Wd>(g0.x, g0.y, g0.z);
+  Wd e = O.e_lj[a];
+  Wd* A = O.A + (long)a * O.mb * 3;
+  Wd* W = O.W + (long)a * O.mb;
   const int t0 = Tk.off[a], t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
   for (int t = t0; t < t1; t++) {
     const long ro = Tk.trec[t];
     if (ro < 0) continue;
-    const double* rec = Tk.rec + ro;
-    g += v3(rec[0], rec[1], rec[2]);
+    if (O.dp && Tk.dp)
+      for (int k = 0; k < kNParam; k++) O.dp[(long)a * kNParam + k] += Tk.dp[(long)t * kNParam + k];
+    const Wd* rec = Tk.rec + ro;
+    g += v3r<Wd>(rec[0], rec[1], rec[2]);
     e += rec[3];
     for (int s = 0; s < nb; s++) {
       A[3 * s] += rec[4 + 3 * s];
@@ -550,7 +664,7 @@ MDG_HD void lj_reduce_atom(const BondList& B, const SpecialTasks& Tk, ForceOut& 
       W[s] += rec[4 + 3 * nb + s];
     }
   }
-  O.glj[a] = make_double4(g.x, g.y, g.z, 0.0);
+  O.glj[a] = make_q4(g.x, g.y, g.z, Wd(0.0));
   O.e_lj[a] = e;
 }
 

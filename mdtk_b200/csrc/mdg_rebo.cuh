@@ -22,16 +22,21 @@ namespace mdg {
 
 // Per-step bond list of the REBO range (pairs with |r| <= R2 of the pair),
 // ascending partner index, atom-major [a * mb + s].
-struct BondList {
+// W is the stored scalar: double, or dual on the adjoint path (values and
+// their tangents along the position direction of that pass).
+template <class W>
+struct BondListT {
+  typedef typename Q4T<W>::T Q4;
   int n, mb;
   const int* nb;        // bond count per atom
   const int* bj;        // partner index
   const int* brev;      // slot of this atom in the partner's list
-  const double4* brv;   // x_a - x_partner, w = |r|
-  const double4* bu;    // unit vector (x_a - x_partner)/|r|, w = f (R cutoff)
-  const double4* bd;    // x = df/dr, y = f' (Rprime cutoff), z = df'/dr
-  const double4* nco;   // per atom: Nt, NC, NH (sums of f over the bonds), w = type
+  const Q4* brv;        // x_a - x_partner, w = |r|
+  const Q4* bu;         // unit vector (x_a - x_partner)/|r|, w = f (R cutoff)
+  const Q4* bd;         // x = df/dr, y = f' (Rprime cutoff), z = df'/dr
+  const Q4* nco;        // per atom: Nt, NC, NH (sums of f over the bonds), w = type
 };
+typedef BondListT<double> BondList;
 
 // A pair vector as AtomsPair holds it (AtomsPair.hpp:35-160): rv = x_1 - x_2.
 // Real is the arithmetic type (double, or f32 on the mixed-precision path).
@@ -39,7 +44,7 @@ template <class Real>
 struct PairGT {
   V3T<Real> rv, u;    // vector and unit vector
   Real r, f, df;      // length and REBO cosine cutoff (R cutoffs of the pair types)
-  double rd;          // the length in double (the pair terms V_R, V_A use it on every path)
+  typename Wide<Real>::T rd;  // the length in the wide type (the pair terms V_R, V_A use it on every path)
   Real ralt;          // r_alter (b*_ij uses R1 of the pair, AIREBO_LJ.cxx:196-198)
   int alter;
 };
@@ -55,13 +60,27 @@ MDG_HD PairGT<Real> pair_reverse(const PairGT<Real>& p)
 }
 
 // Gradient routing for one evaluating atom.  Contributions arrive in the
-// arithmetic type and are accumulated in double.
-template <class Real>
+// arithmetic type and are accumulated in its wide type (double; dual on the
+// adjoint path).  ADJ marks the accumulating sink of the adjoint path: terms
+// then also record the derivatives of their energy with respect to the
+// differentiated parameters (par) and apply the corrections that turn the
+// forward Jacobian product of a non-gradient force into its transpose.
+template <class Real, bool ADJ = false>
 struct SinkT {
+  typedef typename Wide<Real>::T Wd;
+  static constexpr bool kAdj = ADJ;
   int a;           // evaluating atom
-  V3 g;            // dE/dx_a accumulated here
-  double* A;       // [mb*3] this atom's bond slots: gradient owed to each partner
-  double* W;       // [mb]   third-shell coefficients of this atom's bond slots
+  V3T<Wd> g;       // dE/dx_a accumulated here
+  Wd* A;           // [mb*3] this atom's bond slots: gradient owed to each partner
+  Wd* W;           // [mb]   third-shell coefficients of this atom's bond slots
+  Wd* dp;          // [kNParam] energy derivatives by parameter (ADJ only)
+  int jt;          // ADJ: 1 = tangents give J^T u (adjoint), 0 = J u (tangent-linear)
+  // d(energy)/d(parameter k), recorded by the lower-index end (the end that
+  // owns the term's energy)
+  MDG_HD void par(int lo, int k, Wd v)
+  {
+    if (ADJ && a == lo) dp[k] += v;
+  }
   MDG_HD void pair(int p, int q, V3T<Real> v)
   {
     if (p == a) g += to_d(v);
@@ -70,7 +89,7 @@ struct SinkT {
   MDG_HD void cbond(int c, int s, V3T<Real> v)
   {
     if (c == a) {
-      const V3 d = to_d(v);
+      const V3T<Wd> d = to_d(v);
       g += d;
       A[3 * s + 0] -= d.x;
       A[3 * s + 1] -= d.y;
@@ -91,6 +110,8 @@ typedef SinkT<double> Sink;
 // multiply-adds differently, so the two modes agree to rounding.)
 template <class Real>
 struct PairSinkT {
+  static constexpr bool kAdj = false;
+  MDG_HD void par(int, int, double) {}
   int a, b;          // lo, hi
   V3 ga, gb;
   double *Aa, *Wa, *Ab, *Wb;
@@ -126,19 +147,20 @@ struct PairSinkT {
 
 template <class Real, class TB>
 struct ReboT {
+  typedef typename Wide<Real>::T Wd;
   const ReboParams& P;
   const TB& T;
-  const BondList& B;
+  const BondListT<Wd>& B;
   unsigned int* status;
 
-  MDG_HD int type(int i) const { return (int)B.nco[i].w; }
+  MDG_HD int type(int i) const { return (int)val(B.nco[i].w); }
   MDG_HD double R2(int ti, int tj) const { return P.R[ti][tj][1]; }
 
   // ---- coordination numbers (REBO::Nt/NH/NC, REBO.cxx:423-502) ----
   // which: 0 = all neighbours (Nt), 1 = H only (NH), 2 = C only (NC).
   MDG_HD Real Nval(int c, int o, const PairGT<Real>& p, int which) const
   {
-    double4 n = B.nco[c];
+    const auto n = B.nco[c];
     Real N = which == 0 ? n.x : (which == 1 ? n.z : n.y);
     int to = type(o);
     bool sub = (which == 0) || (which == 1 && to == kH) || (which == 2 && to == kC);
@@ -166,7 +188,7 @@ struct ReboT {
       }
       Real df = B.bd[q].x;
       if (df != 0.0) {
-        double4 u = B.bu[q];
+        const auto u = B.bu[q];
         sink.cbond(c, s, xyz<Real>(u) * (V * df));
       }
     }
@@ -236,8 +258,8 @@ struct ReboT {
       const int q = c * B.mb + s;
       const int k = B.bj[q];
       if (k == o) continue;
-      double4 rv = B.brv[q];
-      double4 u = B.bu[q];
+      const auto rv = B.brv[q];
+      const auto u = B.bu[q];
       Real ex = expterm(c, o, p, k, rv.w);
       if (ex != 0.0) {
         Real gv = G(c, o, p, s, xyz<Real>(rv), rv.w, xyz<Real>(u), Nco, 0.0, dummy);
@@ -259,8 +281,8 @@ struct ReboT {
       const int q = c * B.mb + s;
       const int k = B.bj[q];
       if (k == o) continue;
-      double4 rv = B.brv[q];
-      double4 u = B.bu[q];
+      const auto rv = B.brv[q];
+      const auto u = B.bu[q];
       V3T<Real> brv = xyz<Real>(rv), bu3 = xyz<Real>(u);
       Real ex = expterm(c, o, p, k, rv.w);
       if (ex == 0.0) continue;
@@ -345,7 +367,7 @@ struct ReboT {
       const int q = c * B.mb + s;
       const int k = B.bj[q];
       if (k == o || type(k) != kC) continue;
-      double4 u = B.bu[q];
+      const auto u = B.bu[q];
       Real f = u.w;
       Real N = Nk_excl(k, B.brv[q].w, f, c);
       Real Sp = Sprime(N, P.Ntot[0], P.Ntot[1]);
@@ -385,7 +407,7 @@ struct ReboT {
       const int qi = i * B.mb + si;
       const int k = B.bj[qi];
       if (k == j) continue;
-      double4 rk = B.brv[qi];
+      const auto rk = B.brv[qi];
       const V3T<Real> b = xyz<Real>(rk);  // x_i - x_k
       for (int sj = 0; sj < nbj; sj++) {
         const int qj = j * B.mb + sj;
@@ -394,7 +416,7 @@ struct ReboT {
         if (k == l) continue;
         Real sin_ik = sqrt(norm2(cross(a, -b))) / (p.r * rk.w);
         if (fabs(sin_ik) < 0.1) continue;
-        double4 rl = B.brv[qj];
+        const auto rl = B.brv[qj];
         const V3T<Real> cc = xyz<Real>(rl);  // x_j - x_l
         Real sin_jl = sqrt(norm2(cross(a, -cc))) / (p.r * rl.w);
         if (fabs(sin_jl) < 0.1) continue;
@@ -427,12 +449,12 @@ struct ReboT {
           }
           Real vk = (1.0 - SQR(cdh)) * fjl * V;
           if (vk != 0.0 && rk.w >= P.Rp[ti][tk][0] && rk.w <= P.Rp[ti][tk][1]) {
-            double4 uk = B.bu[qi];
+            const auto uk = B.bu[qi];
             sink.cbond(i, si, xyz<Real>(uk) * (dSprime(Real(rk.w), P.Rp[ti][tk][0], P.Rp[ti][tk][1]) * vk));
           }
           Real vl = (1.0 - SQR(cdh)) * fik * V;
           if (vl != 0.0 && rl.w >= P.Rp[tj][tl][0] && rl.w <= P.Rp[tj][tl][1]) {
-            double4 ul = B.bu[qj];
+            const auto ul = B.bu[qj];
             sink.cbond(j, sj, xyz<Real>(ul) * (dSprime(Real(rl.w), P.Rp[tj][tl][0], P.Rp[tj][tl][1]) * vl));
           }
         }
@@ -503,21 +525,22 @@ struct ReboT {
 
   // ---- repulsive / attractive pair terms (REBO.cxx:134-198) ----
   // Return f*V_R and -f*V_A; with V != 0 route V * d/d(r_ij) to the pair.
-  // Evaluated in double from the double length on every path: their
-  // exponentials are the largest, most cancelling terms of the bond energy,
-  // and a float length alone would put ~alpha*r*eps_f of relative error into
-  // them.
+  // Evaluated in the wide type (double, or dual on the adjoint path) from the
+  // wide length on every path: their exponentials are the largest, most
+  // cancelling terms of the bond energy, and a float length alone would put
+  // ~alpha*r*eps_f of relative error into them.
   template <class S>
   MDG_HD Real VR(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
   {
     const Real f = p.f;
     if (f == 0.0) return 0.0;
     int ti = type(i), tj = type(j);
-    const double r = p.rd, Q = P.Q[ti][tj], A = P.A[ti][tj], al = P.alpha[ti][tj];
-    const double t1 = A * exp(-al * r);
-    const double val = (1 + Q / r) * t1;
+    const Wd r = p.rd;
+    const double Q = P.Q[ti][tj], A = P.A[ti][tj], al = P.alpha[ti][tj];
+    const Wd t1 = A * exp(-al * r);
+    const Wd val = (1 + Q / r) * t1;
     if (V != 0.0) {
-      const double der = -t1 * (Q + al * r * r + al * r * Q) / (r * r);
+      const Wd der = -t1 * (Q + al * r * r + al * r * Q) / (r * r);
       sink.pair(i, j, p.u * Real(der * dbl(f) * dbl(V)));
       if (p.df != 0.0) sink.pair(i, j, p.u * Real((val * dbl(V)) * dbl(p.df)));
     }
@@ -529,13 +552,13 @@ struct ReboT {
     const Real f = p.f;
     if (f == 0.0) return 0.0;
     int ti = type(i), tj = type(j);
-    const double r = p.rd;
-    const double t1 = P.B[0][ti][tj] * exp(-P.beta[0][ti][tj] * r);
-    const double t2 = P.B[1][ti][tj] * exp(-P.beta[1][ti][tj] * r);
-    const double t3 = P.B[2][ti][tj] * exp(-P.beta[2][ti][tj] * r);
-    const double val = t1 + t2 + t3;
+    const Wd r = p.rd;
+    const Wd t1 = P.B[0][ti][tj] * exp(-P.beta[0][ti][tj] * r);
+    const Wd t2 = P.B[1][ti][tj] * exp(-P.beta[1][ti][tj] * r);
+    const Wd t3 = P.B[2][ti][tj] * exp(-P.beta[2][ti][tj] * r);
+    const Wd val = t1 + t2 + t3;
     if (V != 0.0) {
-      const double der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
+      const Wd der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
       sink.pair(i, j, p.u * Real(-der * dbl(f) * dbl(V)));
       if (p.df != 0.0) sink.pair(i, j, p.u * Real((-val * dbl(V)) * dbl(p.df)));
     }
@@ -549,9 +572,26 @@ struct ReboT {
     SinkT<Real> dummy;
     Real vav = VA(i, j, p, 0.0, dummy);
     Real E = VR(i, j, p, 1.0, sink);
+    Real bav = 0.0;
     if (vav != 0.0) {
-      Real bav = baver(i, j, p, vav, sink);
+      bav = baver(i, j, p, vav, sink);
       E += bav * VA(i, j, p, bav, sink);
+    }
+    if constexpr (S::kAdj) {
+      // derivatives of this bond's energy by the C-C pair parameters: V_R is
+      // linear in A, V_A's first term in B1 (the bond order does not depend on
+      // A, alpha, B1, beta1)
+      if (type(i) == kC && type(j) == kC && p.f != 0.0) {
+        const Wd r = p.rd, f = dbl(p.f);
+        const double Q = P.Q[kC][kC], A = P.A[kC][kC], al = P.alpha[kC][kC];
+        const double B1 = P.B[0][kC][kC], be1 = P.beta[0][kC][kC];
+        const Wd eR = f * (1 + Q / r) * exp(-al * r);  // d(f V_R)/dA
+        const Wd e1 = f * exp(-be1 * r);                 // -d(f V_A)/dB1
+        sink.par(i, kParReboA, eR);
+        sink.par(i, kParReboAlpha, -r * A * eR);
+        sink.par(i, kParReboB1, -dbl(bav) * e1);
+        sink.par(i, kParReboBeta1, dbl(bav) * r * B1 * e1);
+      }
     }
     return E;
   }
@@ -560,10 +600,10 @@ typedef ReboT<double, ReboTables> Rebo;
 
 // Pair record of bond slot q of atom c (the pair c -> partner).
 template <class Real = double>
-MDG_HD PairGT<Real> pair_from_slot(const BondList& B, int q)
+MDG_HD PairGT<Real> pair_from_slot(const BondListT<typename Wide<Real>::T>& B, int q)
 {
   PairGT<Real> p;
-  double4 rv = B.brv[q], u = B.bu[q], d = B.bd[q];
+  const auto rv = B.brv[q], u = B.bu[q], d = B.bd[q];
   p.rv = xyz<Real>(rv);
   p.u = xyz<Real>(u);
   p.r = rv.w;

@@ -179,6 +179,114 @@ MDG_HD double t_value(const ReboTables& tb, int fam, double i, double j, double 
 }
 
 // ---------------------------------------------------------------------------
+// Dual arguments (adjoint path).  Values and first-derivative outputs are the
+// FP64 path's (the same cells, the same integer shortcut); tangents come from
+// the derivatives of the cell polynomials.  At an exact-integer argument the
+// second derivatives are taken from the cell the argument opens (the one the
+// non-integer path uses just above it).
+
+// d/dx of poly1(c, x, deriv)
+MDG_HD double poly1_dx(const double* c, double x, int deriv)
+{
+  double v = 0.0;
+  for (int t = 0; t < 6; t++) {
+    const int p = t - deriv;
+    if (c[t] == 0.0 || p < 1) continue;
+    v += c[t] * p * ipow(x, p - 1);
+  }
+  return v;
+}
+
+MDG_HD dual g_eval(const GSpline& g, dual cost, int deriv)
+{
+  int p = 0;
+  for (p = 0; p < g.npieces; p++)
+    if (cost.v <= g.x2[p]) break;
+  if (p >= g.npieces) p = g.npieces - 1;
+  const double* c = deriv ? g.df[p] : g.f[p];
+  return dual(poly1(c, cost.v, deriv), poly1_dx(c, cost.v, deriv) * cost.d);
+}
+
+// gradient of poly2(c, x0, x1, d) in (x0, x1)
+MDG_HD void poly2_grad(const double* c, double x0, double x1, int d, double* g)
+{
+  g[0] = g[1] = 0.0;
+  for (int t = 0; t < 16; t++) {
+    const double ct = c[t];
+    if (ct == 0.0) continue;
+    int p0 = t & 3, p1 = t >> 2;
+    if (d == 1) p0 -= 1;
+    if (d == 2) p1 -= 1;
+    if (p0 < 0 || p1 < 0) continue;
+    if (p0 >= 1) g[0] += ct * p0 * ipow(x0, p0 - 1) * ipow(x1, p1);
+    if (p1 >= 1) g[1] += ct * p1 * ipow(x0, p0) * ipow(x1, p1 - 1);
+  }
+}
+
+MDG_HD void p_eval(const ReboTables& tb, int fam, dual h, dual c, dual& v, dual& dh, dual& dc, unsigned int* status)
+{
+  double vv, dhv, dcv;
+  p_eval(tb, fam, h.v, c.v, vv, dhv, dcv, status);
+  double a[2] = {0.0, 0.0}, b[2] = {0.0, 0.0};
+  if (h.v >= 0 && c.v >= 0 && h.v < 4 && c.v < 4) {
+    const double* cell = tb.P[fam][(int)h.v][(int)c.v][0];
+    poly2_grad(cell + 16, h.v, c.v, 1, a);
+    poly2_grad(cell + 32, h.v, c.v, 2, b);
+  }
+  v = dual(vv, dhv * h.d + dcv * c.d);
+  dh = dual(dhv, a[0] * h.d + a[1] * c.d);
+  dc = dual(dcv, b[0] * h.d + b[1] * c.d);
+}
+
+MDG_HD dual p_value(const ReboTables& tb, int fam, dual h, dual c)
+{
+  dual v, dh, dc;
+  p_eval(tb, fam, h, c, v, dh, dc, nullptr);
+  return v;
+}
+
+// gradient of poly3(c, x0, x1, x2, d) in (x0, x1, x2)
+MDG_HD void poly3_grad(const double* c, double x0, double x1, double x2, int d, double* g)
+{
+  g[0] = g[1] = g[2] = 0.0;
+  for (int t = 0; t < 64; t++) {
+    const double ct = c[t];
+    if (ct == 0.0) continue;
+    int p0 = t & 3, p1 = (t >> 2) & 3, p2 = t >> 4;
+    if (d == 1) p0 -= 1;
+    if (d == 2) p1 -= 1;
+    if (d == 3) p2 -= 1;
+    if (p0 < 0 || p1 < 0 || p2 < 0) continue;
+    const double a0 = ipow(x0, p0), a1 = ipow(x1, p1), a2 = ipow(x2, p2);
+    if (p0 >= 1) g[0] += ct * p0 * ipow(x0, p0 - 1) * a1 * a2;
+    if (p1 >= 1) g[1] += ct * p1 * a0 * ipow(x1, p1 - 1) * a2;
+    if (p2 >= 1) g[2] += ct * p2 * a0 * a1 * ipow(x2, p2 - 1);
+  }
+}
+
+MDG_HD void t_eval(const ReboTables& tb, int fam, dual i, dual j, dual k, dual* out, unsigned int* status)
+{
+  double o[4];
+  t_eval(tb, fam, i.v, j.v, k.v, o, status);
+  double kv = k.v, kd = k.d;
+  if (kv > 15) { kv = 15; kd = 0.0; }
+  double h[4][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  if (i.v >= 0 && j.v >= 0 && k.v >= 1 && i.v < 4 && j.v < 4) {
+    const double* cell = tb.T[fam][(int)i.v][(int)j.v][(int)kv][0];
+    for (int q = 1; q < 4; q++) poly3_grad(cell + 64 * q, i.v, j.v, kv, q, h[q]);
+  }
+  out[0] = dual(o[0], o[1] * i.d + o[2] * j.d + o[3] * kd);
+  for (int q = 1; q < 4; q++) out[q] = dual(o[q], h[q][0] * i.d + h[q][1] * j.d + h[q][2] * kd);
+}
+
+MDG_HD dual t_value(const ReboTables& tb, int fam, dual i, dual j, dual k)
+{
+  dual o[4];
+  t_eval(tb, fam, i, j, k, o, nullptr);
+  return o[0];
+}
+
+// ---------------------------------------------------------------------------
 // FP32 tables of the mixed-precision path.  The FP64 tables above keep the
 // reference's monomials in absolute coordinates, whose terms cancel to ~1e-7
 // of their magnitude (sum |terms| ~3e6 in the pi_rc cells): float cannot

@@ -260,48 +260,64 @@ MDG_HD void brev_atom(BondBuild& B, int a)
   }
 }
 
-// Per-atom force-evaluation outputs.
-struct ForceOut {
+// Per-atom force-evaluation outputs (W: double, or dual on the adjoint path).
+template <class Ws>
+struct ForceOutT {
+  typedef typename Q4T<Ws>::T Q4;
   int mb;
-  double* A;        // [n * mb * 3] gradient owed to the partner of each bond slot
-  double* W;        // [n * mb]     third-shell coefficients
-  double4* gown;    // [n] own gradient (REBO + torsion kernel)
-  double4* glj;     // [n] own gradient (LJ kernels)
-  double* e_rebo;   // [n] per-atom energies (lower-index end of each bond)
-  double* e_tors;
-  double* e_lj;
+  Ws* A;            // [n * mb * 3] gradient owed to the partner of each bond slot
+  Ws* W;            // [n * mb]     third-shell coefficients
+  Q4* gown;         // [n] own gradient (REBO + torsion kernel)
+  Q4* glj;          // [n] own gradient (LJ kernels)
+  Ws* e_rebo;       // [n] per-atom energies (lower-index end of each bond)
+  Ws* e_tors;
+  Ws* e_lj;
+  Ws* dp;           // [n * kNParam] energy derivatives by parameter (adjoint path only)
+  int jt;           // adjoint path: 1 = J^T u, 0 = J u in the gradient's tangents
 };
+typedef ForceOutT<double> ForceOut;
 
 // REBO (+ torsion) for every bond of atom a, evaluated as the reference's
-// bond (min, max) and routed through a Sink for atom a.
-MDG_HD void rebo_atom(const Rebo& R, const TorsParams& TP, int do_rebo, int do_tors, ForceOut& O, int a)
+// bond (min, max) and routed through a Sink for atom a.  ADJ: the adjoint
+// path (duals; parameter derivatives into O.dp).
+template <bool ADJ = false, class Real, class TB>
+MDG_HD void rebo_atom(const ReboT<Real, TB>& R, const TorsParams& TP, int do_rebo, int do_tors,
+                      ForceOutT<typename Wide<Real>::T>& O, int a)
 {
-  const BondList& B = R.B;
-  Sink sink;
+  typedef typename Wide<Real>::T Wd;
+  const auto& B = R.B;
+  SinkT<Real, ADJ> sink;
   sink.a = a;
-  sink.g = v3(0, 0, 0);
+  sink.g = v3r<Wd>(0.0, 0.0, 0.0);
   sink.A = O.A + (long)a * O.mb * 3;
   sink.W = O.W + (long)a * O.mb;
+  sink.dp = nullptr;
+  sink.jt = 1;
+  if constexpr (ADJ) {
+    sink.jt = O.jt;
+    sink.dp = O.dp + (long)a * kNParam;
+    for (int k = 0; k < kNParam; k++) sink.dp[k] = 0.0;
+  }
   for (int s = 0; s < O.mb * 3; s++) sink.A[s] = 0.0;
   for (int s = 0; s < O.mb; s++) sink.W[s] = 0.0;
-  double er = 0.0, et = 0.0;
+  Wd er = 0.0, et = 0.0;
   const int nb = B.nb[a];
   for (int s = 0; s < nb; s++) {
     const int q = a * B.mb + s;
     const int b = B.bj[q];
-    PairG p = pair_from_slot(B, q);
+    PairGT<Real> p = pair_from_slot<Real>(B, q);
     int lo = a, hi = b;
     if (b < a) { lo = b; hi = a; p = pair_reverse(p); }
     if (do_rebo) {
-      double E = R.bond(lo, hi, p, sink);
+      Wd E = dbl(R.bond(lo, hi, p, sink));
       if (a == lo) er += E;
     }
     if (do_tors) {
-      double E = etors_bond(R, TP, lo, hi, p, sink);
+      Wd E = dbl(etors_bond(R, TP, lo, hi, p, sink));
       if (a == lo) et += E;
     }
   }
-  O.gown[a] = make_double4(sink.g.x, sink.g.y, sink.g.z, 0.0);
+  O.gown[a] = make_q4(sink.g.x, sink.g.y, sink.g.z, Wd(0.0));
   O.e_rebo[a] = er;
   O.e_tors[a] = et;
 }
@@ -328,7 +344,7 @@ template <class Real, class TB>
 MDG_HD void rebo_task(const ReboT<Real, TB>& R, const TorsParams& TP, int do_rebo, int do_tors, double* rec, int a,
                       int s)
 {
-  const BondList& B = R.B;
+  const auto& B = R.B;
   const int nb = B.nb[a];
   SinkT<Real> sink;
   sink.a = a;
@@ -363,7 +379,7 @@ template <class Real, class TB>
 MDG_HD void rebo_pair_task(const ReboT<Real, TB>& R, const TorsParams& TP, int do_rebo, int do_tors, double* rlo,
                            double* rhi, int lo, int s, int hi)
 {
-  const BondList& B = R.B;
+  const auto& B = R.B;
   const int na = B.nb[lo], nb = B.nb[hi];
   PairSinkT<Real> sink;
   sink.a = lo;
@@ -395,17 +411,19 @@ MDG_HD void rebo_pair_task(const ReboT<Real, TB>& R, const TorsParams& TP, int d
 // Total dE/dx_a: own parts, what bond partners owe a, and the third-shell
 // switching derivatives (dfThem through N_conj) resolved by gathering the
 // coefficients of the bonds around a and around each switching partner.
-MDG_HD V3 gather_atom(const BondList& B, const ForceOut& O, int a, int with_lj, const double4* gextra)
+template <class Ws>
+MDG_HD V3T<Ws> gather_atom(const BondListT<Ws>& B, const ForceOutT<Ws>& O, int a, int with_lj,
+                           const typename Q4T<Ws>::T* gextra)
 {
-  double4 g0 = O.gown[a];
-  V3 g = v3(g0.x, g0.y, g0.z);
+  const auto g0 = O.gown[a];
+  V3T<Ws> g = v3r<Ws>(g0.x, g0.y, g0.z);
   if (with_lj) {
-    double4 g1 = O.glj[a];
-    g += v3(g1.x, g1.y, g1.z);
+    const auto g1 = O.glj[a];
+    g += v3r<Ws>(g1.x, g1.y, g1.z);
   }
   if (gextra) {
-    double4 g2 = gextra[a];
-    g += v3(g2.x, g2.y, g2.z);
+    const auto g2 = gextra[a];
+    g += v3r<Ws>(g2.x, g2.y, g2.z);
   }
   const int nb = B.nb[a];
   for (int s = 0; s < nb; s++) {
@@ -413,22 +431,22 @@ MDG_HD V3 gather_atom(const BondList& B, const ForceOut& O, int a, int with_lj, 
     const int k = B.bj[q];
     const int r = B.brev[q];
     if (r < 0) continue;  // partner list truncated by an overflow (already flagged)
-    const double* Ak = O.A + ((long)k * O.mb + r) * 3;
-    g += v3(Ak[0], Ak[1], Ak[2]);
+    const Ws* Ak = O.A + ((long)k * O.mb + r) * 3;
+    g += v3r<Ws>(Ak[0], Ak[1], Ak[2]);
   }
   for (int s = 0; s < nb; s++) {
     const int q = a * B.mb + s;
-    const double df = B.bd[q].x;
+    const Ws df = B.bd[q].x;
     if (df == 0.0) continue;
     const int m = B.bj[q];
-    double wa = 0.0;
+    Ws wa = 0.0;
     for (int t = 0; t < nb; t++) {
       if (t == s) continue;
       const int qt = a * B.mb + t;
       if (B.brev[qt] < 0) continue;
       wa += O.W[(long)B.bj[qt] * O.mb + B.brev[qt]];
     }
-    double wm = 0.0;
+    Ws wm = 0.0;
     const int nbm = B.nb[m];
     for (int t = 0; t < nbm; t++) {
       const int qt = m * B.mb + t;
@@ -436,8 +454,8 @@ MDG_HD V3 gather_atom(const BondList& B, const ForceOut& O, int a, int with_lj, 
       if (c == a || B.brev[qt] < 0) continue;
       wm += O.W[(long)c * O.mb + B.brev[qt]];
     }
-    double4 u = B.bu[q];
-    g += v3(u.x, u.y, u.z) * (df * (wa + wm));
+    const auto u = B.bu[q];
+    g += v3r<Ws>(u.x, u.y, u.z) * (df * (wa + wm));
   }
   return g;
 }

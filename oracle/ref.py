@@ -49,6 +49,7 @@ def lib():
         L.ref_energy_proxy.argtypes = [vp, dp, dp]
         L.ref_nl_pairs.restype = ctypes.c_long
         L.ref_nl_pairs.argtypes = [vp, ctypes.c_int, ip, ctypes.c_long]
+        L.ref_set_param.argtypes = [vp, ctypes.c_int, ctypes.c_double]
         L.ref_rcutoff.restype = ctypes.c_double
         L.ref_rcutoff.argtypes = [vp, ctypes.c_int]
         L.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, ip, dp, dp, dp]
@@ -130,6 +131,10 @@ class RefSystem:
         out = np.zeros((max(cnt, 1), 2), dtype=np.int32)
         _check(lib().ref_nl_pairs(self.h, index, _ip(out), cnt))
         return out[:cnt]
+
+    def set_param(self, pid: int, value: float):
+        """Override a C-C pair parameter (ids as include/mdg.h MDG_PARAM_*)."""
+        _check(lib().ref_set_param(self.h, pid, ctypes.c_double(value)))
 
     def rcutoff(self, index: int) -> float:
         return float(lib().ref_rcutoff(self.h, index))

@@ -73,13 +73,14 @@ struct RefCtx
   FixedDtLoop loop;
   int potset;
   int brenner_set;
+  int lj_cut_mode;
   std::vector<std::string> names;
   REBO* rebo;
   AIREBO* lj;
   ETors* etors;
   Brenner* brenner;
   bool nl_ready;
-  RefCtx() : potset(0), brenner_set(1), rebo(0), lj(0), etors(0), brenner(0), nl_ready(false) {}
+  RefCtx() : potset(0), brenner_set(1), lj_cut_mode(0), rebo(0), lj(0), etors(0), brenner(0), nl_ready(false) {}
 };
 
 ElementID el_from_z(int z)
@@ -123,6 +124,7 @@ void* ref_create(int potset, int brenner_set, int lj_cut_mode)
     RefCtx* c = new RefCtx();
     c->potset = potset;
     c->brenner_set = brenner_set;
+    c->lj_cut_mode = lj_cut_mode;
     c->loop.preventFileOutput = true;
     if (potset & POT_REBO) {
       c->rebo = new REBO();
@@ -284,6 +286,52 @@ long ref_nl_pairs(void* h, int index, int* pairs, long cap)
     g_last_error = e.what();
     return -1;
   }
+}
+
+/* Override one C-C pair parameter (Angstrom / eV) of the potentials in place,
+ * re-deriving what AIREBO::setupPotential derives from it
+ * (AIREBO_LJ.cxx:229-262): id 0 = AIREBO zeta_[C][C], 1 = AIREBO
+ * sigma_[C][C], 2 = REBO A_[C][C], 3 = REBO B_[0][C][C], 4 = REBO
+ * alpha_[C][C], 5 = REBO beta_[0][C][C].  Test support for finite
+ * differences of the reference with respect to its parameters. */
+int ref_set_param(void* h, int id, double value)
+{
+  RefCtx* c = (RefCtx*)h;
+  const int C = 0, H = 1;  // REBO::C, REBO::H (REBO.hpp:157-158)
+  if (id <= 1 && !c->lj) { g_last_error = "no AIREBO LJ term"; return -1; }
+  if (id >= 2 && !c->rebo) { g_last_error = "no REBO term"; return -1; }
+  switch (id) {
+    case 0:
+    case 1: {
+      AIREBO* a = c->lj;
+      if (id == 0) a->zeta_[C][C] = value * eV;
+      else a->sigma_[C][C] = value * Ao;
+      a->sigma_[C][H] = 0.5 * (a->sigma_[C][C] + a->sigma_[H][H]);
+      a->sigma_[H][C] = a->sigma_[C][H];
+      a->zeta_[C][H] = sqrt(a->zeta_[C][C] * a->zeta_[H][H]);
+      a->zeta_[H][C] = a->zeta_[C][H];
+      for (int x = 0; x < 2; x++)
+        for (int y = 0; y < 2; y++) {
+          a->RLJ_[x][y][0] = a->sigma_[x][y];
+          a->RLJ_[x][y][1] = a->sigma_[x][y] * pow(2.0, 1.0 / 6.0);
+          if (c->lj_cut_mode == 1) {
+            a->R_[x][y][0] = 3.0 * a->sigma_[x][y] - 0.5 * Ao;
+            a->R_[x][y][1] = 3.0 * a->sigma_[x][y];
+          }
+        }
+      if (c->lj_cut_mode == 1) {
+        a->nl.Rcutoff = a->getRcutoff();
+        c->nl_ready = false;
+      }
+      break;
+    }
+    case 2: c->rebo->A_[C][C] = value * eV; break;
+    case 3: c->rebo->B_[0][C][C] = value * eV; break;
+    case 4: c->rebo->alpha_[C][C] = value / Ao; break;
+    case 5: c->rebo->beta_[0][C][C] = value / Ao; break;
+    default: g_last_error = "unknown parameter id"; return -1;
+  }
+  return 0;
 }
 
 double ref_rcutoff(void* h, int index)

@@ -135,3 +135,26 @@ def test_reference_torsion_force_is_not_the_energy_gradient():
     d = np.random.default_rng(8).normal(size=s["pos"].shape)
     dd = ref.rs_energy_dir(s, bits, d).sum()
     assert abs(dd - np.sum(go * d)) > 1e-6 * np.linalg.norm(go) * np.linalg.norm(d)
+
+
+def test_parameter_override_acts_on_the_reference():
+    """ref_set_param changes the reference's own members: REBO's V_R is
+    linear in A_CC and the LJ energy of pure carbon is linear in eps_CC, so
+    equal steps of the parameter give equal energy steps; sigma_CC moves the
+    LJ energy; restoring a parameter restores the energy bitwise."""
+    s = B.amorphous_carbon(300, seed=91)
+    r = ref.RefSystem(ref.POT_AIREBO)
+    r.set_atoms(s["z"], s["pos"], s["vel"], s["box"], s["pbc"])
+    e0, et0, _ = r.compute()
+    for pid, base, term in ((2, 10953.544, 0), (0, 0.00284, 1)):
+        es = []
+        for k in range(3):
+            r.set_param(pid, base * (1 + 0.01 * k))
+            es.append(r.compute()[1][term])
+        d1, d2 = es[1] - es[0], es[2] - es[1]
+        assert d1 != 0.0 and abs(d1 - d2) <= 1e-9 * abs(d1), (pid, d1, d2)
+        r.set_param(pid, base)
+    e1, et1, _ = r.compute()
+    assert e1 == e0
+    r.set_param(1, 3.41)
+    assert r.compute()[1][1] != et0[1]
