@@ -141,6 +141,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="instead of the throughput line: the FP32-mixed vs FP64 study on the 512,000-atom diamond")
+    ap.add_argument("--study-steps", type=int, default=5000)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -180,6 +183,9 @@ def main():
     def barrier():
         if dist is not None:
             dist.barrier()
+
+    if args.precision_study:
+        return precision_study(args, local, rank)
 
     s = build_system(seed=1 + rank)
     n = len(s["z"])
@@ -354,6 +360,102 @@ def main():
                    "workload": "cluster impacts: AB graphite slabs 800-6000 atoms (lateral PBC, open z, fixed "
                                "bottom layer) + 13-atom C cluster at 10-100 eV, AIREBO"}
         del bx
+        # the same batch in FP64 (batching without the precision change), and
+        # the plain FP64 path on the same systems one at a time (a sample of
+        # them, scaled by atoms): what running the impacts sequentially costs
+        b64 = M.Context(potentials=M.POT_AIREBO, precision=M.PREC_FP64, device=local)
+        b64.set_batch(systems)
+        b64.set_stream(stream.cuda_stream)
+        b64.run(max(args.warmup, 3), BATCH_DT_FS, energies=False)
+        b64.sync()
+        kb64 = min(args.steps, 20)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b64_ms = 0.0
+        for k in range(kb64):
+            flush.zero_()
+            e0.record(stream)
+            b64.run(1, BATCH_DT_FS, energies=False)
+            e1.record(stream)
+            e1.synchronize()
+            b64_ms += e0.elapsed_time(e1)
+        batched["fp64_batched"] = {"value": world * nb_atoms * kb64 / (b64_ms * 1e-3), "unit": "atom-steps/s",
+                                   "steps": kb64, "ms_per_step": b64_ms / kb64}
+        del b64
+        seq_atoms, seq_ms, nseq, kseq = 0, 0.0, 16, 20
+        for sysd in systems[:nseq]:
+            cx = M.Context(potentials=M.POT_AIREBO, precision=M.PREC_FP64, device=local)
+            cx.set_system(sysd["z"], sysd["pos"], sysd["vel"], sysd["box"], sysd["pbc"], sysd["fixed"])
+            cx.set_stream(stream.cuda_stream)
+            cx.run(max(args.warmup, 3), BATCH_DT_FS, energies=False)
+            cx.sync()
+            flush.zero_()
+            e0.record(stream)
+            cx.run(kseq, BATCH_DT_FS, energies=False)
+            e1.record(stream)
+            e1.synchronize()
+            seq_ms += e0.elapsed_time(e1)
+            seq_atoms += len(sysd["z"]) * kseq
+            del cx
+        batched["fp64_sequential"] = {
+            "value": world * seq_atoms / (seq_ms * 1e-3), "unit": "atom-steps/s",
+            "sample": f"first {nseq} of the {BATCH_SYSTEMS} systems, one context each, {kseq} steps each "
+                      f"(graph-replayed), run one after another"}
+
+    # Adjoint variant: gradients of a 200-step trajectory loss with respect to
+    # the six C-C pair parameters, x0 and v0 (4,096-atom amorphous carbon at
+    # 2.0 g/cm^3, pre-relaxed 500 steps at 3,000 K, dt 0.5 fs, checkpoint every
+    # 20 steps, loss = mean |x_200 - x_target|^2 + 1e-5 E_total), FP64
+    adjoint = None
+    if not args.no_variants:
+        from mdtk_b200 import builders as B
+        a0 = B.amorphous_carbon(ADJ_ATOMS, density_g_cm3=2.0, min_sep=1.2, seed=81 + rank)
+        a5 = B.relax_hot(a0, 500, 3000.0, ADJ_DT_FS, M.POT_AIREBO, seed=82 + rank, device=local)
+        ax = M.Context(potentials=M.POT_AIREBO, device=local, task_mode=1)
+        ax.set_system(a5["z"], a5["pos"], a5["vel"], a5["box"], a5["pbc"], a5["fixed"])
+        ax.set_stream(stream.cuda_stream)
+        m = B.masses(a5["z"])[:, None]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def grad_once():
+            ax.set_state(a5["pos"], a5["vel"])
+            e0.record(stream)
+            t0 = time.perf_counter()
+            xN, vN, _ = ax.adjoint_forward(ADJ_STEPS, ADJ_DT_FS, ADJ_EVERY)
+            e1.record(stream)
+            t1 = time.perf_counter()
+            e1.synchronize()
+            fwd_ms = e0.elapsed_time(e1)
+            target = xN + 0.01 * np.random.default_rng(83).normal(size=xN.shape)
+            sx = 2.0 * (xN - target) / ADJ_ATOMS
+            sv = 1e-5 * m * vN / B.EV_PER_AMU_A2FS2
+            e0.record(stream)
+            t2 = time.perf_counter()
+            gp, _, _ = ax.adjoint_backward(sx, sv, 1e-5)
+            e1.record(stream)
+            t3 = time.perf_counter()
+            e1.synchronize()
+            return fwd_ms, e0.elapsed_time(e1), (t1 - t0) * 1e3, (t3 - t2) * 1e3, gp
+
+        grad_once()  # buffers, lists, warm-up
+        fwd_ms, bwd_ms, fwd_wall, bwd_wall, gp = grad_once()
+        ax.set_state(a5["pos"], a5["vel"])
+        ax.run(3, ADJ_DT_FS, energies=False)
+        ax.sync()
+        e0.record(stream)
+        ax.run(ADJ_STEPS, ADJ_DT_FS, energies=False)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms = e0.elapsed_time(e1)
+        adjoint = {
+            "value": world * ADJ_ATOMS * ADJ_STEPS / ((fwd_ms + bwd_ms) * 1e-3), "unit": "atom-steps/s (gradient)",
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "forward_wall_ms": fwd_wall, "backward_wall_ms": bwd_wall,
+            "plain_fp64_run_ms": plain_ms, "gradient_over_plain": (fwd_ms + bwd_ms) / plain_ms,
+            "grad_params": dict(zip(M.PARAM_NAMES, [float(x) for x in gp])),
+            "workload": f"{ADJ_ATOMS} C amorphous 2.0 g/cm^3, pre-relaxed 500 steps at 3000 K, {ADJ_STEPS} steps "
+                        f"dt {ADJ_DT_FS} fs, checkpoint every {ADJ_EVERY}, AIREBO FP64; gradients w.r.t. eps, "
+                        f"sigma, A, B1, alpha, beta1 (C-C), x0, v0",
+            "timer": "CUDA events on the library stream around each (host-driven) call"}
+        del ax
 
     if rank == 0:
         line = {
@@ -365,7 +467,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches, "clocks": clk, "kernels": kern, "roofline": roof, "e2e": e2e,
             "fp64_peak_tflops": fp64_peak,
-            "variants": {"fp32_mixed": mixed, "batched": batched},
+            "variants": {"fp32_mixed": mixed, "batched": batched, "adjoint": adjoint},
         }
         if world == 1 and not args.no_cpu_baseline:
             try:
@@ -381,6 +483,67 @@ def main():
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+ADJ_ATOMS, ADJ_STEPS, ADJ_DT_FS, ADJ_EVERY = 4096, 200, 0.5, 20
+
+# 512,000-atom diamond of the precision study (40^3 cells, a = 3.567 A,
+# Gaussian displacements sigma 0.05 A, 600 K, dt 0.5 fs)
+STUDY_CELLS, STUDY_DT_FS = 40, 0.5
+
+
+def precision_study(args, local, rank):
+    """FP32-mixed against FP64 on the 512,000-atom diamond: force and energy
+    error at the start, device time per step of each, and the NVE drift and
+    fluctuation of each over --study-steps steps.  Prints one JSON line."""
+    import torch
+    import mdtk_b200 as M
+    from mdtk_b200 import builders as B
+    torch.cuda.set_device(local)
+    s = B.diamond(STUDY_CELLS, temp_k=600.0, disp_sigma=0.05, seed=7 + rank)
+    n = len(s["z"])
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    out = {"study": "precision", "atoms": n, "steps": args.study_steps, "dt_fs": STUDY_DT_FS,
+           "workload": f"diamond {STUDY_CELLS}^3 cells ({n} C), Gaussian displacements 0.05 A, 600 K, AIREBO"}
+    ctxs, grads, energies = {}, {}, {}
+    for name, prec in (("fp64", M.PREC_FP64), ("fp32_mixed", M.PREC_FP32_MIXED)):
+        c = M.Context(potentials=M.POT_AIREBO, precision=prec, device=local)
+        c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+        c.set_stream(stream.cuda_stream)
+        e, et, g = c.compute()
+        ctxs[name], grads[name], energies[name] = c, g, (e, et)
+    d = grads["fp32_mixed"] - grads["fp64"]
+    out["force_err"] = {"norm_rel": float(np.linalg.norm(d) / np.linalg.norm(grads["fp64"])),
+                        "max_abs_over_rms": float(np.abs(d).max() / np.sqrt((grads["fp64"] ** 2).mean()))}
+    out["energy_err_rel"] = abs(energies["fp32_mixed"][0] - energies["fp64"][0]) / abs(energies["fp64"][0])
+    out["energy_terms"] = {k: [float(x) for x in v[1][:3]] for k, v in energies.items()}
+    for name, c in ctxs.items():
+        c.run(3, STUDY_DT_FS, energies=False)
+        c.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c.run(50, STUDY_DT_FS, energies=False)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 50
+        c.set_state(s["pos"], s["vel"])
+        t0 = time.perf_counter()
+        _, etot = c.run(args.study_steps, STUDY_DT_FS)
+        wall = time.perf_counter() - t0
+        k0 = max(1, len(etot) // 100)
+        e = np.asarray(etot[k0:]) / n
+        t = (np.arange(k0, len(etot)) + 1) * STUDY_DT_FS * 1e-3
+        a, b = np.polyfit(t, e, 1)
+        out[name] = {"ms_per_step": ms, "atom_steps_per_s": n / (ms * 1e-3),
+                     "nve_drift_ev_per_atom_per_ps": float(a),
+                     "nve_rms_fluct_ev_per_atom": float(np.sqrt(np.mean((e - (a * t + b)) ** 2))),
+                     "e_total_first_last_ev_per_atom": [float(etot[0] / n), float(etot[-1] / n)],
+                     "run_wall_s": wall}
+    out["speedup_mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_mixed"]["ms_per_step"]
+    if rank == 0:
+        print(json.dumps(out))
     return 0
 
 
