@@ -557,7 +557,7 @@ FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_plain": 5151.5, "lj_special":
 STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
 # dram read+write bytes per launch from an ncu capture of the same workload
 # (profiles/hot_kernels_airebo_ethane43688_fp64.md), or None.
-TRAFFIC_PER_LAUNCH = {"rebo_tors": 22.87e6, "lj_plain": 47.32e6, "lj_special": 24.57e6, "bond_reduce": 35.04e6}
+TRAFFIC_PER_LAUNCH = {"rebo_tors": 22.91e6, "lj_plain": 47.45e6, "lj_special": 24.79e6, "bond_reduce": 35.04e6}
 
 
 if __name__ == "__main__":

@@ -375,6 +375,7 @@ int adj_dual_pass(mdg_ctx* c, int transpose = 1)
     DT.cnt = c->cij.cnt;
     DT.ent = c->cij.ent;
     DT.w = w->cw;
+    DT.mask = c->cij.mask;
     LAUNCH(c, "adj_cij", k_adj_cij, nblk(n), kThreads, DB, c->cij, w->cw);
     LAUNCH(c, "adj_lj_plain", k_adj_lj_plain, nblk(n), kThreads, c->ljp, DT, S, c->nl[1], w->tan, O);
     const SpecialTasks& P = c->spc;

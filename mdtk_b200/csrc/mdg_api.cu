@@ -966,7 +966,7 @@ void free_system(mdg_ctx* c)
     std::memset(&c->grid[l], 0, sizeof(Grid));
     c->has_list[l] = false;
   }
-  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
+  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
                 c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work, c->spc.wrev,
                 c->spc.wcnt, c->scan_tiles};
   c->scan_tiles = nullptr;
@@ -1554,6 +1554,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     c->cij.cnt = dalloc<int>(n);
     c->cij.ent = dalloc<int4>((size_t)n * c->cij.cap);
     c->cij.w = dalloc<double>((size_t)n * c->cij.cap);
+    c->cij.mask = dalloc<unsigned long long>(n);
     SpecialTasks& X = c->spc;
     X.cap = c->prm.cap_special;
     X.task_cap = (int)std::min<long>((long)n * c->prm.special_avg, 1L << 30);
@@ -1573,7 +1574,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     X.wcnt = dalloc<unsigned long long>(1);
     if (!X.work || !X.wrev || !X.wcnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ work list)");
     CK(cudaMemset(X.wcnt, 0, sizeof(unsigned long long)));
-    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
+    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->cij.mask || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
         !X.trec || !X.rec || !X.mid || !X.midc)
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
     CK(cudaMemset(X.cnt, 0, n * sizeof(int)));

@@ -61,15 +61,19 @@ MDG_HD Real etors_bond(const ReboT<Real, TB>& R, const TorsParams& TP, int i, in
       if (cosd < -1.0) cosd = -1.0;
       if (cosd > 1.0) cosd = 1.0;
       Real cdh = -cosd;
-      Real val = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0) - 0.1 * eps;
+      // ((1 + cdh)/2)^5 and ^4 by multiplication (the reference's pow, equal to rounding)
+      const Real hx = 0.5 * (1.0 + cdh);
+      const Real hx2 = hx * hx, hx4 = hx2 * hx2;
+      Real val = (256.0 / 405.0) * eps * (hx4 * hx) - 0.1 * eps;
       Real V = wki * wij * wjl;  // seed of Vtors (AIREBO_ETors.cxx:78)
       if (val != 0.0) {
-        Real der = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0 - 1.0) * 0.5;
+        Real der = (256.0 / 405.0) * eps * hx4 * 0.5;
         Real Vd = -1.0 * der * V;
         if (Vd != 0.0 && e2 != 0.0) {
-          Real cr = e1 / e2;
-          V3T<Real> U = w / e2 - u * (cr / uu);
-          V3T<Real> Wv = u / e2 - w * (cr / ww);
+          const Real ie2 = Real(1.0) / e2;
+          Real cr = e1 * ie2;
+          V3T<Real> U = w * ie2 - u * (cr / uu);
+          V3T<Real> Wv = u * ie2 - w * (cr / ww);
           sink.pair(i, j, (cross(U, b) + cross(c, Wv)) * Vd);
           sink.cbond(i, si, cross(a, U) * Vd);
           sink.cbond(j, sj, cross(Wv, a) * Vd);
@@ -92,7 +96,7 @@ MDG_HD Real etors_bond(const ReboT<Real, TB>& R, const TorsParams& TP, int i, in
       if constexpr (S::kAdj) {
         // -4 der grad(W) (grad(cdh).u): tangent only
         if (sink.jt && e2 != 0.0) {
-          const Real der = (256.0 / 405.0) * eps * pow(0.5 * (1.0 + cdh), 5.0 - 1.0) * 0.5;
+          const Real der = (256.0 / 405.0) * eps * hx4 * 0.5;
           const Real kw = Real(0.0, -4.0 * mdg::val(der) * cdh.d);
           if (dfk != 0.0) sink.cbond(i, si, values_of(xyz<Real>(uk) * (wij * wjl * dfk)) * kw);
           if (p.df != 0.0) sink.pair(i, j, values_of(p.u * (wki * wjl * p.df)) * kw);

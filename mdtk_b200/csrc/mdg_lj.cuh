@@ -94,6 +94,7 @@ struct CijTableT {
   int* cnt;        // [n]
   int4* ent;       // [n * cap] x = target, y = path length, z = k, w = m
   W* w;            // [n * cap]
+  unsigned long long* mask;  // [n] bit (target & 63) of every target: a clear bit means "no entry"
 };
 typedef CijTableT<double> CijTable;
 
@@ -182,11 +183,14 @@ MDG_HD void cij_build_atom(const BondList& B, CijTable& T, int i, unsigned int* 
     }
     tgt[b + 1] = t; len[b + 1] = l; pk[b + 1] = k; pm[b + 1] = m; w[b + 1] = ww;
   }
+  unsigned long long mask = 0ull;
   for (int e = 0; e < n; e++) {
     T.ent[(long)i * T.cap + e] = make_int4(tgt[e], len[e], pk[e], pm[e]);
     T.w[(long)i * T.cap + e] = w[e];
+    mask |= 1ull << (tgt[e] & 63);
   }
   T.cnt[i] = n;
+  T.mask[i] = mask;
 }
 
 // Lookup of target j in the table of i (binary search).  Returns the entry
@@ -194,6 +198,9 @@ MDG_HD void cij_build_atom(const BondList& B, CijTable& T, int i, unsigned int* 
 template <class W>
 MDG_HD int cij_find(const CijTableT<W>& T, int i, int j)
 {
+  // most LJ partners are beyond three bonds: one mask load rules them out
+  // without the dependent loads of the search
+  if (!((T.mask[i] >> (j & 63)) & 1ull)) return -1;
   int lo = 0, hi = T.cnt[i] - 1;
   const int4* e = T.ent + (long)i * T.cap;
   while (lo <= hi) {
@@ -238,15 +245,16 @@ MDG_HD void vlj(const LJParams& P, int ti, int tj, int i, int j, const PairGT<Re
   val = 0.0;
   if (fv == 0.0) return;
   const Wd r = pl.rd;
+  const Wd ir = Wd(1.0) / r;
   const double sigma = P.sigma[ti][tj], zeta = P.eps[ti][tj];
-  const Wd sdr = sigma / r;
+  const Wd sdr = sigma * ir;
   Wd s6 = sdr;
   for (int q = 2; q <= 6; q++) s6 *= sdr;
   const Wd s12 = s6 * s6;
   const Wd vd = 4.0 * zeta * (s12 - s6);
   val = vd;
   if (V != 0.0) {
-    const Wd der = 4.0 * zeta * (-12.0 * s12 / r + 6.0 * s6 / r);
+    const Wd der = 4.0 * zeta * (-12.0 * s12 + 6.0 * s6) * ir;
     sink.pair(i, j, pl.u * Real(der * dbl(fv) * dbl(V)));
     if (pl.df != 0.0) sink.pair(i, j, pl.u * Real((vd * dbl(V)) * dbl(pl.df)));
   }
@@ -454,7 +462,7 @@ MDG_HD PairGT<Real> pair_geom(V3 rv, double r, const double4* tan, int lo, int h
     p.rv = cvt3<Real>(rv);
     p.r = r;
     p.rd = r;
-    p.u = cvt3<Real>(rv / r);
+    p.u = cvt3<Real>(rv * (1.0 / r));
   }
   p.alter = 0;
   p.ralt = 0.0;
@@ -616,7 +624,7 @@ MDG_HD void lj_special_pair_task(const LJT<Real, TB>& X, const State& St, Specia
   p.rv = cvt3<Real>(rv);
   p.r = r;
   p.rd = r;
-  p.u = cvt3<Real>(rv / r);
+  p.u = cvt3<Real>(rv * (1.0 / r));
   cutoff(p.r, X.P.R[ta][tb][0], X.P.R[ta][tb][1], p.f, p.df);
   p.alter = 0;
   p.ralt = 0.0;

@@ -229,9 +229,9 @@ struct ReboT {
     }
     if (Vc != 0.0) {
       // d cos(theta_ock) / d(x_c - x_o) and d/d(x_c - x_k) (FGeneral.hpp:152-178)
-      Real e2s = SQR(e2);
-      V3T<Real> dpa = (bk_rv * e2 - p.u * (bk_r * e1)) / e2s;
-      V3T<Real> dpb = (p.rv * e2 - bk_u * (p.r * e1)) / e2s;
+      const Real ie2s = Real(1.0) / SQR(e2);
+      V3T<Real> dpa = (bk_rv * e2 - p.u * (bk_r * e1)) * ie2s;
+      V3T<Real> dpb = (p.rv * e2 - bk_u * (p.r * e1)) * ie2s;
       sink.pair(c, o, dpa * Vc);
       sink.cbond(c, s_k, dpb * Vc);
     }
@@ -320,16 +320,19 @@ struct ReboT {
     return v;
   }
 
-  // p^{sigma pi}_co = D^-1/2 (REBO::p_sigma_pi, REBO.cxx:267-278).
+  // p^{sigma pi}_co = D^-1/2 (REBO::p_sigma_pi, REBO.cxx:267-278); the
+  // reference's pow(D, -1/2) and pow(D, -3/2) as 1/sqrt(D) and its cube
+  // (equal to rounding, a fraction of pow's instructions).
   template <class S>
   MDG_HD Real p_sigma_pi(int c, int o, const PairGT<Real>& p, Real V, S& sink) const
   {
     Real DVal = D_value(c, o, p);
+    const Real ir = Real(1.0) / sqrt(DVal);
     if (V != 0.0) {
-      Real Der = -0.5 * pow(DVal, -0.5 - 1.0);
+      Real Der = -0.5 * (ir * ir * ir);
       D_grad(c, o, p, Der * V, sink);
     }
-    return pow(DVal, -0.5);
+    return ir;
   }
 
   // N_conj halves (REBO::NconjSum1/2, REBO.cxx:540-606): sum over C
@@ -437,9 +440,10 @@ struct ReboT {
         if (V != 0.0) {
           Real Vd = 2.0 * cdh * fik * fjl * V;
           if (Vd != 0.0 && e2 != 0.0) {
-            Real cr = e1 / e2;
-            V3T<Real> U = w / e2 - u * (cr / uu);
-            V3T<Real> Wv = u / e2 - w * (cr / ww);
+            const Real ie2 = Real(1.0) / e2;
+            Real cr = e1 * ie2;
+            V3T<Real> U = w * ie2 - u * (cr / uu);
+            V3T<Real> Wv = u * ie2 - w * (cr / ww);
             V3T<Real> da = cross(U, b) + cross(cc, Wv);
             V3T<Real> db = cross(a, U);
             V3T<Real> dc = cross(Wv, a);
