@@ -246,6 +246,12 @@ int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const d
  * ran, its timings of one force evaluation in each mode (ms; 0 otherwise). */
 int mdg_task_mode(mdg_ctx* ctx, int* mode, float* ms_directed, float* ms_per_bond);
 
+/* The launch configuration the autotuner chose (task_mode 0): overlap = 1
+ * when the REBO tasks run on a second stream concurrently with the LJ
+ * kernels, rebo_blocks = the REBO task kernel's grid.  No reference
+ * counterpart. */
+int mdg_tuned_launch(mdg_ctx* ctx, int* overlap, int* rebo_blocks);
+
 /* ---- Batched systems ----
  * Many independent systems of uneven size in one context (the reference runs
  * impacts one after another, mdtrajsim/main.cpp:295-345): atoms of system s

@@ -99,6 +99,7 @@ def lib():
         L.mdg_task_mode.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
                                     ctypes.POINTER(ctypes.c_float)]
         L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
+        L.mdg_tuned_launch.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.mdg_sync.argtypes = [vp]
         L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
         L.mdg_launch_count.argtypes = [vp]
@@ -240,6 +241,13 @@ class Context:
         b = ctypes.c_float()
         _check(lib().mdg_task_mode(self.h, ctypes.byref(m), ctypes.byref(a), ctypes.byref(b)))
         return m.value, a.value, b.value
+
+    def tuned_launch(self):
+        """(overlap, rebo_blocks): the autotuner's launch choice."""
+        o = ctypes.c_int()
+        b = ctypes.c_int()
+        _check(lib().mdg_tuned_launch(self.h, ctypes.byref(o), ctypes.byref(b)))
+        return o.value, b.value
 
     def batch_energies(self) -> np.ndarray:
         """[nsys, 4]: REBO, LJ, torsion, kinetic energy of each system."""

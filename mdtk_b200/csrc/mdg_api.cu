@@ -807,7 +807,14 @@ struct mdg_ctx {
   CijTable cij;
   SpecialTasks spc;
   BondTasks bt;
-  int rebo_task_blocks = 0;
+  int rebo_task_blocks = 0;   // resident capacity of the REBO task kernel (blocks)
+  int rebo_grid = 0;          // blocks it is launched with (the autotuner's choice; 0 = capacity)
+  // REBO tasks on a second stream, concurrent with the LJ chain (which does
+  // not read their records until the reduction): fork/join by events, also
+  // inside a captured step
+  bool overlap = false;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool tuned = false;        // the autotuner ran for this system
   float tune_ms[2] = {0, 0};  // its timings of one force evaluation per task mode
 
@@ -986,6 +993,8 @@ void free_system(mdg_ctx* c)
   for (int l = 0; l < 2; l++) { c->d_snc[l] = nullptr; c->d_slo[l] = nullptr; c->d_scs[l] = nullptr; }
   c->nsys = 1;
   c->tuned = false;
+  c->overlap = false;
+  c->rebo_grid = 0;
   c->h_first.clear();
   c->h_boxes.clear();
   c->h_sys.clear();
@@ -1117,6 +1126,14 @@ void prof_end(mdg_ctx* c);
     prof_end(c);                                                      \
     (c)->launches++;                                                  \
   } while (0)
+// The same on another stream (never while profiling: the events are on c->stream).
+#define LAUNCH_ON(c, STREAM, NAME, KERNEL, GRID, BLOCK, ...)          \
+  do {                                                                \
+    prof_begin(c, NAME);                                              \
+    KERNEL<<<(GRID), (BLOCK), 0, (STREAM)>>>(__VA_ARGS__);            \
+    prof_end(c);                                                      \
+    (c)->launches++;                                                  \
+  } while (0)
 
 int rebuild_lists(mdg_ctx* c)
 {
@@ -1156,26 +1173,35 @@ int evaluate(mdg_ctx* c)
   LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
   const bool f32p = c->prm.precision == MDG_PREC_FP32_MIXED;
+  const bool ovl = tasks && lj && c->overlap && !c->prof && c->side;
+  cudaStream_t rs = c->stream;
+  if (ovl) {
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    rs = c->side;
+  }
   if (tasks) {
     const int ir = rebo ? 1 : 0, it = tors ? 1 : 0;
+    const int grid = c->rebo_grid > 0 ? c->rebo_grid : c->rebo_task_blocks;
     if (f32p && c->bt.pairs) {
       auto kern = k_rebo_pair_task<f32, ReboTables32>;
-      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
-             c->d_status);
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
+                c->d_status);
     } else if (f32p) {
       auto kern = k_rebo_task<f32, ReboTables32>;
-      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
-             c->d_status);
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
+                c->d_status);
     } else if (c->bt.pairs) {
       auto kern = k_rebo_pair_task<double, ReboTables>;
-      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
-             c->d_status);
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
+                c->d_status);
     } else {
       auto kern = k_rebo_task<double, ReboTables>;
-      LAUNCH(c, "rebo_tors", kern, c->rebo_task_blocks, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
-             c->d_status);
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
+                c->d_status);
     }
   }
+  if (ovl) CK(cudaEventRecord(c->ev_join, c->side));
   else
     LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
            tors ? 1 : 0, c->fo, c->d_status);
@@ -1216,6 +1242,7 @@ int evaluate(mdg_ctx* c)
              c->spc, c->d_status);
     }
   }
+  if (ovl) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   if (tasks || lj)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
@@ -1342,6 +1369,12 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
     cudaMemcpy(c->d_bp, &bp, sizeof(BrennerParams), cudaMemcpyHostToDevice);
     delete bt;
   }
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    mdg_destroy(c);
+    return fail(MDG_ERR_CUDA, "cudaStreamCreate / cudaEventCreate");
+  }
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     mdg_destroy(c);
     return fail(MDG_ERR_CUDA, "cudaStreamCreate");
@@ -1369,6 +1402,9 @@ int mdg_destroy(mdg_ctx* c)
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return MDG_OK;
@@ -1708,38 +1744,70 @@ int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* 
   return MDG_OK;
 }
 
-// The autotuner: with task_mode 0, times one force evaluation in each REBO
-// task mode (after one untimed evaluation each; best of three) on the first
-// run of a system and keeps the faster.  Both modes compute the same terms
-// (equal to rounding), so the choice changes only the speed.
+// The autotuner: with task_mode 0, on the first run of a system, times one
+// force evaluation (after one untimed evaluation; best of three) in each
+// configuration of the REBO work and keeps the fastest:
+//   - the split: one task per directed bond, or one per bond (both route the
+//     same terms into the same records, equal to rounding);
+//   - with the LJ term, where the REBO tasks run: in order before the LJ
+//     chain with the grid at the kernel's resident capacity, or on the second
+//     stream concurrently with the LJ chain with 1, 2 or all resident blocks
+//     per SM (fewer blocks leave the SMs' registers to the LJ kernels).
+// The choice changes only the speed; results are bitwise the same for a
+// given split.
 static int autotune(mdg_ctx* c)
 {
   if (c->tuned || !c->bt.ctr) return MDG_OK;
   c->tuned = true;
   if (c->prm.task_mode != 0) return MDG_OK;
+  const bool lj = c->prm.potentials & MDG_POT_AIREBO_LJ;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  struct Cfg { bool overlap; int grid; };
+  std::vector<Cfg> cfgs = {{false, c->rebo_task_blocks}};
+  if (lj)
+    for (int per : {1, 2})
+      if (sms * per < c->rebo_task_blocks) cfgs.push_back({true, sms * per});
+  if (lj) cfgs.push_back({true, c->rebo_task_blocks});
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
+  float best_all = 1e30f;
+  int best_mode = 0;
+  Cfg best_cfg = cfgs[0];
   for (int mode = 0; mode < 2; mode++) {
     c->bt.pairs = mode;
-    int rc = evaluate(c);
-    if (rc) return rc;
-    float best = 1e30f;
-    for (int r = 0; r < 3; r++) {
-      CK(cudaEventRecord(e0, c->stream));
-      rc = evaluate(c);
+    c->tune_ms[mode] = 1e30f;
+    for (const Cfg& g : cfgs) {
+      c->overlap = g.overlap;
+      c->rebo_grid = g.grid;
+      int rc = evaluate(c);
       if (rc) return rc;
-      CK(cudaEventRecord(e1, c->stream));
-      CK(cudaEventSynchronize(e1));
-      float ms = 0.0f;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
-      best = std::min(best, ms);
+      float best = 1e30f;
+      for (int r = 0; r < 3; r++) {
+        CK(cudaEventRecord(e0, c->stream));
+        rc = evaluate(c);
+        if (rc) return rc;
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+      }
+      c->tune_ms[mode] = std::min(c->tune_ms[mode], best);
+      if (best < best_all) {
+        best_all = best;
+        best_mode = mode;
+        best_cfg = g;
+      }
     }
-    c->tune_ms[mode] = best;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  c->bt.pairs = c->tune_ms[1] < c->tune_ms[0] ? 1 : 0;
+  c->bt.pairs = best_mode;
+  c->overlap = best_cfg.overlap;
+  c->rebo_grid = best_cfg.grid;
   return read_status(c);
 }
 
@@ -1891,6 +1959,14 @@ int mdg_batch_energies(mdg_ctx* c, double* e_sys)
   rc = read_status(c);
   if (rc) return rc;
   for (size_t q = 0; q < h.size(); q++) e_sys[q] = h[q] * c->unit_e;
+  return MDG_OK;
+}
+
+int mdg_tuned_launch(mdg_ctx* c, int* overlap, int* rebo_blocks)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  if (overlap) *overlap = c->overlap ? 1 : 0;
+  if (rebo_blocks) *rebo_blocks = c->rebo_grid > 0 ? c->rebo_grid : c->rebo_task_blocks;
   return MDG_OK;
 }
 
