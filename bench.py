@@ -173,16 +173,10 @@ def main():
     import torch
     import mdtk_b200 as M
 
+    from mdtk_b200.replicas import Replicas, aggregate_rate
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    reps = Replicas("nccl")
+    barrier = reps.barrier
 
     if args.precision_study:
         return precision_study(args, local, rank)
@@ -220,11 +214,8 @@ def main():
     clk = clocks.stop()
     ctx.sync()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n * args.steps / (total_ms * 1e-3)
+    total_ms = reps.max(total_ms)
+    value = aggregate_rate(n * args.steps, world, total_ms * 1e-3)
 
     # per-kernel device times over a short profiled window (same stream)
     ctx.set_profiling(True)
@@ -268,10 +259,7 @@ def main():
     for k in range(args.e2e_steps):
         ctx.step_host(1, DT_FS, pos, vel)
     t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = reps.max(t_e2e)
     e2e = {"value": world * n * args.e2e_steps / t_e2e, "unit": "atom-steps/s",
            "h2d_bytes_per_step": 2 * 32 * n, "d2h_bytes_per_step": 2 * 32 * n + 16,
            "steps": args.e2e_steps, "timer": "host wall clock around mdg_step_host calls (each ends synchronised)"}
@@ -304,10 +292,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         mix_ms = sum(a.elapsed_time(b) for a, b in evm)
-        if dist is not None:
-            t = torch.tensor([mix_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            mix_ms = float(t.item())
+        mix_ms = reps.max(mix_ms)
         mixed = {"value": world * n * kmix / (mix_ms * 1e-3), "unit": "atom-steps/s", "steps": kmix,
                  "ms_per_step": mix_ms / kmix,
                  "force_err_vs_fp64": {"norm_rel": rel, "max_abs_over_rms": maxrms},
@@ -340,10 +325,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         b_ms = sum(a.elapsed_time(b) for a, b in evb)
-        if dist is not None:
-            t = torch.tensor([b_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            b_ms = float(t.item())
+        b_ms = reps.max(b_ms)
         bx.sync()
         bx.set_profiling(True)
         for k in range(5):
@@ -481,8 +463,7 @@ def main():
                 line["cpu_baseline"] = {"value": None, "unit": "atom-steps/s", "cores": 1, "kind": "reference",
                                         "sample": f"unavailable: {e}"}
         print(json.dumps(line))
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 
