@@ -351,50 +351,26 @@ __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
 
-// Plain LJ pairs, one warp per atom.  Only ~1/4 of an LJ-list entry is
-// inside the pair's cutoff, so the warp first filters 32 entries at a time
-// (position load + distance) and appends the survivors, in list order, to a
-// per-warp queue in shared memory; every 32 queued pairs are then evaluated
-// with all lanes busy.  Pairs that need b*_ij or a connectivity gradient are
-// compacted, in list order, into the atom's special list.
-template <class Real>
-__global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, State S, NList L,
-                                                       const int* nbonds, ForceOut O, SpecialTasks Tk,
-                                                       unsigned int* status)
+// LJ pairs inside their cutoff, one warp per atom: the atom's LJ list is
+// read 32 entries at a time and the entries within the pair's cutoff R2 are
+// appended, in list order, to the atom's in-range list (about a quarter of
+// the list).  It needs only positions and the list, so it runs concurrently
+// with the bond and connectivity kernels; its few registers let many warps
+// hide the position gathers.
+__global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NList L, int* inr, int* inr_cnt)
 {
-  __shared__ int queue[kThreads / 32][64];
-  if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
   const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (a >= S.n) return;  // whole warps
-  int* q = queue[threadIdx.x >> 5];
   const double4 pa = S.pos[a];
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
   const Box& box = box_of(S, a);
   const int cnt = L.cnt[a];
   const int* lst = L.list + (long)a * L.cap;
+  int* out = inr + (long)a * L.cap;
   const unsigned below = (1u << lane) - 1u;
-  SinkT<Real> sk;
-  sk.a = a;
-  sk.g = v3(0, 0, 0);
-  sk.A = nullptr;
-  sk.W = nullptr;
-  double e = 0.0;
-  int nsp = 0, qn = 0;
-  auto evaluate = [&](int nq) {
-    int kind = 0, b = -1;
-    if (lane < nq) {
-      b = q[lane];
-      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
-    if (kind == 2) {
-      const int pos = nsp + __popc(m & below);
-      if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
-    }
-    nsp += __popc(m);
-  };
+  int k = 0;
   for (int base = 0; base < cnt; base += 32) {
     const int s = base + lane;
     bool in = false;
@@ -407,18 +383,51 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
       in = !(norm2(rv) > R2 * R2);
     }
     const unsigned m = __ballot_sync(0xffffffffu, in);
-    if (in) q[qn + __popc(m & below)] = b;
-    qn += __popc(m);
-    __syncwarp();
-    if (qn >= 32) {
-      evaluate(32);
-      __syncwarp();
-      if (lane < qn - 32) q[lane] = q[lane + 32];
-      __syncwarp();
-      qn -= 32;
-    }
+    if (in) out[k + __popc(m & below)] = b;
+    k += __popc(m);
   }
-  if (qn > 0) evaluate(qn);
+  if (lane == 0) inr_cnt[a] = k;
+}
+
+// Plain LJ pairs, one warp per atom over its in-range list, 32 pairs per
+// round with every lane busy (the last round excepted).  Pairs that need
+// b*_ij or a connectivity gradient are compacted, in list order, into the
+// atom's special list.
+template <class Real>
+__global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* inr,
+                                                       const int* inr_cnt, const int* nbonds, ForceOut O,
+                                                       SpecialTasks Tk, unsigned int* status)
+{
+  if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (a >= S.n) return;  // whole warps
+  const double4 pa = S.pos[a];
+  const V3 xa = v3(pa.x, pa.y, pa.z);
+  const int ta = (int)pa.w;
+  const int cnt = inr_cnt[a];
+  const int* q = inr + (long)a * L.cap;
+  const unsigned below = (1u << lane) - 1u;
+  SinkT<Real> sk;
+  sk.a = a;
+  sk.g = v3(0, 0, 0);
+  sk.A = nullptr;
+  sk.W = nullptr;
+  double e = 0.0;
+  int nsp = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    int kind = 0, b = -1;
+    if (base + lane < cnt) {
+      b = q[base + lane];
+      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
+    if (kind == 2) {
+      const int pos = nsp + __popc(m & below);
+      if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
+    }
+    nsp += __popc(m);
+  }
   double gx = sk.g.x, gy = sk.g.y, gz = sk.g.z;
   for (int o = 16; o > 0; o >>= 1) {
     gx += __shfl_xor_sync(0xffffffffu, gx, o);
@@ -812,9 +821,13 @@ struct mdg_ctx {
   // REBO tasks on a second stream, concurrent with the LJ chain (which does
   // not read their records until the reduction): fork/join by events, also
   // inside a captured step
+  // and the LJ distance filter on a third, concurrently with the bond and
+  // connectivity kernels
   bool overlap = false;
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t side = nullptr, side2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
+  int* lj_inr = nullptr;      // [n * LJ list cap] in-range LJ partners of the step, list order
+  int* lj_inr_cnt = nullptr;  // [n]
   bool tuned = false;        // the autotuner ran for this system
   float tune_ms[2] = {0, 0};  // its timings of one force evaluation per task mode
 
@@ -975,7 +988,9 @@ void free_system(mdg_ctx* c)
   }
   void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
                 c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work, c->spc.wrev,
-                c->spc.wcnt, c->scan_tiles};
+                c->spc.wcnt, c->scan_tiles, c->lj_inr, c->lj_inr_cnt};
+  c->lj_inr = nullptr;
+  c->lj_inr_cnt = nullptr;
   c->scan_tiles = nullptr;
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   c->step_graph = nullptr;
@@ -1169,11 +1184,23 @@ int evaluate(mdg_ctx* c)
   const int pot = c->prm.potentials;
   const bool rebo = pot & MDG_POT_REBO, tors = pot & MDG_POT_ETORS, lj = pot & MDG_POT_AIREBO_LJ;
   const bool tasks = c->bt.ctr != nullptr;
+  const bool ovl = tasks && lj && c->overlap && !c->prof && c->side;
+  if (lj) {
+    // the in-range filter needs only positions and the LJ list
+    cudaStream_t fs = c->stream;
+    if (ovl) {
+      CK(cudaEventRecord(c->ev_fork2, c->stream));
+      CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
+      fs = c->side2;
+    }
+    LAUNCH_ON(c, fs, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
+              c->lj_inr_cnt);
+    if (ovl) CK(cudaEventRecord(c->ev_join2, c->side2));
+  }
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
   LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
   const bool f32p = c->prm.precision == MDG_PREC_FP32_MIXED;
-  const bool ovl = tasks && lj && c->overlap && !c->prof && c->side;
   cudaStream_t rs = c->stream;
   if (ovl) {
     CK(cudaEventRecord(c->ev_fork, c->stream));
@@ -1201,20 +1228,21 @@ int evaluate(mdg_ctx* c)
                 c->d_status);
     }
   }
-  if (ovl) CK(cudaEventRecord(c->ev_join, c->side));
   else
     LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
            tors ? 1 : 0, c->fo, c->d_status);
+  if (ovl) CK(cudaEventRecord(c->ev_join, c->side));
   if (pot & MDG_POT_BRENNER)
     LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
     LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
+    if (ovl) CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
     if (f32p)
-      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb,
-             c->fo, c->spc, c->d_status);
+      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
+             c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
     else
-      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->bb.nb,
-             c->fo, c->spc, c->d_status);
+      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
+             c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
     ScanPair sp;
     sp.in[0] = c->spc.cnt;
     sp.in[1] = c->spc.rsz;
@@ -1370,8 +1398,11 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
     delete bt;
   }
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) != cudaSuccess) {
     mdg_destroy(c);
     return fail(MDG_ERR_CUDA, "cudaStreamCreate / cudaEventCreate");
   }
@@ -1404,7 +1435,10 @@ int mdg_destroy(mdg_ctx* c)
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
+  if (c->ev_join2) cudaEventDestroy(c->ev_join2);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->side2) cudaStreamDestroy(c->side2);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return MDG_OK;
@@ -1530,6 +1564,11 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     L.list = dalloc<int>((size_t)n * L.cap);
     L.pos0 = dalloc<double4>(n);
     if (!L.cnt || !L.list || !L.pos0) return fail(MDG_ERR_CUDA, "cudaMalloc (neighbour list)");
+    if (l == 1) {
+      c->lj_inr = dalloc<int>((size_t)n * L.cap);
+      c->lj_inr_cnt = dalloc<int>(n);
+      if (!c->lj_inr || !c->lj_inr_cnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ in-range list)");
+    }
     int rc = nsys > 1 ? setup_grid_batch(c, l, hpos) : setup_grid(c, l, hpos);
     if (rc) return rc;
   }
