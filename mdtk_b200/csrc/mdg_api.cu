@@ -1150,26 +1150,37 @@ void prof_end(mdg_ctx* c);
     (c)->launches++;                                                  \
   } while (0)
 
+// Displacement check and (when it fires) cell-list rebuild of list l on
+// stream st; each list has its own partials, flags and grid, so the two
+// lists can run on different streams.
+constexpr int kDispParts = 64;
+int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
+{
+  if (!c->has_list[l]) return MDG_OK;
+  State S = c->S();
+  NList& L = c->nl[l];
+  Grid& g = c->grid[l];
+  int* need = c->d_need + l;
+  double* part = c->d_part + 2 * kDispParts * l;
+  LAUNCH_ON(c, st, "nl_disp_partial", k_disp_partial, kDispParts, kThreads, S, L, part);
+  LAUNCH_ON(c, st, "nl_disp_final", k_disp_final, 1, 32, part, kDispParts, L.trigger, need, c->d_force + l);
+  if (!g.brute) {
+    LAUNCH_ON(c, st, "nl_cell_clear", k_cell_clear, nblk(g.ncell), kThreads, g, need);
+    LAUNCH_ON(c, st, "nl_cell_count", k_cell_count, nblk(c->n), kThreads, S, g, need);
+    LAUNCH_ON(c, st, "nl_cell_scan", k_cell_scan, 1, 1024, g, need);
+    LAUNCH_ON(c, st, "nl_cell_fill", k_cell_fill, nblk(c->n), kThreads, S, g, need);
+    LAUNCH_ON(c, st, "nl_cell_sort", k_cell_sort, nblk(g.ncell), kThreads, g, need);
+  }
+  LAUNCH_ON(c, st, l == 0 ? "nl_build_rebo" : "nl_build_lj", k_nl_build, nblk(c->n), kThreads, S, g, L, need,
+            c->d_status);
+  return MDG_OK;
+}
+
 int rebuild_lists(mdg_ctx* c)
 {
-  State S = c->S();
-  int nparts = 64;
-  for (int l = 0; l < 2; l++) {
-    if (!c->has_list[l]) continue;
-    NList& L = c->nl[l];
-    Grid& g = c->grid[l];
-    int* need = c->d_need + l;
-    LAUNCH(c, "nl_disp_partial", k_disp_partial, nparts, kThreads, S, L, c->d_part);
-    LAUNCH(c, "nl_disp_final", k_disp_final, 1, 32, c->d_part, nparts, L.trigger, need, c->d_force + l);
-    if (!g.brute) {
-      LAUNCH(c, "nl_cell_clear", k_cell_clear, nblk(g.ncell), kThreads, g, need);
-      LAUNCH(c, "nl_cell_count", k_cell_count, nblk(c->n), kThreads, S, g, need);
-      LAUNCH(c, "nl_cell_scan", k_cell_scan, 1, 1024, g, need);
-      LAUNCH(c, "nl_cell_fill", k_cell_fill, nblk(c->n), kThreads, S, g, need);
-      LAUNCH(c, "nl_cell_sort", k_cell_sort, nblk(g.ncell), kThreads, g, need);
-    }
-    LAUNCH(c, l == 0 ? "nl_build_rebo" : "nl_build_lj", k_nl_build, nblk(c->n), kThreads, S, g, L, need, c->d_status);
-  }
+  int rc = rebuild_list(c, 0, c->stream);
+  if (!rc) rc = rebuild_list(c, 1, c->stream);
+  if (rc) return rc;
   return launch_check(c);
 }
 
@@ -1178,24 +1189,30 @@ int rebuild_lists(mdg_ctx* c)
 // (or d_energy when slot < 0).
 int evaluate(mdg_ctx* c)
 {
-  int rc = rebuild_lists(c);
-  if (rc) return rc;
   State S = c->S();
   const int pot = c->prm.potentials;
   const bool rebo = pot & MDG_POT_REBO, tors = pot & MDG_POT_ETORS, lj = pot & MDG_POT_AIREBO_LJ;
   const bool tasks = c->bt.ctr != nullptr;
   const bool ovl = tasks && lj && c->overlap && !c->prof && c->side;
-  if (lj) {
-    // the in-range filter needs only positions and the LJ list
-    cudaStream_t fs = c->stream;
-    if (ovl) {
-      CK(cudaEventRecord(c->ev_fork2, c->stream));
-      CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
-      fs = c->side2;
-    }
-    LAUNCH_ON(c, fs, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
+  int rc;
+  if (ovl) {
+    // the LJ list's check/rebuild and the in-range filter (positions and the
+    // LJ list only) on the third stream, beside the REBO list and the bonds
+    CK(cudaEventRecord(c->ev_fork2, c->stream));
+    CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
+    rc = rebuild_list(c, 1, c->side2);
+    if (rc) return rc;
+    LAUNCH_ON(c, c->side2, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
               c->lj_inr_cnt);
-    if (ovl) CK(cudaEventRecord(c->ev_join2, c->side2));
+    CK(cudaEventRecord(c->ev_join2, c->side2));
+    rc = rebuild_list(c, 0, c->stream);
+    if (rc) return rc;
+  } else {
+    rc = rebuild_lists(c);
+    if (rc) return rc;
+    if (lj)
+      LAUNCH(c, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
+             c->lj_inr_cnt);
   }
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
   LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
@@ -1574,7 +1591,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   }
   int one[2] = {1, 1};
   CK(cudaMemcpy(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice));
-  c->d_part = dalloc<double>(2 * 64);
+  c->d_part = dalloc<double>(2 * 2 * kDispParts);
 
   // bonds and force outputs
   const int mb = c->mb;
