@@ -410,12 +410,7 @@ int adj_eval_at(mdg_ctx* c, const double4* p)
 
 int adj_step(mdg_ctx* c, double dt)
 {
-  State S = c->S();
-  LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dt);
-  int rc = evaluate(c);
-  if (rc) return rc;
-  LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dt, c->e_kin, c->d_status);
-  return launch_check(c);
+  return evaluate(c, &dt);  // position update, forces, velocity update (mdg_run's step)
 }
 
 template <class T>

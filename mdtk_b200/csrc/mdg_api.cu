@@ -48,30 +48,39 @@ inline int nblk(int n, int t = kThreads) { return (n + t - 1) / t; }
 
 // ---------------------------------------------------------------- kernels
 
-__global__ void k_disp_partial(State S, NList L, double* part)
+// Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
+// of the step) and, per block, the two largest displacements since each
+// list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
+__global__ void k_step_start(State S, double dt, int do_pos, NList L0, NList L1, int nl, double* part)
 {
-  __shared__ double s1[kThreads], s2[kThreads];
+  __shared__ double s1[2][kThreads], s2[2][kThreads];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double d1 = 0.0, d2 = 0.0;
+  double d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
   for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
-    double d = disp_atom(S, L, a);
-    if (d >= d1) { d2 = d1; d1 = d; }
-    else if (d >= d2) d2 = d;
+    if (do_pos) verlet_pos_atom(S, dt, a);
+    for (int l = 0; l < nl; l++) {
+      const double d = disp_atom(S, l == 0 ? L0 : L1, a);
+      if (d >= d1[l]) { d2[l] = d1[l]; d1[l] = d; }
+      else if (d >= d2[l]) d2[l] = d;
+    }
   }
-  s1[threadIdx.x] = d1;
-  s2[threadIdx.x] = d2;
+  for (int l = 0; l < nl; l++) {
+    s1[l][threadIdx.x] = d1[l];
+    s2[l][threadIdx.x] = d2[l];
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < nl) {
+    const int l = threadIdx.x;
     double t1 = 0.0, t2 = 0.0;
     for (int q = 0; q < blockDim.x; q++) {
-      double x[2] = {s1[q], s2[q]};
+      double x[2] = {s1[l][q], s2[l][q]};
       for (int z = 0; z < 2; z++) {
         if (x[z] >= t1) { t2 = t1; t1 = x[z]; }
         else if (x[z] >= t2) t2 = x[z];
       }
     }
-    part[2 * blockIdx.x] = t1;
-    part[2 * blockIdx.x + 1] = t2;
+    part[2 * gridDim.x * l + 2 * blockIdx.x] = t1;
+    part[2 * gridDim.x * l + 2 * blockIdx.x + 1] = t2;
   }
 }
 
@@ -610,10 +619,20 @@ __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, d
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
 }
 
-__global__ void k_verlet_pos(State S, double dt)
+// The gather and the end of a step in one pass (eq 2-4 and applyPBC): the
+// gather reads bond records and unit vectors, never positions, so each atom's
+// velocity, acceleration and wrap follow its own gradient at once.
+__global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, double dt,
+                            double* ekin, unsigned int* status)
 {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < S.n) verlet_pos_atom(S, dt, i);
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.n) return;
+  V3 g = gather_atom(B, O, a, with_lj, nullptr);
+  if (with_lj) g += mid_gather_atom(B, Tk, a);
+  grad[a] = make_double4(g.x, g.y, g.z, 0.0);
+  verlet_vel_atom(S, g, dt, a, status);
+  const double4 v = S.vel[a];
+  ekin[a] = S.mass[a] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
 }
 
 // initial accelerations (SimLoop.cxx:305-321)
@@ -625,16 +644,6 @@ __global__ void k_init_acc(State S, const double4* grad)
   double m = S.mass[i];
   double4 g = grad[i];
   S.acc[i] = make_double4(-g.x / m * kAccConv, -g.y / m * kAccConv, -g.z / m * kAccConv, 0.0);
-}
-
-__global__ void k_verlet_vel(State S, const double4* grad, double dt, double* ekin, unsigned int* status)
-{
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S.n) return;
-  double4 g = grad[i];
-  verlet_vel_atom(S, v3(g.x, g.y, g.z), dt, i, status);
-  double4 v = S.vel[i];
-  ekin[i] = S.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
 }
 
 __global__ void k_ekin(State S, double* ekin)
@@ -1150,10 +1159,21 @@ void prof_end(mdg_ctx* c);
     (c)->launches++;                                                  \
   } while (0)
 
-// Displacement check and (when it fires) cell-list rebuild of list l on
-// stream st; each list has its own partials, flags and grid, so the two
-// lists can run on different streams.
-constexpr int kDispParts = 64;
+// The displacement partials of both lists (after the step's position update
+// when step_dt is given) in one pass over the atoms.
+constexpr int kDispParts = 296;  // 2 blocks per SM of a B200
+int step_start(mdg_ctx* c, const double* step_dt)
+{
+  State S = c->S();
+  const int nl = c->has_list[1] ? 2 : 1;
+  LAUNCH(c, step_dt ? "verlet_pos_disp" : "nl_disp_partial", k_step_start, kDispParts, kThreads, S,
+         step_dt ? *step_dt : 0.0, step_dt ? 1 : 0, c->nl[0], c->nl[1], nl, c->d_part);
+  return MDG_OK;
+}
+
+// Displacement decision and (when it fires) cell-list rebuild of list l on
+// stream st, from the partials of step_start; each list has its own
+// partials, flags and grid, so the two lists can run on different streams.
 int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
 {
   if (!c->has_list[l]) return MDG_OK;
@@ -1162,7 +1182,6 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
   Grid& g = c->grid[l];
   int* need = c->d_need + l;
   double* part = c->d_part + 2 * kDispParts * l;
-  LAUNCH_ON(c, st, "nl_disp_partial", k_disp_partial, kDispParts, kThreads, S, L, part);
   LAUNCH_ON(c, st, "nl_disp_final", k_disp_final, 1, 32, part, kDispParts, L.trigger, need, c->d_force + l);
   if (!g.brute) {
     LAUNCH_ON(c, st, "nl_cell_clear", k_cell_clear, nblk(g.ncell), kThreads, g, need);
@@ -1176,18 +1195,20 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
   return MDG_OK;
 }
 
-int rebuild_lists(mdg_ctx* c)
+int rebuild_lists(mdg_ctx* c, const double* step_dt = nullptr)
 {
-  int rc = rebuild_list(c, 0, c->stream);
+  int rc = step_start(c, step_dt);
+  if (!rc) rc = rebuild_list(c, 0, c->stream);
   if (!rc) rc = rebuild_list(c, 1, c->stream);
   if (rc) return rc;
   return launch_check(c);
 }
 
 // One force evaluation at the current positions; leaves dE/dx in c->grad and
-// per-atom energies in c->fo.  Energies are summed into elog slot `slot`
-// (or d_energy when slot < 0).
-int evaluate(mdg_ctx* c)
+// per-atom energies in c->fo.  With step_dt, the evaluation is the body of a
+// velocity-Verlet step: the position update comes first (fused with the
+// displacement check) and the velocity update last (fused with the gather).
+int evaluate(mdg_ctx* c, const double* step_dt = nullptr)
 {
   State S = c->S();
   const int pot = c->prm.potentials;
@@ -1198,6 +1219,8 @@ int evaluate(mdg_ctx* c)
   if (ovl) {
     // the LJ list's check/rebuild and the in-range filter (positions and the
     // LJ list only) on the third stream, beside the REBO list and the bonds
+    rc = step_start(c, step_dt);
+    if (rc) return rc;
     CK(cudaEventRecord(c->ev_fork2, c->stream));
     CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
     rc = rebuild_list(c, 1, c->side2);
@@ -1208,7 +1231,7 @@ int evaluate(mdg_ctx* c)
     rc = rebuild_list(c, 0, c->stream);
     if (rc) return rc;
   } else {
-    rc = rebuild_lists(c);
+    rc = rebuild_lists(c, step_dt);
     if (rc) return rc;
     if (lj)
       LAUNCH(c, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
@@ -1291,7 +1314,11 @@ int evaluate(mdg_ctx* c)
   if (tasks || lj)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
-  LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
+  if (step_dt)
+    LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
+           *step_dt, c->e_kin, c->d_status);
+  else
+    LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
   return launch_check(c);
 }
 
@@ -1898,9 +1925,7 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
       cudaGraph_t g = nullptr;
       int64_t l0 = c->launches;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
-      rc = evaluate(c);
-      LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
+      rc = evaluate(c, &dtf);  // position update, forces, velocity update
       cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
       c->graph_launches = (int)(c->launches - l0);
       c->launches = l0;
@@ -1919,10 +1944,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     return launch_check(c);
   }
   for (int s = 0; s < nsteps; s++) {
-    LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
-    rc = evaluate(c);
+    rc = evaluate(c, &dtf);  // position update, forces, velocity update
     if (rc) return rc;
-    LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
     if (log) {
       rc = reduce_energies(c, c->d_elog, 4, s, true);
       if (rc) return rc;
@@ -1975,10 +1998,8 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->elog_cap = need;
   }
   for (int s = 0; s < nsteps; s++) {
-    LAUNCH(c, "verlet_pos", k_verlet_pos, nblk(c->n), kThreads, S, dtf);
-    rc = evaluate(c);
+    rc = evaluate(c, &dtf);  // position update, forces, velocity update
     if (rc) return rc;
-    LAUNCH(c, "verlet_vel", k_verlet_vel, nblk(c->n), kThreads, S, c->grad, dtf, c->e_kin, c->d_status);
     rc = sys_energies(c, c->d_elog + (int64_t)s * c->nsys * 4);
     if (rc) return rc;
   }
