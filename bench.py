@@ -537,8 +537,8 @@ def precision_study(args, local, rank):
 FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_plain": 5151.5, "lj_special": 5205.5}
 STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
 # dram read+write bytes per launch from an ncu capture of the same workload
-# (profiles/hot_kernels_airebo_ethane43688_fp64.md), or None.
-TRAFFIC_PER_LAUNCH = {"rebo_tors": 22.91e6, "lj_plain": 47.45e6, "lj_special": 24.79e6, "bond_reduce": 35.04e6}
+# (`ncu --set full`, one launch of each kernel), or None.
+TRAFFIC_PER_LAUNCH = {"rebo_tors": 22.84e6, "lj_plain": 22.85e6, "lj_special": 22.70e6, "lj_filter": 36.49e6}
 
 
 if __name__ == "__main__":

@@ -48,13 +48,20 @@ inline int nblk(int n, int t = kThreads) { return (n + t - 1) / t; }
 
 // ---------------------------------------------------------------- kernels
 
+// (t1, t2) <- the two largest of {t1, t2, u1, u2}, given t1 >= t2, u1 >= u2.
+__device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, double u2)
+{
+  if (u1 >= t1) { t2 = fmax(t1, u2); t1 = u1; }
+  else t2 = fmax(t2, u1);
+}
+
 // Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
 // of the step) and, per block, the two largest displacements since each
 // list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
 __global__ void k_step_start(State S, double dt, int do_pos, NList L0, NList L1, int nl, double* part)
 {
-  __shared__ double s1[2][kThreads], s2[2][kThreads];
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double s1[2][kThreads / 32], s2[2][kThreads / 32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
   for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
     if (do_pos) verlet_pos_atom(S, dt, a);
@@ -65,38 +72,48 @@ __global__ void k_step_start(State S, double dt, int do_pos, NList L0, NList L1,
     }
   }
   for (int l = 0; l < nl; l++) {
-    s1[l][threadIdx.x] = d1[l];
-    s2[l][threadIdx.x] = d2[l];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u1 = __shfl_down_sync(0xffffffffu, d1[l], o), u2 = __shfl_down_sync(0xffffffffu, d2[l], o);
+      top2_merge(d1[l], d2[l], u1, u2);
+    }
+    if (lane == 0) {
+      s1[l][wid] = d1[l];
+      s2[l][wid] = d2[l];
+    }
   }
   __syncthreads();
   if (threadIdx.x < nl) {
     const int l = threadIdx.x;
     double t1 = 0.0, t2 = 0.0;
-    for (int q = 0; q < blockDim.x; q++) {
-      double x[2] = {s1[l][q], s2[l][q]};
-      for (int z = 0; z < 2; z++) {
-        if (x[z] >= t1) { t2 = t1; t1 = x[z]; }
-        else if (x[z] >= t2) t2 = x[z];
-      }
-    }
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) top2_merge(t1, t2, s1[l][w], s2[l][w]);
     part[2 * gridDim.x * l + 2 * blockIdx.x] = t1;
     part[2 * gridDim.x * l + 2 * blockIdx.x + 1] = t2;
   }
 }
 
-// need = force || top1 + top2 > trigger (NeighbourList::MovedTooMuch)
+// need = force || top1 + top2 > trigger (NeighbourList::MovedTooMuch); one
+// warp: each lane keeps the two largest of a strided share of the partials,
+// then the lanes' pairs are merged by shuffles (the two largest of a set do
+// not depend on the order they are met in).
 __global__ void k_disp_final(const double* part, int nparts, double trigger, int* need, int* force)
 {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x;
+  if (lane >= 32) return;
   double t1 = 0.0, t2 = 0.0;
-  for (int q = 0; q < 2 * nparts; q++) {
-    double x = part[q];
+  for (int q = lane; q < 2 * nparts; q += 32) {
+    const double x = part[q];
     if (x >= t1) { t2 = t1; t1 = x; }
     else if (x >= t2) t2 = x;
   }
-  int nd = (*force) || (t1 + t2 > trigger);
-  *need = nd;
-  *force = 0;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double u1 = __shfl_down_sync(0xffffffffu, t1, o), u2 = __shfl_down_sync(0xffffffffu, t2, o);
+    top2_merge(t1, t2, u1, u2);
+  }
+  if (lane == 0) {
+    const int nd = (*force) || (t1 + t2 > trigger);
+    *need = nd;
+    *force = 0;
+  }
 }
 
 __global__ void k_cell_clear(Grid g, const int* need)
