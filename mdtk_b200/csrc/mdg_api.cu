@@ -652,6 +652,28 @@ __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk
   ekin[a] = S.mass[a] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
 }
 
+// Host-step layout conversion: io = [pos (n*3) | vel (n*3)] in the caller's
+// units; the species in pos.w is kept.
+__global__ void k_state_unpack(State S, const double* io, double ul, double uv)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  const double* p = io + 3 * (long)i;
+  const double* v = io + 3 * ((long)S.n + i);
+  S.pos[i] = make_double4(p[0] * ul, p[1] * ul, p[2] * ul, S.pos[i].w);
+  S.vel[i] = make_double4(v[0] * uv, v[1] * uv, v[2] * uv, 0.0);
+}
+__global__ void k_state_pack(State S, double* io, double ul, double uv)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  const double4 p = S.pos[i], v = S.vel[i];
+  double* po = io + 3 * (long)i;
+  double* vo = io + 3 * ((long)S.n + i);
+  po[0] = p.x / ul; po[1] = p.y / ul; po[2] = p.z / ul;
+  vo[0] = v.x / uv; vo[1] = v.y / uv; vo[2] = v.z / uv;
+}
+
 // initial accelerations (SimLoop.cxx:305-321)
 __global__ void k_init_acc(State S, const double4* grad)
 {
@@ -874,6 +896,7 @@ struct mdg_ctx {
   std::vector<std::pair<std::string, size_t>> prof_recs;  // name, index of the start event
   // host staging for mdg_step_host
   double4* h_stage = nullptr;
+  double* d_io = nullptr;       // [6 n] the host step's pos and vel in the caller's [n*3] layout
   std::vector<int> h_type;
   AdjWs* adj = nullptr;       // adjoint path, allocated on first use
 
@@ -1045,6 +1068,8 @@ void free_system(mdg_ctx* c)
   std::memset(&c->bt, 0, sizeof(c->bt));
   if (c->h_stage) cudaFreeHost(c->h_stage);
   c->h_stage = nullptr;
+  if (c->d_io) cudaFree(c->d_io);
+  c->d_io = nullptr;
   c->pos = c->vel = c->acc = c->grad = nullptr;
   c->image = nullptr;
   c->fixed = nullptr;
@@ -1724,6 +1749,8 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   }
   if (cudaHostAlloc((void**)&c->h_stage, 2 * (size_t)n * sizeof(double4), cudaHostAllocDefault) != cudaSuccess)
     return fail(MDG_ERR_CUDA, "cudaHostAlloc (staging)");
+  c->d_io = dalloc<double>(6 * (size_t)n);
+  if (!c->d_io) return fail(MDG_ERR_CUDA, "cudaMalloc (host-step staging)");
   CK(cudaDeviceSynchronize());
   return MDG_OK;
 }
@@ -1911,6 +1938,30 @@ static int autotune(mdg_ctx* c)
   return read_status(c);
 }
 
+// The captured step (position update, forces, velocity update) for time
+// step dtf on the context's stream, captured again when either changes.
+static int ensure_step_graph(mdg_ctx* c, double dtf)
+{
+  if (c->step_graph && c->graph_dt == dtf && c->graph_stream == c->stream) return MDG_OK;
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
+  cudaGraph_t g = nullptr;
+  int64_t l0 = c->launches;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = evaluate(c, &dtf);
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  c->graph_launches = (int)(c->launches - l0);
+  c->launches = l0;
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&c->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+  c->graph_dt = dtf;
+  c->graph_stream = c->stream;
+  return MDG_OK;
+}
+
 int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
@@ -1933,36 +1984,22 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     if (!c->d_elog) return fail(MDG_ERR_CUDA, "cudaMalloc (energy log)");
     c->elog_cap = (int64_t)nsteps * 4;
   }
-  // Without per-step energies (and without profiling) a step is replayed
-  // from a CUDA graph: same kernels, same arguments, no host launch cost.
-  if (!log && !c->prof && nsteps > 0) {
-    if (!c->step_graph || c->graph_dt != dtf || c->graph_stream != c->stream) {
-      if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
-      c->step_graph = nullptr;
-      cudaGraph_t g = nullptr;
-      int64_t l0 = c->launches;
-      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      rc = evaluate(c, &dtf);  // position update, forces, velocity update
-      cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-      c->graph_launches = (int)(c->launches - l0);
-      c->launches = l0;
-      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-      if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&c->step_graph, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-      c->graph_dt = dtf;
-      c->graph_stream = c->stream;
-    }
-    for (int s = 0; s < nsteps; s++) {
-      CK(cudaGraphLaunch(c->step_graph, c->stream));
-      c->launches += c->graph_launches;
-    }
-    return launch_check(c);
+  // Unless profiling, a step is replayed from a CUDA graph: same kernels,
+  // same arguments, no host launch cost; the per-step energy sums (when
+  // asked for) follow each replay.
+  const bool graph = !c->prof && nsteps > 0;
+  if (graph) {
+    rc = ensure_step_graph(c, dtf);
+    if (rc) return rc;
   }
   for (int s = 0; s < nsteps; s++) {
-    rc = evaluate(c, &dtf);  // position update, forces, velocity update
-    if (rc) return rc;
+    if (graph) {
+      CK(cudaGraphLaunch(c->step_graph, c->stream));
+      c->launches += c->graph_launches;
+    } else {
+      rc = evaluate(c, &dtf);  // position update, forces, velocity update
+      if (rc) return rc;
+    }
     if (log) {
       rc = reduce_energies(c, c->d_elog, 4, s, true);
       if (rc) return rc;
@@ -2145,26 +2182,20 @@ int mdg_step_host(mdg_ctx* c, int nsteps, double dt, double* pos, double* vel, d
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (!pos || !vel) return fail(MDG_ERR_ARG, "null state buffer");
   const int n = c->n;
-  double4* hp = c->h_stage;
-  double4* hv = c->h_stage + n;
-  for (int i = 0; i < n; i++) {
-    hp[i] = make_double4(pos[3 * i] * c->unit_len, pos[3 * i + 1] * c->unit_len, pos[3 * i + 2] * c->unit_len,
-                         (double)c->h_type[i]);
-    hv[i] = make_double4(vel[3 * i] * c->unit_vel, vel[3 * i + 1] * c->unit_vel, vel[3 * i + 2] * c->unit_vel, 0.0);
-  }
-  CK(cudaMemcpyAsync(c->pos, hp, n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->vel, hv, n * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  // the caller's [n*3] arrays move as they are (one copy each way; DMA
+  // straight from and to them when they are pinned) and are converted to and
+  // from the device layout by kernels
+  double* io = c->d_io;
+  CK(cudaMemcpyAsync(io, pos, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(io + 3 * (size_t)n, vel, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  State S = c->S();
+  LAUNCH(c, "state_unpack", k_state_unpack, nblk(n), kThreads, S, io, c->unit_len, c->unit_vel);
   int rc = mdg_run(c, nsteps, dt, epot, etot);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(hp, c->pos, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(hv, c->vel, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-  rc = read_status(c);
-  if (rc) return rc;
-  for (int i = 0; i < n; i++) {
-    pos[3 * i] = hp[i].x / c->unit_len; pos[3 * i + 1] = hp[i].y / c->unit_len; pos[3 * i + 2] = hp[i].z / c->unit_len;
-    vel[3 * i] = hv[i].x / c->unit_vel; vel[3 * i + 1] = hv[i].y / c->unit_vel; vel[3 * i + 2] = hv[i].z / c->unit_vel;
-  }
-  return MDG_OK;
+  LAUNCH(c, "state_pack", k_state_pack, nblk(n), kThreads, S, io, c->unit_len, c->unit_vel);
+  CK(cudaMemcpyAsync(pos, io, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(vel, io + 3 * (size_t)n, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return read_status(c);
 }
 
 int mdg_pipe_peak(int device, int fp32, double* tflops)
