@@ -246,6 +246,32 @@ int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const d
  * ran, its timings of one force evaluation in each mode (ms; 0 otherwise). */
 int mdg_task_mode(mdg_ctx* ctx, int* mode, float* ms_directed, float* ms_per_bond);
 
+/* ---- Thermal bath and adaptive time step ----
+ * The SimLoop step's thermal bath (SimLoop.cxx:352-388, geometries
+ * SimLoop.hpp:96-191) and adaptive dt (SimLoop.cxx:405-416), both off by
+ * default.  A free atom inside the bath (and flagged, Atom::apply_ThermalBath)
+ * feels dF = -V M gamma (1 - sqrt(T0/T)), T the bath's temperature at the
+ * start of the step (SimLoop::actualTemperatureOfThermalBath).  Batched
+ * contexts keep one bath temperature, dt and time per system. */
+#define MDG_TB_NONE 0
+#define MDG_TB_UNIVERSE 1  /* every atom (TB_GEOM_UNIVERSE) */
+#define MDG_TB_BOX 2       /* ThermalBathGeomBox: params zMin, dBoundary, zMinOfFreeZone; needs periodic x, y */
+#define MDG_TB_SPHERE 3    /* ThermalBathGeomSphere: params cx, cy, cz, radius, zMinOfFreeZone; open box */
+
+/* T0 in K; gamma in 1/(time unit) (the reference's default is 1e13 / s);
+ * params in length units; apply: NULL (every atom) or [n] flags. */
+int mdg_set_thermal_bath(mdg_ctx* ctx, int geom, double T0, double gamma, const double* params, const uint8_t* apply);
+
+/* Adaptive dt: after each step dt = 0.05 timeaccel / v_max (v_max over free
+ * atoms with neighbours), clamped to [1e-20, 5e-16] s; dt0 starts it.  While
+ * on, the dt argument of mdg_run / mdg_batch_run is ignored.  Setting it
+ * restarts the simulated time. */
+int mdg_set_adaptive_dt(mdg_ctx* ctx, int on, double timeaccel, double dt0);
+
+/* Simulated time and current dt per system ([nsys] each; time counts the
+ * adaptive steps since mdg_set_adaptive_dt). */
+int mdg_get_time(mdg_ctx* ctx, double* sim_time, double* dt);
+
 /* The launch configuration the autotuner chose (task_mode 0): overlap = 1
  * when the REBO tasks run on a second stream concurrently with the LJ
  * kernels, rebo_blocks = the REBO task kernel's grid.  No reference

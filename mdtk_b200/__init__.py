@@ -37,6 +37,8 @@ PARAM_REBO_BETA1_CC = 5
 NPARAM = 6
 PARAM_NAMES = ("eps_CC", "sigma_CC", "A_CC", "B1_CC", "alpha_CC", "beta1_CC")
 
+TB_NONE, TB_UNIVERSE, TB_BOX, TB_SPHERE = 0, 1, 2, 3
+
 UNITS_AEVFS = 0
 UNITS_CGS = 1
 PREC_FP64 = 0
@@ -100,6 +102,10 @@ def lib():
                                     ctypes.POINTER(ctypes.c_float)]
         L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_tuned_launch.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.mdg_set_thermal_bath.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp,
+                                           ctypes.POINTER(ctypes.c_uint8)]
+        L.mdg_set_adaptive_dt.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.mdg_get_time.argtypes = [vp, dp, dp]
         L.mdg_sync.argtypes = [vp]
         L.mdg_get_state.argtypes = [vp, dp, dp, i32p]
         L.mdg_launch_count.argtypes = [vp]
@@ -241,6 +247,28 @@ class Context:
         b = ctypes.c_float()
         _check(lib().mdg_task_mode(self.h, ctypes.byref(m), ctypes.byref(a), ctypes.byref(b)))
         return m.value, a.value, b.value
+
+    def set_thermal_bath(self, geom: int, T0: float = 0.0, gamma: float = 0.01, params=None, apply=None):
+        """SimLoop's thermal bath: geom TB_* , T0 (K), gamma (1/time unit),
+        params (box: zMin, dBoundary, zMinOfFreeZone; sphere: cx, cy, cz,
+        radius, zMinOfFreeZone), apply: per-atom flags or None."""
+        prm = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        ap = None
+        if apply is not None:
+            self._tb_apply = np.ascontiguousarray(apply, dtype=np.uint8)
+            ap = self._tb_apply.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        _check(lib().mdg_set_thermal_bath(self.h, geom, float(T0), float(gamma), _dp(prm), ap))
+
+    def set_adaptive_dt(self, on: bool, timeaccel: float = 1.0, dt0: float = 0.5):
+        _check(lib().mdg_set_adaptive_dt(self.h, 1 if on else 0, float(timeaccel), float(dt0)))
+
+    def get_time(self):
+        """(simulated time, current dt) per system."""
+        ns = getattr(self, "nsys", 1)
+        t = np.zeros(ns)
+        d = np.zeros(ns)
+        _check(lib().mdg_get_time(self.h, _dp(t), _dp(d)))
+        return t, d
 
     def tuned_launch(self):
         """(overlap, rebo_blocks): the autotuner's launch choice."""

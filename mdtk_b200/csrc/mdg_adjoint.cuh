@@ -286,6 +286,8 @@ int adj_check(mdg_ctx* c)
   if (c->prm.potentials & MDG_POT_BRENNER) return fail(MDG_ERR_ARG, "the adjoint covers REBO, the LJ term and torsion");
   if (c->nsys > 1) return fail(MDG_ERR_ARG, "the adjoint runs on single-system contexts");
   if (c->prm.units != MDG_UNITS_AEVFS) return fail(MDG_ERR_ARG, "the adjoint works in Angstrom / eV / fs units");
+  if (c->tb_geom || c->adaptive)
+    return fail(MDG_ERR_ARG, "the adjoint differentiates fixed-dt steps without a thermal bath");
   return MDG_OK;
 }
 
@@ -410,7 +412,11 @@ int adj_eval_at(mdg_ctx* c, const double4* p)
 
 int adj_step(mdg_ctx* c, double dt)
 {
-  return evaluate(c, &dt);  // position update, forces, velocity update (mdg_run's step)
+  StepDev sd;
+  std::memset(&sd, 0, sizeof(sd));
+  sd.dt = dt;
+  sd.nlc0 = c->nl[0].cnt;
+  return evaluate(c, &sd);  // position update, forces, velocity update (mdg_run's step, fixed dt)
 }
 
 template <class T>

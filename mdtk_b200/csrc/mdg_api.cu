@@ -58,13 +58,13 @@ __device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, do
 // Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
 // of the step) and, per block, the two largest displacements since each
 // list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
-__global__ void k_step_start(State S, double dt, int do_pos, NList L0, NList L1, int nl, double* part)
+__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, int nl, double* part)
 {
   __shared__ double s1[2][kThreads / 32], s2[2][kThreads / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
   for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
-    if (do_pos) verlet_pos_atom(S, dt, a);
+    if (do_pos) verlet_pos_atom(S, step_dt(P, S, a), a);
     for (int l = 0; l < nl; l++) {
       const double d = disp_atom(S, l == 0 ? L0 : L1, a);
       if (d >= d1[l]) { d2[l] = d1[l]; d1[l] = d; }
@@ -639,7 +639,7 @@ __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, d
 // The gather and the end of a step in one pass (eq 2-4 and applyPBC): the
 // gather reads bond records and unit vectors, never positions, so each atom's
 // velocity, acceleration and wrap follow its own gradient at once.
-__global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, double dt,
+__global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, StepDev P,
                             double* ekin, unsigned int* status)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -647,9 +647,70 @@ __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk
   V3 g = gather_atom(B, O, a, with_lj, nullptr);
   if (with_lj) g += mid_gather_atom(B, Tk, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
-  verlet_vel_atom(S, g, dt, a, status);
+  verlet_vel_ext_atom(S, g, P, a, status);
   const double4 v = S.vel[a];
   ekin[a] = S.mass[a] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
+}
+
+// Bath temperature at the start of a step (SimLoop::actualTemperatureOfThermalBath,
+// SimLoop.cxx:526-546): per system, the kinetic energy and count of the free
+// atoms inside the bath.  Grid (blocks per system, systems); partials
+// [system][block][2], summed in a fixed order by k_bath_final.
+__global__ void k_bath_partial(State S, StepDev P, const int64_t* first, double* part)
+{
+  __shared__ double se[kThreads], sn[kThreads];
+  const int sy = blockIdx.y;
+  const long b = first ? first[sy] : 0, e = first ? first[sy + 1] : S.n;
+  double ek = 0.0, cnt = 0.0;
+  for (long i = b + blockIdx.x * (long)blockDim.x + threadIdx.x; i < e; i += (long)gridDim.x * blockDim.x) {
+    if (S.fixed && S.fixed[i]) continue;
+    if (!in_bath(P, S, (int)i)) continue;
+    const double4 v = S.vel[i];
+    ek += S.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
+    cnt += 1.0;
+  }
+  se[threadIdx.x] = ek;
+  sn[threadIdx.x] = cnt;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      se[threadIdx.x] += se[threadIdx.x + w];
+      sn[threadIdx.x] += sn[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * ((long)sy * gridDim.x + blockIdx.x)] = se[0];
+    part[2 * ((long)sy * gridDim.x + blockIdx.x) + 1] = sn[0];
+  }
+}
+__global__ void k_bath_final(const double* part, int nblk_sys, int nsys, double* T)
+{
+  const int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= nsys) return;
+  double ek = 0.0, cnt = 0.0;
+  for (int q = 0; q < nblk_sys; q++) {
+    ek += part[2 * ((long)sy * nblk_sys + q)];
+    cnt += part[2 * ((long)sy * nblk_sys + q) + 1];
+  }
+  T[sy] = cnt == 0.0 ? 0.0 : ek / (3.0 / 2.0 * 8.617343e-5 * cnt);  // kb in eV/K (mdtk/consts.cxx:32)
+}
+
+// End of a step with adaptive dt (SimLoop.cxx:405-416): the simulated time
+// advances by the step's dt, then dt = 0.05 timeaccel / v_max clamped to
+// [1e-5, 0.5] fs (0.5 fs without a moving atom).
+__global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, double* time, double timeaccel)
+{
+  const int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= nsys) return;
+  const double vm = __longlong_as_double((long long)vmax[sy]);
+  const double dt_max = 0.5, dt_min = 1e-5;
+  double d = vm != 0.0 ? 0.05 * timeaccel / vm : dt_max;
+  if (d > dt_max) d = dt_max;
+  if (d < dt_min) d = dt_min;
+  time[sy] += dt[sy];
+  dt[sy] = d;
+  vmax[sy] = 0ull;
 }
 
 // Host-step layout conversion: io = [pos (n*3) | vel (n*3)] in the caller's
@@ -886,6 +947,23 @@ struct mdg_ctx {
   // one MD step captured as a CUDA graph (replayed when no per-step energies are wanted)
   cudaGraphExec_t step_graph = nullptr;
   double graph_dt = 0.0;
+  int graph_cfg = -1;           // step_cfg the graph was captured with
+  int step_cfg = 0;             // bumped when the thermal bath or the dt mode changes
+
+  // thermal bath (SimLoop::thermalBath*, SimLoop.hpp:96-191) and adaptive dt
+  // (SimLoop.cxx:405-416); internal units (K, 1/fs, Angstrom)
+  int tb_geom = 0;
+  double tb_T0 = 0.0, tb_gamma = 1e13 * 1e-15;  // ThermalBathCommon defaults (1e13 / s)
+  double tb_gp[5] = {0, 0, 0, 0, 0};
+  unsigned char* d_tb_apply = nullptr;  // [n] Atom::apply_ThermalBath (null: every atom)
+  double* d_tb_T = nullptr;             // [nsys] bath temperature at the step start
+  double* d_tb_part = nullptr;          // [2 * kBathBlocks (+ nsys)] partial sums
+  bool adaptive = false;
+  double timeaccel = 1.0;               // SimLoop::timeaccel (1 Angstrom)
+  double dt0 = 0.5;                     // starting time step of the adaptive mode (fs)
+  double* d_dt = nullptr;               // [nsys] current time step (adaptive dt)
+  double* d_time = nullptr;             // [nsys] simulated time since the mode was set
+  unsigned long long* d_vmax = nullptr; // [nsys] bits of the step's largest |v|
   cudaStream_t graph_stream = nullptr;
   int graph_launches = 0;
 
@@ -1020,6 +1098,14 @@ void adj_free(mdg_ctx* c);
 void free_system(mdg_ctx* c)
 {
   adj_free(c);
+  {
+    void* st[] = {c->d_tb_apply, c->d_tb_T, c->d_tb_part, c->d_dt, c->d_time, c->d_vmax};
+    for (void* p : st)
+      if (p) cudaFree(p);
+    c->d_tb_apply = nullptr;
+    c->d_tb_T = c->d_tb_part = c->d_dt = c->d_time = nullptr;
+    c->d_vmax = nullptr;
+  }
   void* ptrs[] = {c->pos, c->vel, c->acc, c->grad, c->image, c->fixed, c->mass,
                   c->bb.nb, c->bb.bj, c->bb.brev, c->bb.brv, c->bb.bu, c->bb.bd, c->bb.nco,
                   c->fo.A, c->fo.W, c->fo.gown, c->fo.glj, c->fo.e_rebo, c->fo.e_tors, c->fo.e_lj,
@@ -1202,14 +1288,24 @@ void prof_end(mdg_ctx* c);
   } while (0)
 
 // The displacement partials of both lists (after the step's position update
-// when step_dt is given) in one pass over the atoms.
+// when a step is given; before it, the bath temperature) in one pass over
+// the atoms.
 constexpr int kDispParts = 296;  // 2 blocks per SM of a B200
-int step_start(mdg_ctx* c, const double* step_dt)
+constexpr int kBathBlocks = 120;
+int step_start(mdg_ctx* c, const StepDev* step)
 {
   State S = c->S();
   const int nl = c->has_list[1] ? 2 : 1;
-  LAUNCH(c, step_dt ? "verlet_pos_disp" : "nl_disp_partial", k_step_start, kDispParts, kThreads, S,
-         step_dt ? *step_dt : 0.0, step_dt ? 1 : 0, c->nl[0], c->nl[1], nl, c->d_part);
+  if (step && step->tb_geom) {
+    const int bps = std::max(1, kBathBlocks / c->nsys);
+    LAUNCH(c, "bath_temp_partial", k_bath_partial, dim3(bps, c->nsys), kThreads, S, *step,
+           c->nsys > 1 ? c->d_first : nullptr, c->d_tb_part);
+    LAUNCH(c, "bath_temp_final", k_bath_final, nblk(c->nsys), kThreads, c->d_tb_part, bps, c->nsys, c->d_tb_T);
+  }
+  StepDev none;
+  std::memset(&none, 0, sizeof(none));
+  LAUNCH(c, step ? "verlet_pos_disp" : "nl_disp_partial", k_step_start, kDispParts, kThreads, S,
+         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], nl, c->d_part);
   return MDG_OK;
 }
 
@@ -1237,9 +1333,9 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
   return MDG_OK;
 }
 
-int rebuild_lists(mdg_ctx* c, const double* step_dt = nullptr)
+int rebuild_lists(mdg_ctx* c, const StepDev* step = nullptr)
 {
-  int rc = step_start(c, step_dt);
+  int rc = step_start(c, step);
   if (!rc) rc = rebuild_list(c, 0, c->stream);
   if (!rc) rc = rebuild_list(c, 1, c->stream);
   if (rc) return rc;
@@ -1247,10 +1343,11 @@ int rebuild_lists(mdg_ctx* c, const double* step_dt = nullptr)
 }
 
 // One force evaluation at the current positions; leaves dE/dx in c->grad and
-// per-atom energies in c->fo.  With step_dt, the evaluation is the body of a
+// per-atom energies in c->fo.  With a step, the evaluation is the body of a
 // velocity-Verlet step: the position update comes first (fused with the
-// displacement check) and the velocity update last (fused with the gather).
-int evaluate(mdg_ctx* c, const double* step_dt = nullptr)
+// displacement check) and the velocity update last (fused with the gather),
+// with the thermal bath and the adaptive dt when they are on.
+int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
 {
   State S = c->S();
   const int pot = c->prm.potentials;
@@ -1261,7 +1358,7 @@ int evaluate(mdg_ctx* c, const double* step_dt = nullptr)
   if (ovl) {
     // the LJ list's check/rebuild and the in-range filter (positions and the
     // LJ list only) on the third stream, beside the REBO list and the bonds
-    rc = step_start(c, step_dt);
+    rc = step_start(c, step);
     if (rc) return rc;
     CK(cudaEventRecord(c->ev_fork2, c->stream));
     CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
@@ -1273,7 +1370,7 @@ int evaluate(mdg_ctx* c, const double* step_dt = nullptr)
     rc = rebuild_list(c, 0, c->stream);
     if (rc) return rc;
   } else {
-    rc = rebuild_lists(c, step_dt);
+    rc = rebuild_lists(c, step);
     if (rc) return rc;
     if (lj)
       LAUNCH(c, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
@@ -1356,9 +1453,13 @@ int evaluate(mdg_ctx* c, const double* step_dt = nullptr)
   if (tasks || lj)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
-  if (step_dt)
+  if (step) {
     LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
-           *step_dt, c->e_kin, c->d_status);
+           *step, c->e_kin, c->d_status);
+    if (step->vmax)
+      LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_time,
+             c->timeaccel);
+  }
   else
     LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
   return launch_check(c);
@@ -1751,6 +1852,22 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     return fail(MDG_ERR_CUDA, "cudaHostAlloc (staging)");
   c->d_io = dalloc<double>(6 * (size_t)n);
   if (!c->d_io) return fail(MDG_ERR_CUDA, "cudaMalloc (host-step staging)");
+  // per-system step state: bath temperature, adaptive dt, time, v_max
+  c->d_tb_T = dalloc<double>(nsys);
+  c->d_tb_part = dalloc<double>(2 * (size_t)std::max(kBathBlocks, nsys));
+  c->d_dt = dalloc<double>(nsys);
+  c->d_time = dalloc<double>(nsys);
+  c->d_vmax = dalloc<unsigned long long>(nsys);
+  if (!c->d_tb_T || !c->d_tb_part || !c->d_dt || !c->d_time || !c->d_vmax)
+    return fail(MDG_ERR_CUDA, "cudaMalloc (step state)");
+  {
+    std::vector<double> dt0((size_t)nsys, c->dt0);
+    CK(cudaMemcpy(c->d_dt, dt0.data(), nsys * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->d_time, 0, nsys * sizeof(double)));
+    CK(cudaMemset(c->d_vmax, 0, nsys * sizeof(unsigned long long)));
+    CK(cudaMemset(c->d_tb_T, 0, nsys * sizeof(double)));
+  }
+  c->step_cfg++;
   CK(cudaDeviceSynchronize());
   return MDG_OK;
 }
@@ -1940,15 +2057,37 @@ static int autotune(mdg_ctx* c)
 
 // The captured step (position update, forces, velocity update) for time
 // step dtf on the context's stream, captured again when either changes.
+// The step descriptor of the context's current configuration (fixed dt dtf,
+// or the device's per-system dt when adaptive; the thermal bath when set).
+static StepDev step_dev(mdg_ctx* c, double dtf)
+{
+  StepDev P;
+  std::memset(&P, 0, sizeof(P));
+  P.dt = dtf;
+  P.d_dt = c->adaptive ? c->d_dt : nullptr;
+  P.tb_geom = c->tb_geom;
+  P.T0 = c->tb_T0;
+  P.gamma = c->tb_gamma;
+  for (int k = 0; k < 5; k++) P.gp[k] = c->tb_gp[k];
+  P.tb_apply = c->d_tb_apply;
+  P.tb_T = c->d_tb_T;
+  P.vmax = c->adaptive ? c->d_vmax : nullptr;
+  P.nlc0 = c->nl[0].cnt;
+  P.nlc1 = c->has_list[1] ? c->nl[1].cnt : nullptr;
+  return P;
+}
+
 static int ensure_step_graph(mdg_ctx* c, double dtf)
 {
-  if (c->step_graph && c->graph_dt == dtf && c->graph_stream == c->stream) return MDG_OK;
+  if (c->step_graph && c->graph_dt == dtf && c->graph_stream == c->stream && c->graph_cfg == c->step_cfg)
+    return MDG_OK;
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   c->step_graph = nullptr;
   cudaGraph_t g = nullptr;
   int64_t l0 = c->launches;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = evaluate(c, &dtf);
+  const StepDev sd = step_dev(c, dtf);
+  int rc = evaluate(c, &sd);
   cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
   c->graph_launches = (int)(c->launches - l0);
   c->launches = l0;
@@ -1959,6 +2098,7 @@ static int ensure_step_graph(mdg_ctx* c, double dtf)
   if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
   c->graph_dt = dtf;
   c->graph_stream = c->stream;
+  c->graph_cfg = c->step_cfg;
   return MDG_OK;
 }
 
@@ -1997,7 +2137,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
       CK(cudaGraphLaunch(c->step_graph, c->stream));
       c->launches += c->graph_launches;
     } else {
-      rc = evaluate(c, &dtf);  // position update, forces, velocity update
+      const StepDev sd = step_dev(c, dtf);
+      rc = evaluate(c, &sd);  // position update, forces, velocity update
       if (rc) return rc;
     }
     if (log) {
@@ -2052,7 +2193,8 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->elog_cap = need;
   }
   for (int s = 0; s < nsteps; s++) {
-    rc = evaluate(c, &dtf);  // position update, forces, velocity update
+    const StepDev sd = step_dev(c, dtf);
+    rc = evaluate(c, &sd);  // position update, forces, velocity update
     if (rc) return rc;
     rc = sys_energies(c, c->d_elog + (int64_t)s * c->nsys * 4);
     if (rc) return rc;
@@ -2090,6 +2232,82 @@ int mdg_batch_energies(mdg_ctx* c, double* e_sys)
   rc = read_status(c);
   if (rc) return rc;
   for (size_t q = 0; q < h.size(); q++) e_sys[q] = h[q] * c->unit_e;
+  return MDG_OK;
+}
+
+int mdg_set_thermal_bath(mdg_ctx* c, int geom, double T0, double gamma, const double* params, const uint8_t* apply)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  if (geom < MDG_TB_NONE || geom > MDG_TB_SPHERE) return fail(MDG_ERR_ARG, "unknown thermal bath geometry");
+  if (geom != MDG_TB_NONE) {
+    if (!(T0 >= 0.0) || !(gamma >= 0.0) || !std::isfinite(T0) || !std::isfinite(gamma))
+      return fail(MDG_ERR_ARG, "bath temperature and friction rate must be finite and non-negative");
+    if ((geom == MDG_TB_BOX || geom == MDG_TB_SPHERE) && !params) return fail(MDG_ERR_ARG, "null bath geometry");
+    if (apply && !c->n) return fail(MDG_ERR_STATE, "per-atom bath flags need a loaded system");
+    // the geometries' own REQUIREs (SimLoop.hpp:140, 166): a box bath needs
+    // lateral periodicity, a sphere bath none
+    for (const Box& b : c->h_boxes) {
+      if (geom == MDG_TB_BOX && !(b.pbc[0] && b.pbc[1]))
+        return fail(MDG_ERR_ARG, "a box thermal bath needs periodic x and y (ThermalBathGeomBox)");
+      if (geom == MDG_TB_SPHERE && (b.pbc[0] || b.pbc[1] || b.pbc[2]))
+        return fail(MDG_ERR_ARG, "a sphere thermal bath needs an open box (ThermalBathGeomSphere)");
+    }
+  }
+  const double tconv = (c->prm.units == MDG_UNITS_CGS) ? kFs : 1.0;  // 1/(time unit) -> 1/fs
+  c->tb_geom = geom;
+  c->tb_T0 = T0;
+  c->tb_gamma = gamma * tconv;
+  for (int k = 0; k < 5; k++) c->tb_gp[k] = 0.0;
+  if (geom == MDG_TB_BOX)
+    for (int k = 0; k < 3; k++) c->tb_gp[k] = params[k] * c->unit_len;
+  if (geom == MDG_TB_SPHERE)
+    for (int k = 0; k < 5; k++) c->tb_gp[k] = params[k] * c->unit_len;
+  if (c->d_tb_apply) cudaFree(c->d_tb_apply);
+  c->d_tb_apply = nullptr;
+  if (apply) {
+    c->d_tb_apply = dalloc<unsigned char>(c->n);
+    if (!c->d_tb_apply) return fail(MDG_ERR_CUDA, "cudaMalloc (bath flags)");
+    CK(cudaMemcpy(c->d_tb_apply, apply, c->n, cudaMemcpyHostToDevice));
+  }
+  c->step_cfg++;
+  return MDG_OK;
+}
+
+int mdg_set_adaptive_dt(mdg_ctx* c, int on, double timeaccel, double dt0)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  const double tconv = (c->prm.units == MDG_UNITS_CGS) ? 1.0 / kFs : 1.0;  // time unit -> fs
+  if (on && !(timeaccel > 0.0 && dt0 > 0.0 && std::isfinite(timeaccel) && std::isfinite(dt0)))
+    return fail(MDG_ERR_ARG, "timeaccel and the starting dt must be finite and positive");
+  c->adaptive = on != 0;
+  if (on) {
+    c->timeaccel = timeaccel * c->unit_len;
+    c->dt0 = std::min(std::max(dt0 * tconv, 1e-5), 0.5);
+    if (c->n) {
+      std::vector<double> d((size_t)c->nsys, c->dt0);
+      CK(cudaMemcpyAsync(c->d_dt, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemsetAsync(c->d_time, 0, c->nsys * sizeof(double), c->stream));
+      CK(cudaMemsetAsync(c->d_vmax, 0, c->nsys * sizeof(unsigned long long), c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+  }
+  c->step_cfg++;
+  return MDG_OK;
+}
+
+int mdg_get_time(mdg_ctx* c, double* sim_time, double* dt)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  std::vector<double> t((size_t)c->nsys), d((size_t)c->nsys);
+  CK(cudaMemcpyAsync(t.data(), c->d_time, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(d.data(), c->d_dt, d.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  int rc = read_status(c);
+  if (rc) return rc;
+  const double tconv = (c->prm.units == MDG_UNITS_CGS) ? kFs : 1.0;  // fs -> time unit
+  for (int s = 0; s < c->nsys; s++) {
+    if (sim_time) sim_time[s] = t[s] * tconv;
+    if (dt) dt[s] = d[s] * tconv;
+  }
   return MDG_OK;
 }
 

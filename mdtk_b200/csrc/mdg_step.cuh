@@ -503,6 +503,44 @@ MDG_HD void wrap_atom(State& S, int i, unsigned int* status)
   S.image[i] = im;
 }
 
+// Thermal bath and adaptive time step of the step body (SimLoop.cxx:280-287,
+// 352-388, 394-416; the bath geometries of SimLoop.hpp:96-191).  Times in fs,
+// lengths in Angstrom, the friction rate gamma in 1/fs.
+struct StepDev {
+  double dt;                      // fixed time step when d_dt is null
+  const double* d_dt;             // per-system time step (adaptive dt) or null
+  int tb_geom;                    // 0 none, 1 universe, 2 box, 3 sphere (SimLoop::TB_GEOM_*)
+  double T0, gamma;               // bath temperature (K), friction rate
+  double gp[5];                   // box: zMin, dBoundary, zMinOfFreeZone; sphere: cx, cy, cz, radius, zMinOfFreeZone
+  const unsigned char* tb_apply;  // per atom Atom::apply_ThermalBath (null: every atom)
+  const double* tb_T;             // per system: the bath temperature at the step start
+  unsigned long long* vmax;       // per system: bits of the largest |v| (adaptive dt), or null
+  const int* nlc0;                // list counts, FProxy::hasNeighbors (FProxy.hpp:99-105)
+  const int* nlc1;                // (null when there is no second list)
+};
+
+MDG_HD int sys_of(const State& S, int i) { return S.sys ? S.sys[i] : 0; }
+MDG_HD double step_dt(const StepDev& P, const State& S, int i) { return P.d_dt ? P.d_dt[sys_of(S, i)] : P.dt; }
+
+// SimLoop::thermalBathShouldBeApplied (SimLoop.hpp:164-191) at atom i's
+// current coordinates.
+MDG_HD bool in_bath(const StepDev& P, const State& S, int i)
+{
+  if (!P.tb_geom || (P.tb_apply && !P.tb_apply[i])) return false;
+  if (P.tb_geom == 1) return true;
+  const double4 x = S.pos[i];
+  if (P.tb_geom == 2) {
+    const Box& b = box_of(S, i);
+    const bool lateral = b.pbc[0] && b.pbc[1];
+    return (x.z > P.gp[0]) ||
+           (lateral && ((x.x < 0.0 + P.gp[1]) || (x.x > b.L[0] - P.gp[1]) || (x.y < 0.0 + P.gp[1]) ||
+                        (x.y > b.L[1] - P.gp[1])) &&
+            x.z > P.gp[2]);
+  }
+  const double dx = P.gp[0] - x.x, dy = P.gp[1] - x.y, dz = P.gp[2] - x.z;
+  return x.z > P.gp[4] && sqrt(dx * dx + dy * dy + dz * dz) > P.gp[3];
+}
+
 // eq 2-4 (SimLoop.cxx:339-399) without the thermal bath: v += a_old dt/2,
 // a = F/M, v += a dt/2; then applyPBC (SimLoop.cxx:401).
 MDG_HD void verlet_vel_atom(State& S, V3 grad, double dt, int i, unsigned int* status)
@@ -518,4 +556,40 @@ MDG_HD void verlet_vel_atom(State& S, V3 grad, double dt, int i, unsigned int* s
   wrap_atom(S, i, status);
 }
 
+// eq 2-4 with the thermal bath and the adaptive-dt maximum: a bath atom
+// feels dF = -V M gamma (1 - sqrt(T0/T)) with T0/T clamped to [-5, 5] (0 when
+// |T| < 1e-5), so a = F/M - gamma (1 - sqrt(T0/T)) v_n; |v_{n+1}| of free
+// atoms with neighbours enters the system's maximum (SimLoop.cxx:352-398).
+MDG_HD void verlet_vel_ext_atom(State& S, V3 grad, const StepDev& P, int i, unsigned int* status)
+{
+  if (!(S.fixed && S.fixed[i])) {
+    const double dt = step_dt(P, S, i);
+    double4 v = S.vel[i], ac = S.acc[i];
+    double m = S.mass[i];
+    V3 vdt2 = v3(v.x + ac.x * dt / 2.0, v.y + ac.y * dt / 2.0, v.z + ac.z * dt / 2.0);
+    V3 an = v3(-grad.x / m * kAccConv, -grad.y / m * kAccConv, -grad.z / m * kAccConv);
+    if (in_bath(P, S, i)) {
+      const double T = P.tb_T[sys_of(S, i)];
+      double r = (fabs(T) < 1e-5) ? 0.0 : P.T0 / T;
+      if (r < -5.0) r = -5.0;
+      if (r > 5.0) r = 5.0;
+      const double k = P.gamma * (1.0 - sqrt(r));
+      an = v3(an.x - v.x * k, an.y - v.y * k, an.z - v.z * k);
+    }
+    S.acc[i] = make_double4(an.x, an.y, an.z, 0.0);
+    const V3 vn = v3(vdt2.x + an.x * dt / 2.0, vdt2.y + an.y * dt / 2.0, vdt2.z + an.z * dt / 2.0);
+    S.vel[i] = make_double4(vn.x, vn.y, vn.z, 0.0);
+#if defined(__CUDA_ARCH__)
+    if (P.vmax && (P.nlc0[i] > 0 || (P.nlc1 && P.nlc1[i] > 0))) {
+      const double vm = sqrt(vn.x * vn.x + vn.y * vn.y + vn.z * vn.z);
+      // non-negative doubles order like their bit patterns: the maximum does
+      // not depend on the order of the atomics
+      atomicMax(P.vmax + sys_of(S, i), (unsigned long long)__double_as_longlong(vm));
+    }
+#endif
+  }
+  wrap_atom(S, i, status);
+}
+
 }  // namespace mdg
+

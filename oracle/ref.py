@@ -50,6 +50,10 @@ def lib():
         L.ref_nl_pairs.restype = ctypes.c_long
         L.ref_nl_pairs.argtypes = [vp, ctypes.c_int, ip, ctypes.c_long]
         L.ref_set_param.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.ref_set_bath.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp,
+                                   ctypes.POINTER(ctypes.c_ubyte)]
+        L.ref_set_adaptive.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.ref_last_run_dts.argtypes = [vp, dp, ctypes.c_int]
         L.ref_rcutoff.restype = ctypes.c_double
         L.ref_rcutoff.argtypes = [vp, ctypes.c_int]
         L.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, ip, dp, dp, dp]
@@ -131,6 +135,23 @@ class RefSystem:
         out = np.zeros((max(cnt, 1), 2), dtype=np.int32)
         _check(lib().ref_nl_pairs(self.h, index, _ip(out), cnt))
         return out[:cnt]
+
+    def set_bath(self, geom: int, T0: float, gamma_per_s: float, params=None, flags=None):
+        """SimLoop's thermal bath (geom 0 none, 1 universe, 2 box, 3 sphere)."""
+        self._bp = np.zeros(5) if params is None else np.ascontiguousarray(np.resize(params, 5), dtype=np.float64)
+        fl = None
+        if flags is not None:
+            self._bf = np.ascontiguousarray(flags, dtype=np.uint8)
+            fl = self._bf.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
+        _check(lib().ref_set_bath(self.h, geom, T0, gamma_per_s, _dp(self._bp), fl))
+
+    def set_adaptive(self, on: bool, timeaccel: float = 1.0, dt0: float = 0.5):
+        _check(lib().ref_set_adaptive(self.h, 1 if on else 0, timeaccel, dt0))
+
+    def last_run_dts(self, n: int) -> np.ndarray:
+        out = np.zeros(n)
+        lib().ref_last_run_dts(self.h, _dp(out), n)
+        return out
 
     def set_param(self, pid: int, value: float):
         """Override a C-C pair parameter (ids as include/mdg.h MDG_PARAM_*)."""

@@ -51,12 +51,15 @@ class FixedDtLoop : public SimLoop
 public:
   Float fixed_dt;
   Float ekin_before;
-  std::vector<double> epot_log, etot_log, t_log;
-  FixedDtLoop() : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0) {}
+  bool adaptive;  // leave dt to SimLoop's own adaptation (SimLoop.cxx:405-416)
+  int max_iter;   // adaptive runs stop after this many iterations
+  std::vector<double> epot_log, etot_log, t_log, dt_log;
+  FixedDtLoop() : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0), adaptive(false), max_iter(0) {}
   virtual void doBeforeIteration()
   {
     t_log.push_back(wall_now());
-    dt = fixed_dt;
+    if (!adaptive) dt = fixed_dt;
+    dt_log.push_back(dt / fs);
     ekin_before = energyKin();
   }
   virtual void doAfterIteration()
@@ -65,6 +68,7 @@ public:
     Float epot = check.currentEnergy - ekin_before;
     epot_log.push_back(epot / eV);
     etot_log.push_back((epot + energyKin()) / eV);
+    if (adaptive && (int)epot_log.size() >= max_iter) breakSimLoop = true;
   }
 };
 
@@ -74,13 +78,16 @@ struct RefCtx
   int potset;
   int brenner_set;
   int lj_cut_mode;
+  bool adaptive;
+  double dt0_fs;
   std::vector<std::string> names;
   REBO* rebo;
   AIREBO* lj;
   ETors* etors;
   Brenner* brenner;
   bool nl_ready;
-  RefCtx() : potset(0), brenner_set(1), lj_cut_mode(0), rebo(0), lj(0), etors(0), brenner(0), nl_ready(false) {}
+  RefCtx() : potset(0), brenner_set(1), lj_cut_mode(0), adaptive(false), dt0_fs(0.5), rebo(0), lj(0), etors(0),
+             brenner(0), nl_ready(false) {}
 };
 
 ElementID el_from_z(int z)
@@ -288,6 +295,52 @@ long ref_nl_pairs(void* h, int index, int* pairs, long cap)
   }
 }
 
+/* SimLoop's thermal bath (SimLoop.hpp:96-191): geom 0 none, 1 universe,
+ * 2 box (params zMin, dBoundary, zMinOfFreeZone), 3 sphere (params cx, cy, cz,
+ * radius, zMinOfFreeZone); lengths in Angstrom, T0 in K, gamma in 1/s;
+ * flags: NULL or per-atom Atom::apply_ThermalBath (after ref_set_atoms). */
+int ref_set_bath(void* h, int geom, double T0, double gamma, const double* params, const unsigned char* flags)
+{
+  RefCtx* c = (RefCtx*)h;
+  SimLoop& L = c->loop;
+  L.thermalBathGeomType = (SimLoop::TB_GEOM_TYPE)geom;
+  L.thermalBathCommon.To = T0;
+  L.thermalBathCommon.gamma = gamma;
+  if (geom == 2) {
+    L.thermalBathGeomBox.zMin = params[0] * Ao;
+    L.thermalBathGeomBox.dBoundary = params[1] * Ao;
+    L.thermalBathGeomBox.zMinOfFreeZone = params[2] * Ao;
+  }
+  if (geom == 3) {
+    L.thermalBathGeomSphere.center = Vector3D(params[0] * Ao, params[1] * Ao, params[2] * Ao);
+    L.thermalBathGeomSphere.radius = params[3] * Ao;
+    L.thermalBathGeomSphere.zMinOfFreeZone = params[4] * Ao;
+  }
+  if (flags)
+    for (size_t i = 0; i < L.atoms.size(); i++) L.atoms[i].apply_ThermalBath = flags[i] != 0;
+  return 0;
+}
+
+/* Leave dt to SimLoop's adaptation (SimLoop.cxx:405-416) in ref_run, starting
+ * from dt0 (fs), with timeaccel in Angstrom; off = the fixed dt of ref_run. */
+int ref_set_adaptive(void* h, int on, double timeaccel, double dt0)
+{
+  RefCtx* c = (RefCtx*)h;
+  c->adaptive = on != 0;
+  c->dt0_fs = dt0;
+  c->loop.timeaccel = timeaccel * Ao;
+  return 0;
+}
+
+/* Per-iteration dt (fs) of the last ref_run. */
+int ref_last_run_dts(void* h, double* out, int cap)
+{
+  FixedDtLoop& L = ((RefCtx*)h)->loop;
+  int n = (int)L.dt_log.size();
+  for (int i = 0; i < n && i < cap; i++) out[i] = L.dt_log[i];
+  return n;
+}
+
 /* Override one C-C pair parameter (Angstrom / eV) of the potentials in place,
  * re-deriving what AIREBO::setupPotential derives from it
  * (AIREBO_LJ.cxx:229-262): id 0 = AIREBO zeta_[C][C], 1 = AIREBO
@@ -354,10 +407,18 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
     L.simTime = 0.0;
     L.iteration = 0;
     L.simTimeFinal = dt_fs * fs * (nsteps - 0.5);
+    L.adaptive = c->adaptive;
+    if (c->adaptive) {
+      L.dt = c->dt0_fs * fs;
+      L.simTimeFinal = 1e9 * ps;
+      L.max_iter = nsteps;
+      L.breakSimLoop = false;
+    }
     L.simTimeSaveTrajInterval = 1e9 * ps;
     L.epot_log.clear();
     L.etot_log.clear();
     L.t_log.clear();
+    L.dt_log.clear();
     double t_start = wall_now();
     int rc = L.execute();
     L.t_log.insert(L.t_log.begin(), t_start);
