@@ -39,6 +39,7 @@ typedef struct mdg_ctx mdg_ctx;
 #define MDG_ERR_SPLINE_DOMAIN (-9)  /* spline argument out of its domain (cubici.hpp:90,211,305) */
 #define MDG_ERR_STATE (-10)         /* call out of order (e.g. compute before set_system) */
 #define MDG_ERR_TIMEOUT (-11)       /* a bounded device wait gave up */
+#define MDG_ERR_IO (-12)            /* a checkpoint or trajectory file could not be read or written */
 
 /* ---- potential selection (bitmask) ---- */
 #define MDG_POT_REBO 1        /* REBO (AIREBO/REBO.cxx) */
@@ -271,6 +272,74 @@ int mdg_set_adaptive_dt(mdg_ctx* ctx, int on, double timeaccel, double dt0);
 /* Simulated time and current dt per system ([nsys] each; time counts the
  * adaptive steps since mdg_set_adaptive_dt). */
 int mdg_get_time(mdg_ctx* ctx, double* sim_time, double* dt);
+
+/* ---- Checkpoint and trajectory files ----
+ * SimLoopSaver's state files (SimLoopSaver.cxx:118-231 write, 275-625 load):
+ * "<id>.z", ".r", ".v", ".pbc_rect", ".pbc_rect.count", ".pbc_rect.enabled",
+ * ".a", ".indices", ".tag.*", ".thermal_bath.*", ".time", ".check", raw
+ * host-order records in the reference's CGS units; and the XVA text frames of
+ * SimLoop::saveToStreamXVA (SimLoop.cxx:680-748).  Files are written from a
+ * device snapshot by a writer thread while the steps go on; compression as
+ * yaatk::Stream (plain, .gz, .xz; reading also finds .bz2). */
+#define MDG_ZIP_NONE 0
+#define MDG_ZIP_GZIP 1  /* "<file>.gz" (yaatk's gzip_internal) */
+#define MDG_ZIP_XZ 2    /* "<file>.xz" through the xz program (yaatk's first choice) */
+
+/* SimLoopSaver::LOADED_* bits returned by mdg_load_state (SimLoopSaver.hpp:56-71) */
+#define MDG_LOADED_Z 1
+#define MDG_LOADED_R 2
+#define MDG_LOADED_V 4
+#define MDG_LOADED_PBC_RECT 8
+#define MDG_LOADED_PBC_COUNT 16
+#define MDG_LOADED_PBC_ENABLED 32
+#define MDG_LOADED_A 64
+
+/* Per-atom tag bits (Atom::tag, ATOMTAG_TARGET .. ATOMTAG_FULLERENE = bits
+ * 1..6, Atom.hpp:84-90) written to and read from the ".tag.*" files; NULL
+ * clears them.  They do not change the dynamics. */
+int mdg_set_atom_tags(mdg_ctx* ctx, const uint8_t* tags);
+int mdg_get_atom_tags(mdg_ctx* ctx, uint8_t* tags);
+
+/* SimLoopSaver::write(id) for system sys (0 for a single-system context):
+ * returns when the files are written.  The Check record holds the net force
+ * at the current positions, the kinetic energy before the last kick plus the
+ * potential energy, the initial energy of iteration 0 and the energy the
+ * bath has given (SimLoop.cxx:337-385, 1133-1153). */
+int mdg_write_state(mdg_ctx* ctx, int sys, const char* id, int zip);
+
+/* SimLoop::saveToStreamXVA of system sys into path (+ the compression's
+ * extension); returns when the file is written. */
+int mdg_write_xva(mdg_ctx* ctx, int sys, const char* path, int zip);
+
+/* SimLoopSaver::loadIteration: SimLoopSaver::load(id) into this context (it
+ * replaces the loaded system; one system) and SimLoop::iteration = iteration.
+ * Needs the Z numbers and positions; the other files are optional, as in the
+ * reference.  A loaded ".a" is kept (no new initial accelerations) unless
+ * iteration is 0.  *loaded (may be NULL) gets the MDG_LOADED_* bits. */
+int mdg_load_state(mdg_ctx* ctx, const char* id, uint64_t iteration, int* loaded);
+
+/* SimLoop::executeMain's output inside mdg_run / mdg_batch_run
+ * (SimLoop.cxx:263-277): at the top of each iteration, the state files
+ * "<dir>/md%010lu" (SimLoopSaver::generateId) every flush_interval
+ * iterations except iteration 0 (0 = never), and an XVA frame
+ * "<dir>/mde%010lu.xva" at iteration 0 and whenever the simulated time has
+ * crossed a multiple of traj_interval (time units; 0 = never).  Batched
+ * contexts write system s under "<dir>/sys%05d".  dir NULL stops the output.
+ * With adaptive dt and traj_interval > 0 each step reads its time back. */
+int mdg_set_output(mdg_ctx* ctx, const char* dir, int64_t flush_interval, double traj_interval, int zip);
+
+/* Wait for the files queued so far; reports the first write error. */
+int mdg_flush_output(mdg_ctx* ctx);
+
+/* SimLoop::iteration: steps taken since the system was loaded (or the
+ * iteration given to mdg_load_state). */
+int mdg_get_iteration(mdg_ctx* ctx, uint64_t* iteration);
+
+/* Number of atoms loaded (AtomsArray::size), 0 before a system is set. */
+int mdg_atom_count(mdg_ctx* ctx, int* n);
+
+/* SimLoop::simTimeFinal as stored in the ".time" file (time units; default 4 ps). */
+int mdg_set_time_final(mdg_ctx* ctx, double time_final);
 
 /* The launch configuration the autotuner chose (task_mode 0): overlap = 1
  * when the REBO tasks run on a second stream concurrently with the LJ

@@ -39,6 +39,13 @@ PARAM_NAMES = ("eps_CC", "sigma_CC", "A_CC", "B1_CC", "alpha_CC", "beta1_CC")
 
 TB_NONE, TB_UNIVERSE, TB_BOX, TB_SPHERE = 0, 1, 2, 3
 
+# checkpoint and trajectory files (include/mdg.h MDG_ZIP_*, MDG_LOADED_*)
+ZIP_NONE, ZIP_GZIP, ZIP_XZ = 0, 1, 2
+LOADED_Z, LOADED_R, LOADED_V = 1, 2, 4
+LOADED_PBC_RECT, LOADED_PBC_COUNT, LOADED_PBC_ENABLED, LOADED_A = 8, 16, 32, 64
+# Atom tag bits (Atom.hpp:84-90)
+TAG_TARGET, TAG_PROJECTILE, TAG_SUBSTRATE, TAG_MONOMER, TAG_CLUSTER, TAG_FULLERENE = (1 << k for k in range(1, 7))
+
 UNITS_AEVFS = 0
 UNITS_CGS = 1
 PREC_FP64 = 0
@@ -125,6 +132,17 @@ def lib():
         L.mdg_adjoint_backward.argtypes = [vp, dp, dp, ctypes.c_double, dp, dp, dp]
         L.mdg_debug_rebo_tables.argtypes = [dp, ctypes.c_int64]
         L.mdg_debug_rebo_tables.restype = ctypes.c_int64
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        L.mdg_set_atom_tags.argtypes = [vp, u8p]
+        L.mdg_get_atom_tags.argtypes = [vp, u8p]
+        L.mdg_write_state.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.mdg_write_xva.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.mdg_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]
+        L.mdg_set_output.argtypes = [vp, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int]
+        L.mdg_flush_output.argtypes = [vp]
+        L.mdg_get_iteration.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.mdg_set_time_final.argtypes = [vp, ctypes.c_double]
+        L.mdg_atom_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
     return _lib
 
@@ -269,6 +287,55 @@ class Context:
         d = np.zeros(ns)
         _check(lib().mdg_get_time(self.h, _dp(t), _dp(d)))
         return t, d
+
+    # ---- checkpoint and trajectory files (SimLoopSaver, SimLoop::saveToStreamXVA)
+
+    def set_atom_tags(self, tags=None):
+        """Per-atom TAG_* bits carried into the '.tag.*' state files."""
+        t = None if tags is None else np.ascontiguousarray(tags, dtype=np.uint8)
+        _check(lib().mdg_set_atom_tags(self.h, None if t is None else t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def get_atom_tags(self) -> np.ndarray:
+        t = np.zeros(self.n, np.uint8)
+        _check(lib().mdg_get_atom_tags(self.h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return t
+
+    def write_state(self, id: str, zip: int = ZIP_NONE, sys: int = 0):
+        """SimLoopSaver::write(id): the state files '<id>.<attribute>'."""
+        _check(lib().mdg_write_state(self.h, sys, os.fsencode(id), zip))
+
+    def write_xva(self, path: str, zip: int = ZIP_NONE, sys: int = 0):
+        """SimLoop::saveToStreamXVA into path."""
+        _check(lib().mdg_write_xva(self.h, sys, os.fsencode(path), zip))
+
+    def load_state(self, id: str, iteration: int = 0) -> int:
+        """SimLoopSaver::loadIteration: loads '<id>.*' as this context's
+        system at the given iteration; returns the LOADED_* bits."""
+        got = ctypes.c_int()
+        _check(lib().mdg_load_state(self.h, os.fsencode(id), int(iteration), ctypes.byref(got)))
+        n = ctypes.c_int()
+        _check(lib().mdg_atom_count(self.h, ctypes.byref(n)))
+        self.n = n.value
+        self.nsys = 1
+        return got.value
+
+    def set_output(self, dir, flush_interval: int = 0, traj_interval: float = 0.0, zip: int = ZIP_NONE):
+        """SimLoop::executeMain's file output inside run(): state files every
+        flush_interval iterations, XVA frames every traj_interval of time;
+        dir None stops it."""
+        _check(lib().mdg_set_output(self.h, None if dir is None else os.fsencode(dir), int(flush_interval),
+                                    float(traj_interval), zip))
+
+    def flush_output(self):
+        _check(lib().mdg_flush_output(self.h))
+
+    def iteration(self) -> int:
+        it = ctypes.c_uint64()
+        _check(lib().mdg_get_iteration(self.h, ctypes.byref(it)))
+        return it.value
+
+    def set_time_final(self, t: float):
+        _check(lib().mdg_set_time_final(self.h, float(t)))
 
     def tuned_launch(self):
         """(overlap, rebo_blocks): the autotuner's launch choice."""

@@ -566,7 +566,7 @@ int mdg_adjoint_forward(mdg_ctx* c, int nsteps, double dt, int every, double* po
   }
   // a_0 = A(x_0): the accelerations are a function of the initial positions
   State S = c->S();
-  LAUNCH(c, "init_acc", k_init_acc, nblk(n), kThreads, S, c->grad);
+  LAUNCH(c, "init_acc", k_init_acc, nblk(n), kThreads, S, c->grad, nullptr, nullptr);
   c->acc_valid = true;
   rc = adj_save(c, 0);
   for (int s = 1; s <= nsteps && !rc; s++) {

@@ -647,6 +647,10 @@ __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk
   V3 g = gather_atom(B, O, a, with_lj, nullptr);
   if (with_lj) g += mid_gather_atom(B, Tk, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
+  if (P.ekin_pre) {
+    const double4 v0 = S.vel[a];
+    P.ekin_pre[a] = S.mass[a] * (v0.x * v0.x + v0.y * v0.y + v0.z * v0.z) / 2.0 / kAccConv;
+  }
   verlet_vel_ext_atom(S, g, P, a, status);
   const double4 v = S.vel[a];
   ekin[a] = S.mass[a] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0 / kAccConv;
@@ -699,7 +703,8 @@ __global__ void k_bath_final(const double* part, int nblk_sys, int nsys, double*
 // End of a step with adaptive dt (SimLoop.cxx:405-416): the simulated time
 // advances by the step's dt, then dt = 0.05 timeaccel / v_max clamped to
 // [1e-5, 0.5] fs (0.5 fs without a moving atom).
-__global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, double* time, double timeaccel)
+__global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, double* dt_prev, double* time,
+                            double timeaccel)
 {
   const int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= nsys) return;
@@ -709,6 +714,7 @@ __global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, doub
   if (d > dt_max) d = dt_max;
   if (d < dt_min) d = dt_min;
   time[sy] += dt[sy];
+  dt_prev[sy] = dt[sy];
   dt[sy] = d;
   vmax[sy] = 0ull;
 }
@@ -736,14 +742,17 @@ __global__ void k_state_pack(State S, double* io, double ul, double uv)
 }
 
 // initial accelerations (SimLoop.cxx:305-321)
-__global__ void k_init_acc(State S, const double4* grad)
+// (and Atom::an_no_tb, Check::energyTransferredFromBath = 0, SimLoop.cxx:1137)
+__global__ void k_init_acc(State S, const double4* grad, double4* acc_ntb, double* eb)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
+  if (eb) eb[i] = 0.0;
   if (S.fixed && S.fixed[i]) return;
   double m = S.mass[i];
   double4 g = grad[i];
   S.acc[i] = make_double4(-g.x / m * kAccConv, -g.y / m * kAccConv, -g.z / m * kAccConv, 0.0);
+  if (acc_ntb) acc_ntb[i] = S.acc[i];
 }
 
 __global__ void k_ekin(State S, double* ekin)
@@ -789,12 +798,13 @@ __global__ void k_reduce_final(const double* part, int nparts, int narr, double*
 // Per-system energy sums of a batched context: one block per system; each
 // thread sums a strided share of the system's atoms, then a fixed tree
 // (deterministic).  out[4 s + {0,1,2,3}] = REBO, LJ, torsion, kinetic.
-__global__ void k_sys_energy(const int64_t* first, const double* er, const double* el, const double* et,
+__global__ void k_sys_energy(const int64_t* first, int64_t n, const double* er, const double* el, const double* et,
                              const double* ek, double* out, unsigned int* status)
 {
   __shared__ double sh[4][kThreads];
   const int sy = blockIdx.x;
-  const int64_t b = first[sy], e = first[sy + 1];
+  // a single-system context has no offsets array: its one system is [0, n)
+  const int64_t b = first ? first[sy] : 0, e = first ? first[sy + 1] : n;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
     acc[0] += er[i];
@@ -964,8 +974,31 @@ struct mdg_ctx {
   double* d_dt = nullptr;               // [nsys] current time step (adaptive dt)
   double* d_time = nullptr;             // [nsys] simulated time since the mode was set
   unsigned long long* d_vmax = nullptr; // [nsys] bits of the step's largest |v|
+  double* d_dt_prev = nullptr;          // [nsys] the step just taken (SimLoop::dt_prev)
   cudaStream_t graph_stream = nullptr;
   int graph_launches = 0;
+
+  // SimLoop bookkeeping kept for the checkpoint and trajectory files
+  // (SimLoopSaver, SimLoop::saveToStreamXVA): the iteration counter, the time
+  // of fixed-dt steps (adaptive steps keep theirs on the device), the Check
+  // record's inputs
+  uint64_t iteration = 0;               // SimLoop::iteration
+  double time_s = 0.0;                  // SimLoop::simTime (s) of fixed-dt steps
+  double dt_s = 1e-20, dt_prev_s = 1e-20;  // SimLoop::dt, dt_prev (s) of fixed-dt steps
+  double time_final_s = 4e-12;          // SimLoop::simTimeFinal (SimLoop.cxx:48)
+  bool stepped = false;                 // a step ran since the state was set or loaded
+  bool e0_dev = false;                  // Check::initialEnergy is d_e0 (else chk_e0)
+  double chk_e0 = 1.0, chk_eb0 = 0.0;   // Check::initialEnergy, energyTransferredFromBath (erg) of a load
+  bool chk_loaded = false;              // a loaded Check record stands until the next step
+  double chk_net[3] = {0, 0, 0}, chk_cur = 1.0, chk_T = 0.0;
+  double run_t0 = 0.0;                  // wall clock at the first step (SimLoop::CPUTimeUsed_total's start)
+  double* d_e0 = nullptr;               // [nsys * 4] rebo, lj, tors, kin at the first step
+  double* d_ekin_pre = nullptr;         // [n] M V_n^2 / 2 before the last kick
+  double4* acc_ntb = nullptr;           // [n] Atom::an_no_tb (with a bath)
+  double* d_eb = nullptr;               // [n] energy the bath gave each atom (with a bath)
+  std::vector<int32_t> h_z;             // atomic numbers as loaded
+  std::vector<unsigned char> h_fixed, h_tb_apply, h_tags;  // Atom::fixed, apply_ThermalBath, tag bits
+  struct IoState* io = nullptr;         // snapshot slots, writer thread, output schedule
 
   // profiling: event pairs bracketing each launch while enabled
   bool prof = false;
@@ -1094,17 +1127,27 @@ int status_to_code(unsigned int st, std::string& msg)
 }
 
 void adj_free(mdg_ctx* c);
+void io_release(mdg_ctx* c);
+void io_free(mdg_ctx* c);
 
 void free_system(mdg_ctx* c)
 {
+  io_release(c);
   adj_free(c);
   {
-    void* st[] = {c->d_tb_apply, c->d_tb_T, c->d_tb_part, c->d_dt, c->d_time, c->d_vmax};
+    void* st[] = {c->d_tb_apply, c->d_tb_T, c->d_tb_part, c->d_dt, c->d_time, c->d_vmax, c->d_dt_prev,
+                  c->d_e0, c->d_ekin_pre, c->acc_ntb, c->d_eb};
     for (void* p : st)
       if (p) cudaFree(p);
     c->d_tb_apply = nullptr;
-    c->d_tb_T = c->d_tb_part = c->d_dt = c->d_time = nullptr;
+    c->d_tb_T = c->d_tb_part = c->d_dt = c->d_time = c->d_dt_prev = nullptr;
+    c->d_e0 = c->d_ekin_pre = c->d_eb = nullptr;
+    c->acc_ntb = nullptr;
     c->d_vmax = nullptr;
+    c->h_z.clear();
+    c->h_fixed.clear();
+    c->h_tb_apply.clear();
+    c->h_tags.clear();
   }
   void* ptrs[] = {c->pos, c->vel, c->acc, c->grad, c->image, c->fixed, c->mass,
                   c->bb.nb, c->bb.bj, c->bb.brev, c->bb.brv, c->bb.bu, c->bb.bd, c->bb.nco,
@@ -1457,7 +1500,7 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
            *step, c->e_kin, c->d_status);
     if (step->vmax)
-      LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_time,
+      LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_dt_prev, c->d_time,
              c->timeaccel);
   }
   else
@@ -1615,6 +1658,7 @@ int mdg_destroy(mdg_ctx* c)
 {
   if (!c) return MDG_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  io_free(c);
   free_system(c);
   void* ptrs[] = {c->d_tables, c->d_tables32, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy};
   for (void* p : ptrs)
@@ -1635,6 +1679,21 @@ int mdg_set_stream(mdg_ctx* c, void* stream)
 {
   if (!c) return fail(MDG_ERR_ARG, "null context");
   c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return MDG_OK;
+}
+
+// Per-atom bath bookkeeping (Atom::an_no_tb and the energy the bath gave
+// each atom, SimLoop.cxx:362-385), allocated with the first bath; an_no_tb
+// starts as the current an.
+static int ensure_bath_acct(mdg_ctx* c)
+{
+  if (!c->n || c->acc_ntb) return MDG_OK;
+  c->acc_ntb = dalloc<double4>(c->n);
+  c->d_eb = dalloc<double>(c->n);
+  if (!c->acc_ntb || !c->d_eb) return fail(MDG_ERR_CUDA, "cudaMalloc (bath bookkeeping)");
+  CK(cudaMemcpyAsync(c->acc_ntb, c->acc, c->n * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_eb, 0, c->n * sizeof(double), c->stream));
+  c->step_cfg++;
   return MDG_OK;
 }
 
@@ -1856,16 +1915,40 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   c->d_tb_T = dalloc<double>(nsys);
   c->d_tb_part = dalloc<double>(2 * (size_t)std::max(kBathBlocks, nsys));
   c->d_dt = dalloc<double>(nsys);
+  c->d_dt_prev = dalloc<double>(nsys);
   c->d_time = dalloc<double>(nsys);
   c->d_vmax = dalloc<unsigned long long>(nsys);
-  if (!c->d_tb_T || !c->d_tb_part || !c->d_dt || !c->d_time || !c->d_vmax)
+  c->d_e0 = dalloc<double>(4 * (size_t)nsys);
+  c->d_ekin_pre = dalloc<double>(n);
+  if (!c->d_tb_T || !c->d_tb_part || !c->d_dt || !c->d_dt_prev || !c->d_time || !c->d_vmax || !c->d_e0 ||
+      !c->d_ekin_pre)
     return fail(MDG_ERR_CUDA, "cudaMalloc (step state)");
+  CK(cudaMemset(c->d_ekin_pre, 0, n * sizeof(double)));
+  CK(cudaMemset(c->d_e0, 0, 4 * (size_t)nsys * sizeof(double)));
+  c->h_z.assign(z, z + n);
+  c->h_fixed = hf;
+  c->h_tags.assign(n, 0);
+  c->iteration = 0;
+  c->time_s = 0.0;
+  c->dt_s = c->dt_prev_s = 1e-20;
+  c->stepped = c->e0_dev = c->chk_loaded = false;
+  c->chk_e0 = 1.0;
+  c->chk_eb0 = 0.0;
+  c->chk_net[0] = c->chk_net[1] = c->chk_net[2] = 0.0;  // Check::Check (SimLoop.cxx:1280-1286)
+  c->chk_cur = 1.0;
+  c->chk_T = 0.0;
+  c->run_t0 = 0.0;
   {
     std::vector<double> dt0((size_t)nsys, c->dt0);
     CK(cudaMemcpy(c->d_dt, dt0.data(), nsys * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_dt_prev, dt0.data(), nsys * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemset(c->d_time, 0, nsys * sizeof(double)));
     CK(cudaMemset(c->d_vmax, 0, nsys * sizeof(unsigned long long)));
     CK(cudaMemset(c->d_tb_T, 0, nsys * sizeof(double)));
+  }
+  if (c->tb_geom) {
+    int rc = ensure_bath_acct(c);
+    if (rc) return rc;
   }
   c->step_cfg++;
   CK(cudaDeviceSynchronize());
@@ -2074,6 +2157,9 @@ static StepDev step_dev(mdg_ctx* c, double dtf)
   P.vmax = c->adaptive ? c->d_vmax : nullptr;
   P.nlc0 = c->nl[0].cnt;
   P.nlc1 = c->has_list[1] ? c->nl[1].cnt : nullptr;
+  P.ekin_pre = c->d_ekin_pre;
+  P.acc_ntb = c->tb_geom ? c->acc_ntb : nullptr;
+  P.eb = c->tb_geom ? c->d_eb : nullptr;
   return P;
 }
 
@@ -2102,20 +2188,43 @@ static int ensure_step_graph(mdg_ctx* c, double dtf)
   return MDG_OK;
 }
 
+int sys_energies(mdg_ctx* c, double* out_dev);
+// checkpoint and trajectory output around the steps (defined with the file formats)
+int io_run_start(mdg_ctx* c, double dtf);
+int io_before_step(mdg_ctx* c);
+int io_after_step(mdg_ctx* c);
+
+// The first step's accelerations, and at iteration 0 the Check record's
+// initial energy and the bath's energy count (SimLoop.cxx:305-321, 1133-1137).
+static int init_first_step(mdg_ctx* c)
+{
+  if (c->acc_valid) return MDG_OK;
+  int rc = evaluate(c);
+  if (rc) return rc;
+  State S = c->S();
+  const bool first = c->iteration == 0;
+  LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad, c->acc_ntb, first ? c->d_eb : nullptr);
+  if (first) {
+    LAUNCH(c, "ekin", k_ekin, nblk(c->n), kThreads, S, c->e_kin);
+    rc = sys_energies(c, c->d_e0);
+    if (rc) return rc;
+    c->e0_dev = true;
+    c->chk_eb0 = 0.0;
+  }
+  c->acc_valid = true;
+  return MDG_OK;
+}
+
 int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
   const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
-  State S = c->S();
-  int rc;
-  if (!c->acc_valid) {
-    rc = evaluate(c);
-    if (rc) return rc;
-    LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
-    c->acc_valid = true;
-  }
+  int rc = init_first_step(c);
+  if (rc) return rc;
   rc = autotune(c);
+  if (rc) return rc;
+  rc = io_run_start(c, dtf);
   if (rc) return rc;
   const bool log = epot || etot;
   if (log && c->elog_cap < (int64_t)nsteps * 4) {
@@ -2133,6 +2242,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     if (rc) return rc;
   }
   for (int s = 0; s < nsteps; s++) {
+    rc = io_before_step(c);  // scheduled state and trajectory files (SimLoop.cxx:263-277)
+    if (rc) return rc;
     if (graph) {
       CK(cudaGraphLaunch(c->step_graph, c->stream));
       c->launches += c->graph_launches;
@@ -2141,6 +2252,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
       rc = evaluate(c, &sd);  // position update, forces, velocity update
       if (rc) return rc;
     }
+    rc = io_after_step(c);
+    if (rc) return rc;
     if (log) {
       rc = reduce_energies(c, c->d_elog, 4, s, true);
       if (rc) return rc;
@@ -2163,7 +2276,7 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
 
 int sys_energies(mdg_ctx* c, double* out_dev)
 {
-  LAUNCH(c, "sys_energy", k_sys_energy, c->nsys, kThreads, c->d_first ? c->d_first : nullptr, c->fo.e_rebo,
+  LAUNCH(c, "sys_energy", k_sys_energy, c->nsys, kThreads, c->d_first ? c->d_first : nullptr, (int64_t)c->n, c->fo.e_rebo,
          c->fo.e_lj, c->fo.e_tors, c->e_kin, out_dev, c->d_status);
   return launch_check(c);
 }
@@ -2175,15 +2288,11 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
   if (!epot && !etot) return mdg_run(c, nsteps, dt, nullptr, nullptr);
   const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
-  State S = c->S();
-  int rc;
-  if (!c->acc_valid) {
-    rc = evaluate(c);
-    if (rc) return rc;
-    LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad);
-    c->acc_valid = true;
-  }
+  int rc = init_first_step(c);
+  if (rc) return rc;
   rc = autotune(c);
+  if (rc) return rc;
+  rc = io_run_start(c, dtf);
   if (rc) return rc;
   const int64_t need = (int64_t)nsteps * c->nsys * 4;
   if (c->elog_cap < need) {
@@ -2193,8 +2302,12 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     c->elog_cap = need;
   }
   for (int s = 0; s < nsteps; s++) {
+    rc = io_before_step(c);
+    if (rc) return rc;
     const StepDev sd = step_dev(c, dtf);
     rc = evaluate(c, &sd);  // position update, forces, velocity update
+    if (rc) return rc;
+    rc = io_after_step(c);
     if (rc) return rc;
     rc = sys_energies(c, c->d_elog + (int64_t)s * c->nsys * 4);
     if (rc) return rc;
@@ -2264,10 +2377,16 @@ int mdg_set_thermal_bath(mdg_ctx* c, int geom, double T0, double gamma, const do
     for (int k = 0; k < 5; k++) c->tb_gp[k] = params[k] * c->unit_len;
   if (c->d_tb_apply) cudaFree(c->d_tb_apply);
   c->d_tb_apply = nullptr;
+  c->h_tb_apply.clear();
   if (apply) {
     c->d_tb_apply = dalloc<unsigned char>(c->n);
     if (!c->d_tb_apply) return fail(MDG_ERR_CUDA, "cudaMalloc (bath flags)");
     CK(cudaMemcpy(c->d_tb_apply, apply, c->n, cudaMemcpyHostToDevice));
+    c->h_tb_apply.assign(apply, apply + c->n);
+  }
+  if (geom != MDG_TB_NONE) {
+    int rc = ensure_bath_acct(c);
+    if (rc) return rc;
   }
   c->step_cfg++;
   return MDG_OK;
@@ -2286,6 +2405,7 @@ int mdg_set_adaptive_dt(mdg_ctx* c, int on, double timeaccel, double dt0)
     if (c->n) {
       std::vector<double> d((size_t)c->nsys, c->dt0);
       CK(cudaMemcpyAsync(c->d_dt, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->d_dt_prev, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
       CK(cudaMemsetAsync(c->d_time, 0, c->nsys * sizeof(double), c->stream));
       CK(cudaMemsetAsync(c->d_vmax, 0, c->nsys * sizeof(unsigned long long), c->stream));
       CK(cudaStreamSynchronize(c->stream));
@@ -2515,3 +2635,5 @@ int mdg_debug_spline(int precision, int kind, int fam, int n, const double* args
 }
 
 }  // extern "C"
+
+#include "mdg_io.cuh"

@@ -517,6 +517,11 @@ struct StepDev {
   unsigned long long* vmax;       // per system: bits of the largest |v| (adaptive dt), or null
   const int* nlc0;                // list counts, FProxy::hasNeighbors (FProxy.hpp:99-105)
   const int* nlc1;                // (null when there is no second list)
+  double* ekin_pre;               // per atom M V_n^2 / 2 before the kick (SimLoop::energyKin at
+                                  // doEnergyConservationCheck, SimLoop.cxx:337), or null
+  double4* acc_ntb;               // per atom Atom::an_no_tb, updated in the bath branch only
+  double* eb;                     // per atom running sum of Check::energyTransferredFromBath
+                                  // (SimLoop.cxx:362-385); both null without a bath
 };
 
 MDG_HD int sys_of(const State& S, int i) { return S.sys ? S.sys[i] : 0; }
@@ -574,7 +579,20 @@ MDG_HD void verlet_vel_ext_atom(State& S, V3 grad, const StepDev& P, int i, unsi
       if (r < -5.0) r = -5.0;
       if (r > 5.0) r = 5.0;
       const double k = P.gamma * (1.0 - sqrt(r));
+      const V3 an_ntb = an;
       an = v3(an.x - v.x * k, an.y - v.y * k, an.z - v.z * k);
+      if (P.eb) {
+        // the kinetic energy the bath added this step: the half-kicks with
+        // and without the bath term, each from its own previous acceleration
+        const double4 ao = P.acc_ntb[i];
+        P.acc_ntb[i] = make_double4(an_ntb.x, an_ntb.y, an_ntb.z, 0.0);
+        const double h = dt / 2.0;
+        const V3 w = v3(v.x + (ac.x * h + an.x * h), v.y + (ac.y * h + an.y * h), v.z + (ac.z * h + an.z * h));
+        const V3 u = v3(v.x + (ao.x * h + an_ntb.x * h), v.y + (ao.y * h + an_ntb.y * h),
+                        v.z + (ao.z * h + an_ntb.z * h));
+        P.eb[i] += (m * (w.x * w.x + w.y * w.y + w.z * w.z) / 2.0 - m * (u.x * u.x + u.y * u.y + u.z * u.z) / 2.0) /
+                   kAccConv;
+      }
     }
     S.acc[i] = make_double4(an.x, an.y, an.z, 0.0);
     const V3 vn = v3(vdt2.x + an.x * dt / 2.0, vdt2.y + an.y * dt / 2.0, vdt2.z + an.z * dt / 2.0);

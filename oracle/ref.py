@@ -58,6 +58,16 @@ def lib():
         L.ref_rcutoff.argtypes = [vp, ctypes.c_int]
         L.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, ip, dp, dp, dp]
         L.ref_last_run_times.argtypes = [vp, dp, ctypes.c_int]
+        ub = ctypes.POINTER(ctypes.c_ubyte)
+        L.ref_set_zip.argtypes = [ctypes.c_int]
+        L.ref_write_state.argtypes = [vp, ctypes.c_char_p]
+        L.ref_write_xva.argtypes = [vp, ctypes.c_char_p]
+        L.ref_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.c_ulong]
+        L.ref_atom_count.argtypes = [vp]
+        L.ref_get_atoms.argtypes = [vp, dp, dp, dp, ip, ub, ub, ub, ip]
+        L.ref_set_tags.argtypes = [vp, ub]
+        L.ref_get_loop.argtypes = [vp, dp]
+        L.ref_set_output.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, ctypes.c_double]
         L.ref_tables.restype = ctypes.c_long
         L.ref_tables.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_long]
         L.ref_spline_eval.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
@@ -172,6 +182,74 @@ class RefSystem:
         ts = np.zeros(nsteps + 2)
         lib().ref_last_run_times(self.h, _dp(ts), nsteps + 2)
         return {"pos": pos, "vel": vel, "image": img, "epot": ep, "etot": et, "e0": float(e0[0]), "times": ts}
+
+
+def set_zip(mode: int):
+    """Compression of the reference's files: 0 plain, 1 .gz, 2 .xz."""
+    _check(lib().ref_set_zip(mode))
+
+
+def _ub(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
+
+
+def _write_state(self, id: str):
+    """SimLoopSaver::write(id)."""
+    _check(lib().ref_write_state(self.h, os.fsencode(id)))
+
+
+def _write_xva(self, path: str):
+    """SimLoop::saveToStreamXVA into path."""
+    _check(lib().ref_write_xva(self.h, os.fsencode(path)))
+
+
+def _load_state(self, id: str, iteration: int = 0) -> int:
+    """SimLoopSaver::load(id) with SimLoop::iteration = iteration; later
+    runs continue the loaded time and iteration."""
+    got = lib().ref_load_state(self.h, os.fsencode(id), int(iteration))
+    _check(-1 if got < 0 else 0)
+    self.n = lib().ref_atom_count(self.h)
+    return got
+
+
+def _atoms(self) -> dict:
+    """Per-atom state (A, A/fs, A/fs^2) and flags of the reference's atoms."""
+    n = lib().ref_atom_count(self.h)
+    out = {"pos": np.zeros((n, 3)), "vel": np.zeros((n, 3)), "acc": np.zeros((n, 3)),
+           "image": np.zeros((n, 3), np.int32), "fixed": np.zeros(n, np.uint8), "tb_apply": np.zeros(n, np.uint8),
+           "tags": np.zeros(n, np.uint8), "z": np.zeros(n, np.int32)}
+    _check(lib().ref_get_atoms(self.h, _dp(out["pos"]), _dp(out["vel"]), _dp(out["acc"]), _ip(out["image"]),
+                               _ub(out["fixed"]), _ub(out["tb_apply"]), _ub(out["tags"]), _ip(out["z"])))
+    return out
+
+
+def _set_tags(self, tags):
+    t = np.ascontiguousarray(tags, dtype=np.uint8)
+    _check(lib().ref_set_tags(self.h, _ub(t)))
+
+
+def _loop(self) -> dict:
+    """SimLoop scalars: time (fs), dt, dt_prev, iteration, bath, box, Check (eV, K)."""
+    o = np.zeros(22)
+    _check(lib().ref_get_loop(self.h, _dp(o)))
+    return {"time": o[0], "dt": o[1], "dt_prev": o[2], "iteration": int(o[3]), "tb_geom": int(o[4]),
+            "tb_T0": o[5], "tb_gamma": o[6], "tb_params": o[7:12].copy(), "box": o[12:15].copy(),
+            "net_force": o[15:18].copy(), "e0": o[18], "e_cur": o[19], "e_bath": o[20], "T": o[21]}
+
+
+def _set_output(self, dir, flush_interval: int = 0, traj_interval_fs: float = 0.0):
+    """SimLoop's own file output (writestate, writetrajXVA) in later runs."""
+    _check(lib().ref_set_output(self.h, None if dir is None else os.fsencode(dir), int(flush_interval),
+                                float(traj_interval_fs)))
+
+
+RefSystem.set_output = _set_output
+RefSystem.write_state = _write_state
+RefSystem.write_xva = _write_xva
+RefSystem.load_state = _load_state
+RefSystem.atoms = _atoms
+RefSystem.set_tags = _set_tags
+RefSystem.loop = _loop
 
 
 def tables(which: int, brenner_set: int = 1) -> np.ndarray:

@@ -24,8 +24,10 @@
 #include <map>
 #include <set>
 #include <sys/time.h>
+#include <unistd.h>
 
 #include <mdtk/SimLoop.hpp>
+#include <mdtk/SimLoopSaver.hpp>
 #include <mdtk/potentials/manybody/AIREBO/REBO.hpp>
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_LJ.hpp>
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_ETors.hpp>
@@ -79,6 +81,10 @@ struct RefCtx
   int brenner_set;
   int lj_cut_mode;
   bool adaptive;
+  bool keep_time;  // ref_run continues simTime and iteration (a resumed state)
+  std::string out_dir;          // ref_run writes SimLoop's own files here (empty: none)
+  long flush_interval;          // SimLoop::iterationFlushStateInterval for out_dir runs
+  double traj_interval_fs;      // SimLoop::simTimeSaveTrajInterval for out_dir runs
   double dt0_fs;
   std::vector<std::string> names;
   REBO* rebo;
@@ -86,7 +92,7 @@ struct RefCtx
   ETors* etors;
   Brenner* brenner;
   bool nl_ready;
-  RefCtx() : potset(0), brenner_set(1), lj_cut_mode(0), adaptive(false), dt0_fs(0.5), rebo(0), lj(0), etors(0),
+  RefCtx() : potset(0), brenner_set(1), lj_cut_mode(0), adaptive(false), keep_time(false), flush_interval(1000000), traj_interval_fs(0.0), dt0_fs(0.5), rebo(0), lj(0), etors(0),
              brenner(0), nl_ready(false) {}
 };
 
@@ -404,9 +410,11 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
     FixedDtLoop& L = c->loop;
     L.fixed_dt = dt_fs * fs;
     L.dt = L.fixed_dt;
-    L.simTime = 0.0;
-    L.iteration = 0;
-    L.simTimeFinal = dt_fs * fs * (nsteps - 0.5);
+    if (!c->keep_time) {
+      L.simTime = 0.0;
+      L.iteration = 0;
+    }
+    L.simTimeFinal = L.simTime + dt_fs * fs * (nsteps - 0.5);
     L.adaptive = c->adaptive;
     if (c->adaptive) {
       L.dt = c->dt0_fs * fs;
@@ -415,12 +423,29 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
       L.breakSimLoop = false;
     }
     L.simTimeSaveTrajInterval = 1e9 * ps;
+    L.iterationFlushStateInterval = 1000000;
+    char cwd[4096] = {0};
+    const bool out = !c->out_dir.empty();
+    if (out) {
+      // SimLoop writes into the working directory (SimLoop.cxx:807-845, 1084-1092)
+      if (!getcwd(cwd, sizeof(cwd)) || chdir(c->out_dir.c_str()) != 0) {
+        g_last_error = "cannot enter " + c->out_dir;
+        return -1;
+      }
+      L.preventFileOutput = false;
+      L.iterationFlushStateInterval = c->flush_interval;
+      if (c->traj_interval_fs > 0) L.simTimeSaveTrajInterval = c->traj_interval_fs * fs;
+    }
     L.epot_log.clear();
     L.etot_log.clear();
     L.t_log.clear();
     L.dt_log.clear();
     double t_start = wall_now();
     int rc = L.execute();
+    if (out) {
+      L.preventFileOutput = true;
+      if (chdir(cwd) != 0) { g_last_error = "cannot return to the working directory"; return -1; }
+    }
     L.t_log.insert(L.t_log.begin(), t_start);
     L.t_log.push_back(wall_now());
     if (rc != 0) { g_last_error = "SimLoop::execute failed"; return -1; }
@@ -646,4 +671,176 @@ int ref_spline_eval(int fn, int n, const double* x, double* out)
   }
 }
 
+}  // extern "C"
+
+extern "C" {
+/* Compression of the reference's file streams: 0 plain, 1 ".gz" (zlib,
+ * yaatk's gzip_internal), 2 ".xz" (the xz program).  yaatk picks its first
+ * working method at start-up (yaatk.cxx:50); this overrides it. */
+int ref_set_zip(int mode)
+{
+  if (mode == 0) yaatk::Stream::zipInvokeInfoGlobal = yaatk::Stream::ZipInvokeInfo("nozip", "");
+  else if (mode == 1) yaatk::Stream::zipInvokeInfoGlobal = yaatk::Stream::ZipInvokeInfo("gzip_internal", ".gz");
+  else if (mode == 2) yaatk::Stream::zipInvokeInfoGlobal = yaatk::Stream::ZipInvokeInfo("xz", ".xz");
+  else return -1;
+  return 0;
+}
+
+/* SimLoopSaver::write(id) of the current state (SimLoopSaver.cxx:118-231). */
+int ref_write_state(void* h, const char* id)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    mdtk::SimLoopSaver saver(c->loop);
+    return saver.write(id);
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* SimLoop::saveToStreamXVA into path (SimLoop.cxx:680-748), through the same
+ * yaatk text stream writetrajXVA uses. */
+int ref_write_xva(void* h, const char* path)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    c->loop.preventFileOutput = false;
+    {
+      yaatk::text_ofstream fo(path);
+      c->loop.saveToStreamXVA(fo);
+      fo.close();
+    }
+    c->loop.preventFileOutput = true;
+    return 0;
+  } catch (std::exception& e) {
+    c->loop.preventFileOutput = true;
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* SimLoopSaver::load(id) into an emptied atom array with SimLoop::iteration
+ * = iteration (SimLoopSaver::loadIteration, SimLoopSaver.cxx:849-854);
+ * later ref_run calls continue its time and iteration.  Returns the
+ * LOADED_* bits or -1. */
+int ref_load_state(void* h, const char* id, unsigned long iteration)
+{
+  RefCtx* c = (RefCtx*)h;
+  try {
+    c->loop.atoms.clear();
+    mdtk::SimLoopSaver saver(c->loop);
+    int got = saver.load(id);
+    c->loop.iteration = iteration;
+    c->nl_ready = false;
+    c->keep_time = true;
+    return got;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  }
+}
+
+/* Number of atoms, then per-atom state in Angstrom / (A/fs) / (A/fs^2):
+ * coords, V, an, PBC_count, Atom::fixed, apply_ThermalBath, tag bits; any
+ * NULL is skipped. */
+int ref_atom_count(void* h) { return (int)((RefCtx*)h)->loop.atoms.size(); }
+
+int ref_get_atoms(void* h, double* pos, double* vel, double* acc, int* image, unsigned char* fixed,
+                  unsigned char* tb_apply, unsigned char* tags, int* z)
+{
+  RefCtx* c = (RefCtx*)h;
+  AtomsArray& at = c->loop.atoms;
+  const Float vconv = fs / Ao, aconv = fs * fs / Ao;
+  for (size_t i = 0; i < at.size(); i++) {
+    const Atom& a = at[i];
+    if (pos) { pos[3*i] = a.coords.x / Ao; pos[3*i+1] = a.coords.y / Ao; pos[3*i+2] = a.coords.z / Ao; }
+    if (vel) { vel[3*i] = a.V.x * vconv; vel[3*i+1] = a.V.y * vconv; vel[3*i+2] = a.V.z * vconv; }
+    if (acc) { acc[3*i] = a.an.x * aconv; acc[3*i+1] = a.an.y * aconv; acc[3*i+2] = a.an.z * aconv; }
+    if (image) { image[3*i] = a.PBC_count.x; image[3*i+1] = a.PBC_count.y; image[3*i+2] = a.PBC_count.z; }
+    if (fixed) fixed[i] = a.isFixed() ? 1 : 0;
+    if (tb_apply) tb_apply[i] = a.apply_ThermalBath ? 1 : 0;
+    if (tags) {
+      unsigned char t = 0;
+      const unsigned bits[6] = {ATOMTAG_TARGET, ATOMTAG_PROJECTILE, ATOMTAG_SUBSTRATE, ATOMTAG_MONOMER,
+                                ATOMTAG_CLUSTER, ATOMTAG_FULLERENE};
+      for (int k = 0; k < 6; k++) if (a.hasTag(bits[k])) t |= (unsigned char)bits[k];
+      tags[i] = t;
+    }
+    if (z) z[i] = a.ID == H_EL ? 1 : (a.ID == C_EL ? 6 : -1);
+  }
+  return 0;
+}
+
+/* Per-atom tag bits (Atom::tag). */
+int ref_set_tags(void* h, const unsigned char* tags)
+{
+  RefCtx* c = (RefCtx*)h;
+  AtomsArray& at = c->loop.atoms;
+  const unsigned bits[6] = {ATOMTAG_TARGET, ATOMTAG_PROJECTILE, ATOMTAG_SUBSTRATE, ATOMTAG_MONOMER,
+                            ATOMTAG_CLUSTER, ATOMTAG_FULLERENE};
+  for (size_t i = 0; i < at.size(); i++)
+    for (int k = 0; k < 6; k++) {
+      if (tags[i] & bits[k]) at[i].tag(bits[k]);
+      else at[i].untag(bits[k]);
+    }
+  return 0;
+}
+
+/* SimLoop scalars: [0] simTime (fs), [1] dt (fs), [2] dt_prev (fs),
+ * [3] iteration, [4] bath geometry, [5] To (K), [6] gamma (1/s),
+ * [7..11] geometry parameters (A), [12..14] box (A, 0 = open axis),
+ * [15..21] Check: netForce (eV/A x3), initialEnergy, currentEnergy,
+ * energyTransferredFromBath (eV), currentTemperature (K). */
+int ref_get_loop(void* h, double* out)
+{
+  RefCtx* c = (RefCtx*)h;
+  FixedDtLoop& L = c->loop;
+  out[0] = L.simTime / fs;
+  out[1] = L.dt / fs;
+  out[2] = L.dt_prev / fs;
+  out[3] = (double)L.iteration;
+  out[4] = (double)L.thermalBathGeomType;
+  out[5] = L.thermalBathCommon.To;
+  out[6] = L.thermalBathCommon.gamma;
+  for (int k = 7; k < 12; k++) out[k] = 0.0;
+  if (L.thermalBathGeomType == SimLoop::TB_GEOM_BOX) {
+    out[7] = L.thermalBathGeomBox.zMin / Ao;
+    out[8] = L.thermalBathGeomBox.dBoundary / Ao;
+    out[9] = L.thermalBathGeomBox.zMinOfFreeZone / Ao;
+  }
+  if (L.thermalBathGeomType == SimLoop::TB_GEOM_SPHERE) {
+    out[7] = L.thermalBathGeomSphere.center.x / Ao;
+    out[8] = L.thermalBathGeomSphere.center.y / Ao;
+    out[9] = L.thermalBathGeomSphere.center.z / Ao;
+    out[10] = L.thermalBathGeomSphere.radius / Ao;
+    out[11] = L.thermalBathGeomSphere.zMinOfFreeZone / Ao;
+  }
+  const Vector3D pbc = L.atoms.PBC();
+  out[12] = pbc.x != NO_PBC.x ? pbc.x / Ao : 0.0;
+  out[13] = pbc.y != NO_PBC.y ? pbc.y / Ao : 0.0;
+  out[14] = pbc.z != NO_PBC.z ? pbc.z / Ao : 0.0;
+  out[15] = L.check.netForce.x * Ao / eV;
+  out[16] = L.check.netForce.y * Ao / eV;
+  out[17] = L.check.netForce.z * Ao / eV;
+  out[18] = L.check.initialEnergy / eV;
+  out[19] = L.check.currentEnergy / eV;
+  out[20] = L.check.energyTransferredFromBath / eV;
+  out[21] = L.check.currentTemperature;
+  return 0;
+}
+}  // extern "C"
+
+extern "C" {
+/* Let ref_run write SimLoop's own state and XVA files into dir (NULL: none),
+ * with iterationFlushStateInterval = flush_interval and
+ * simTimeSaveTrajInterval = traj_interval_fs (fs; 0 keeps it out of reach). */
+int ref_set_output(void* h, const char* dir, long flush_interval, double traj_interval_fs)
+{
+  RefCtx* c = (RefCtx*)h;
+  c->out_dir = dir ? dir : "";
+  c->flush_interval = flush_interval > 0 ? flush_interval : 1000000;
+  c->traj_interval_fs = traj_interval_fs;
+  return 0;
+}
 }  // extern "C"

@@ -158,3 +158,62 @@ def test_parameter_override_acts_on_the_reference():
     assert e1 == e0
     r.set_param(1, 3.41)
     assert r.compute()[1][1] != et0[1]
+
+
+@pytest.mark.parametrize("zip_mode,ext", [(0, ""), (1, ".gz"), (2, ".xz")])
+def test_reference_state_files_round_trip(tmp_path, zip_mode, ext):
+    """The harness drives the reference's own SimLoopSaver: a state written
+    after 10 steps (box bath, fixed atoms, tags) loads back unchanged, in
+    each of yaatk's compressions, and the loaded run continues where the
+    first would have gone."""
+    s = B.impact(3, n_target=900)
+    zmin = s["pos"][:, 2].min()
+    r = ref.RefSystem(ref.POT_REBO)
+    r.set_atoms(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    tags = np.zeros(len(s["z"]), np.uint8)
+    tags[-13:] = 1 << 2  # ATOMTAG_PROJECTILE
+    r.set_tags(tags)
+    r.set_bath(2, 300.0, 1e13, [zmin - 1.0, 3.0, zmin + 1.0])
+    r.run(10, 0.5)
+    ref.set_zip(zip_mode)
+    try:
+        r.write_state(str(tmp_path / "md0000000010"))
+    finally:
+        ref.set_zip(0)
+    assert os.path.exists(str(tmp_path / "md0000000010.r") + ext)
+    assert os.path.exists(str(tmp_path / "md0000000010.thermal_bath.box") + ext)
+    r2 = ref.RefSystem(ref.POT_REBO)
+    assert r2.load_state(str(tmp_path / "md0000000010"), 10) == 127
+    a, b = r.atoms(), r2.atoms()
+    for k in ("pos", "vel", "acc", "image", "fixed", "tb_apply", "tags", "z"):
+        assert np.array_equal(a[k], b[k]), k
+    la, lb = r.loop(), r2.loop()
+    for k in ("time", "dt", "dt_prev", "iteration", "tb_geom", "tb_T0", "tb_gamma", "e0", "e_cur", "e_bath", "T"):
+        assert la[k] == lb[k], k
+    assert np.array_equal(la["tb_params"], lb["tb_params"]) and np.array_equal(la["box"], lb["box"])
+
+
+def test_reference_xva_layout(tmp_path):
+    """SimLoop::saveToStreamXVA's text layout as the device writer restates
+    it: velocity scale (%g), distance scale, atom count, three lines per atom
+    (V/scale and coords/Ao with two decimals, image counters), the Check
+    record, simTime, dt, iteration, run time (%.10e)."""
+    s = B.diamond(3, temp_k=300.0, seed=9)
+    r = ref.RefSystem(ref.POT_REBO)
+    r.set_atoms(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    r.run(4, 0.5)
+    r.write_xva(str(tmp_path / "f.xva"))
+    lines = open(tmp_path / "f.xva").read().splitlines()
+    n = len(s["z"])
+    v = r.atoms()["vel"] * 1e-8 / 1e-15  # cm/s
+    scale = 10.0 ** (np.ceil(np.log10(np.abs(v).sum() / (3.0 * n))) - 2)
+    assert lines[0] == "%g" % scale and lines[1] == "1e-08" and lines[2] == str(n)
+    assert len(lines) == 3 + 3 * n + 11
+    a = r.atoms()
+    for i in (0, n // 2, n - 1):
+        assert lines[3 + 3 * i] == "%.2f %.2f %.2f" % tuple(a["vel"][i] * 1e7 / scale)
+        assert lines[4 + 3 * i] == "%.2f %.2f %.2f" % tuple(a["pos"][i] * 1e-8 / 1e-8)
+        assert lines[5 + 3 * i] == "%d %d %d" % tuple(a["image"][i])
+    tail = lines[3 + 3 * n:]
+    assert tail[0] == "1" and tail[2] == "1" and tail[1].endswith(" ") and tail[9] == "4"
+    assert all(len(t.split("e")) == 2 for t in tail[3:9] + [tail[10]])
