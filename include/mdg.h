@@ -341,6 +341,57 @@ int mdg_atom_count(mdg_ctx* ctx, int* n);
 /* SimLoop::simTimeFinal as stored in the ".time" file (time units; default 4 ps). */
 int mdg_set_time_final(mdg_ctx* ctx, double time_final);
 
+/* Per-system simulated time and dt (time units, [nsys] each; the adaptive
+ * step's state, SimLoop::simTime and dt of a loaded base state); dt_prev = dt. */
+int mdg_set_time(mdg_ctx* ctx, const double* sim_time, const double* dt);
+
+/* PBC_count of every atom ([n*3]; the wrapped positions stay). */
+int mdg_set_images(mdg_ctx* ctx, const int32_t* image);
+
+/* SimLoop's loop condition simTime < simTimeFinal (SimLoop.cxx:252) per
+ * system, with adaptive dt: a system that reached simTimeFinal takes no more
+ * steps (its later steps have dt 0 and leave it unchanged; its time, dt and
+ * dt_prev stay as its last step left them) and, with output on, gets its
+ * final state files (executeMain's closing writestate) at the iteration it
+ * ended on. */
+int mdg_set_stop_at_time_final(mdg_ctx* ctx, int on);
+
+/* Steps (graph-replayed, checked every 16 steps) until every system reached
+ * simTimeFinal or max_steps were taken; *steps gets the steps taken,
+ * *finished 1 when every system is done.  Waits for the queued files. */
+int mdg_run_until_final(mdg_ctx* ctx, int64_t max_steps, int64_t* steps, int* finished);
+
+/* Output directory of each system of a batched context ([nsys] names,
+ * created if missing; NULL restores "<dir>/sys%05d"). */
+int mdg_set_output_dirs(mdg_ctx* ctx, const char* const* dirs);
+
+/* The XVA interval as a table: interval[k] while simTime < until[k] (time
+ * units, up to 4 entries; mdtrajsim's CustomSimLoop uses 1 ps below 2 ps,
+ * then 5 ps, mdtrajsim/main.cpp:59-60).  Call after mdg_set_output. */
+int mdg_set_traj_schedule(mdg_ctx* ctx, int n, const double* until, const double* interval);
+
+/* ---- SnapshotList (SnapshotList.hpp:38-205) ----
+ * mdtrajsim's snapshots of the projectile and cluster atoms (tag bits 2 and
+ * 5), taken on the device at the top of each iteration whenever simTime has
+ * crossed a multiple of the current interval (CustomSimLoop::isItTimeToSave,
+ * mdtrajsim/main.cpp:52-80: 10 fs below 2 ps, 50 fs below 4 ps, then 100 fs);
+ * records are float coordinates and velocities in CGS and the PBC counters,
+ * as SnapshotList::AtomSnapshot.  Needs the adaptive time step (snapshots
+ * follow simTime); capacity = snapshots kept per system (exceeding it is an
+ * MDG_ERR_CAPACITY status).  With output on, "snapshots.conf" is written in
+ * each system's directory every flush_interval iterations. */
+int mdg_snapshots_enable(mdg_ctx* ctx, int on, int capacity);
+int mdg_snapshots_set_schedule(mdg_ctx* ctx, int n, const double* until, const double* interval);
+int mdg_snapshots_count(mdg_ctx* ctx, int sys, int* nshots, int* natoms);
+/* times [nshots] (time units), indices [natoms] (atomsSelectedForSaving),
+ * pbc_count/pos/vel [nshots * natoms * 3]; any NULL is skipped. */
+int mdg_snapshots_get(mdg_ctx* ctx, int sys, double* times, uint32_t* indices, int32_t* pbc_count, float* pos,
+                      float* vel);
+/* SnapshotList::writestate ("snapshots.conf" layout) or, text != 0, saveInText. */
+int mdg_snapshots_write(mdg_ctx* ctx, int sys, const char* path, int zip, int text);
+/* SnapshotList::loadstate: earlier snapshots of system sys (same selection). */
+int mdg_snapshots_load(mdg_ctx* ctx, int sys, const char* path);
+
 /* The launch configuration the autotuner chose (task_mode 0): overlap = 1
  * when the REBO tasks run on a second stream concurrently with the LJ
  * kernels, rebo_blocks = the REBO task kernel's grid.  No reference

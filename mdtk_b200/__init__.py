@@ -143,6 +143,20 @@ def lib():
         L.mdg_get_iteration.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
         L.mdg_set_time_final.argtypes = [vp, ctypes.c_double]
         L.mdg_atom_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.mdg_set_time.argtypes = [vp, dp, dp]
+        L.mdg_set_stop_at_time_final.argtypes = [vp, ctypes.c_int]
+        L.mdg_run_until_final.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int)]
+        L.mdg_set_output_dirs.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p)]
+        L.mdg_set_traj_schedule.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.mdg_snapshots_enable.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.mdg_snapshots_set_schedule.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.mdg_snapshots_count.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.mdg_snapshots_get.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_uint32), i32p,
+                                        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+        L.mdg_snapshots_write.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        L.mdg_snapshots_load.argtypes = [vp, ctypes.c_int, ctypes.c_char_p]
+        L.mdg_set_images.argtypes = [vp, i32p]
         _lib = L
     return _lib
 
@@ -336,6 +350,71 @@ class Context:
 
     def set_time_final(self, t: float):
         _check(lib().mdg_set_time_final(self.h, float(t)))
+
+    def set_time(self, sim_time, dt):
+        """Per-system simulated time and dt (time units)."""
+        ns = getattr(self, "nsys", 1)
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(sim_time, float), (ns,)))
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, float), (ns,)))
+        _check(lib().mdg_set_time(self.h, _dp(t), _dp(d)))
+
+    def set_images(self, image):
+        """PBC_count of every atom ([n, 3])."""
+        im = np.ascontiguousarray(image, dtype=np.int32)
+        _check(lib().mdg_set_images(self.h, _ip(im)))
+
+    def set_stop_at_time_final(self, on: bool = True):
+        _check(lib().mdg_set_stop_at_time_final(self.h, 1 if on else 0))
+
+    def run_until_final(self, max_steps: int = 10 ** 9):
+        """Steps until every system reached simTimeFinal; (steps, finished)."""
+        st = ctypes.c_int64()
+        fin = ctypes.c_int()
+        _check(lib().mdg_run_until_final(self.h, int(max_steps), ctypes.byref(st), ctypes.byref(fin)))
+        return st.value, bool(fin.value)
+
+    def set_output_dirs(self, dirs):
+        arr = None
+        if dirs is not None:
+            self._dirs = [os.fsencode(d) for d in dirs]
+            arr = (ctypes.c_char_p * len(self._dirs))(*self._dirs)
+        _check(lib().mdg_set_output_dirs(self.h, arr))
+
+    def set_traj_schedule(self, until, interval):
+        u = np.ascontiguousarray(until, dtype=np.float64)
+        v = np.ascontiguousarray(interval, dtype=np.float64)
+        _check(lib().mdg_set_traj_schedule(self.h, len(u), _dp(u), _dp(v)))
+
+    # ---- SnapshotList
+
+    def snapshots_enable(self, on: bool = True, capacity: int = 4096):
+        _check(lib().mdg_snapshots_enable(self.h, 1 if on else 0, int(capacity)))
+
+    def snapshots_set_schedule(self, until, interval):
+        u = np.ascontiguousarray(until, dtype=np.float64)
+        v = np.ascontiguousarray(interval, dtype=np.float64)
+        _check(lib().mdg_snapshots_set_schedule(self.h, len(u), _dp(u), _dp(v)))
+
+    def snapshots(self, sys: int = 0) -> dict:
+        """times (time units), indices, and per snapshot and atom the PBC
+        counters, float coordinates (cm) and velocities (cm/s)."""
+        ns, na = ctypes.c_int(), ctypes.c_int()
+        _check(lib().mdg_snapshots_count(self.h, sys, ctypes.byref(ns), ctypes.byref(na)))
+        t = np.zeros(ns.value)
+        idx = np.zeros(na.value, np.uint32)
+        pc = np.zeros((ns.value, na.value, 3), np.int32)
+        p = np.zeros((ns.value, na.value, 3), np.float32)
+        v = np.zeros((ns.value, na.value, 3), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(lib().mdg_snapshots_get(self.h, sys, _dp(t), idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                       _ip(pc), p.ctypes.data_as(fp), v.ctypes.data_as(fp)))
+        return {"time": t, "indices": idx, "pbc_count": pc, "pos": p, "vel": v}
+
+    def snapshots_write(self, path: str, zip: int = ZIP_NONE, text: bool = False, sys: int = 0):
+        _check(lib().mdg_snapshots_write(self.h, sys, os.fsencode(path), zip, 1 if text else 0))
+
+    def snapshots_load(self, path: str, sys: int = 0):
+        _check(lib().mdg_snapshots_load(self.h, sys, os.fsencode(path)))
 
     def tuned_launch(self):
         """(overlap, rebo_blocks): the autotuner's launch choice."""

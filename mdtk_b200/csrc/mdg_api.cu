@@ -704,10 +704,14 @@ __global__ void k_bath_final(const double* part, int nblk_sys, int nsys, double*
 // advances by the step's dt, then dt = 0.05 timeaccel / v_max clamped to
 // [1e-5, 0.5] fs (0.5 fs without a moving atom).
 __global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, double* dt_prev, double* time,
-                            double timeaccel)
+                            double timeaccel, int* stop, double time_final)
 {
   const int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= nsys) return;
+  if (stop && stop[sy]) {  // finished: time and dt stay as the last step left them
+    vmax[sy] = 0ull;
+    return;
+  }
   const double vm = __longlong_as_double((long long)vmax[sy]);
   const double dt_max = 0.5, dt_min = 1e-5;
   double d = vm != 0.0 ? 0.05 * timeaccel / vm : dt_max;
@@ -717,6 +721,15 @@ __global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, doub
   dt_prev[sy] = dt[sy];
   dt[sy] = d;
   vmax[sy] = 0ull;
+  // the loop runs while simTime < simTimeFinal (SimLoop.cxx:252)
+  if (stop && !(time[sy] < time_final)) stop[sy] = 1;
+}
+
+// Systems already at or past simTimeFinal take no step.
+__global__ void k_stop_init(int nsys, const double* time, int* stop, double time_final)
+{
+  const int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy < nsys) stop[sy] = !(time[sy] < time_final);
 }
 
 // Host-step layout conversion: io = [pos (n*3) | vel (n*3)] in the caller's
@@ -992,6 +1005,9 @@ struct mdg_ctx {
   bool chk_loaded = false;              // a loaded Check record stands until the next step
   double chk_net[3] = {0, 0, 0}, chk_cur = 1.0, chk_T = 0.0;
   double run_t0 = 0.0;                  // wall clock at the first step (SimLoop::CPUTimeUsed_total's start)
+  bool stop_final = false;              // adaptive systems stop at simTimeFinal
+  int* d_stop = nullptr;                // [nsys] a system reached simTimeFinal
+  struct SnapState* snap = nullptr;     // device SnapshotList capture (mdtrajsim)
   double* d_e0 = nullptr;               // [nsys * 4] rebo, lj, tors, kin at the first step
   double* d_ekin_pre = nullptr;         // [n] M V_n^2 / 2 before the last kick
   double4* acc_ntb = nullptr;           // [n] Atom::an_no_tb (with a bath)
@@ -1123,12 +1139,15 @@ int status_to_code(unsigned int st, std::string& msg)
   add(ST_CIJ_OVERFLOW, MDG_ERR_CAPACITY, "connectivity table capacity exceeded;");
   add(ST_RECORD_OVERFLOW, MDG_ERR_CAPACITY, "bond or connectivity record capacity exceeded;");
   add(ST_CELL_OVERFLOW, MDG_ERR_CAPACITY, "cell grid capacity exceeded;");
+  add(ST_SNAP_OVERFLOW, MDG_ERR_CAPACITY, "snapshot list capacity exceeded;");
   return code;
 }
 
 void adj_free(mdg_ctx* c);
 void io_release(mdg_ctx* c);
 void io_free(mdg_ctx* c);
+void snap_free(mdg_ctx* c);
+int snap_capture(mdg_ctx* c);
 
 void free_system(mdg_ctx* c)
 {
@@ -1136,13 +1155,15 @@ void free_system(mdg_ctx* c)
   adj_free(c);
   {
     void* st[] = {c->d_tb_apply, c->d_tb_T, c->d_tb_part, c->d_dt, c->d_time, c->d_vmax, c->d_dt_prev,
-                  c->d_e0, c->d_ekin_pre, c->acc_ntb, c->d_eb};
+                  c->d_e0, c->d_ekin_pre, c->acc_ntb, c->d_eb, c->d_stop};
     for (void* p : st)
       if (p) cudaFree(p);
     c->d_tb_apply = nullptr;
     c->d_tb_T = c->d_tb_part = c->d_dt = c->d_time = c->d_dt_prev = nullptr;
     c->d_e0 = c->d_ekin_pre = c->d_eb = nullptr;
     c->acc_ntb = nullptr;
+    c->d_stop = nullptr;
+    snap_free(c);
     c->d_vmax = nullptr;
     c->h_z.clear();
     c->h_fixed.clear();
@@ -1398,6 +1419,11 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
   const bool tasks = c->bt.ctr != nullptr;
   const bool ovl = tasks && lj && c->overlap && !c->prof && c->side;
   int rc;
+  if (step && c->snap) {
+    // CustomSimLoop::doBeforeIteration's snapshots (mdtrajsim/main.cpp:59-80)
+    rc = snap_capture(c);
+    if (rc) return rc;
+  }
   if (ovl) {
     // the LJ list's check/rebuild and the in-range filter (positions and the
     // LJ list only) on the third stream, beside the REBO list and the bonds
@@ -1501,7 +1527,7 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
            *step, c->e_kin, c->d_status);
     if (step->vmax)
       LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_dt_prev, c->d_time,
-             c->timeaccel);
+             c->timeaccel, c->stop_final ? c->d_stop : nullptr, c->time_final_s / kFs);
   }
   else
     LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
@@ -1920,9 +1946,11 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   c->d_vmax = dalloc<unsigned long long>(nsys);
   c->d_e0 = dalloc<double>(4 * (size_t)nsys);
   c->d_ekin_pre = dalloc<double>(n);
+  c->d_stop = dalloc<int>(nsys);
   if (!c->d_tb_T || !c->d_tb_part || !c->d_dt || !c->d_dt_prev || !c->d_time || !c->d_vmax || !c->d_e0 ||
-      !c->d_ekin_pre)
+      !c->d_ekin_pre || !c->d_stop)
     return fail(MDG_ERR_CUDA, "cudaMalloc (step state)");
+  CK(cudaMemset(c->d_stop, 0, nsys * sizeof(int)));
   CK(cudaMemset(c->d_ekin_pre, 0, n * sizeof(double)));
   CK(cudaMemset(c->d_e0, 0, 4 * (size_t)nsys * sizeof(double)));
   c->h_z.assign(z, z + n);
@@ -2160,6 +2188,7 @@ static StepDev step_dev(mdg_ctx* c, double dtf)
   P.ekin_pre = c->d_ekin_pre;
   P.acc_ntb = c->tb_geom ? c->acc_ntb : nullptr;
   P.eb = c->tb_geom ? c->d_eb : nullptr;
+  P.stop = (c->adaptive && c->stop_final) ? c->d_stop : nullptr;
   return P;
 }
 
@@ -2190,9 +2219,10 @@ static int ensure_step_graph(mdg_ctx* c, double dtf)
 
 int sys_energies(mdg_ctx* c, double* out_dev);
 // checkpoint and trajectory output around the steps (defined with the file formats)
-int io_run_start(mdg_ctx* c, double dtf);
+int io_run_start(mdg_ctx* c, double dtf, bool fresh);
 int io_before_step(mdg_ctx* c);
 int io_after_step(mdg_ctx* c);
+int io_run_end(mdg_ctx* c);
 
 // The first step's accelerations, and at iteration 0 the Check record's
 // initial energy and the bath's energy count (SimLoop.cxx:305-321, 1133-1137).
@@ -2215,7 +2245,9 @@ static int init_first_step(mdg_ctx* c)
   return MDG_OK;
 }
 
-int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
+// fresh: a new SimLoop::execute (dt_prev = dt); else the continuation of
+// the previous call's loop
+static int run_steps(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot, bool fresh)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
@@ -2224,7 +2256,7 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
   if (rc) return rc;
   rc = autotune(c);
   if (rc) return rc;
-  rc = io_run_start(c, dtf);
+  rc = io_run_start(c, dtf, fresh);
   if (rc) return rc;
   const bool log = epot || etot;
   if (log && c->elog_cap < (int64_t)nsteps * 4) {
@@ -2259,6 +2291,8 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
       if (rc) return rc;
     }
   }
+  rc = io_run_end(c);
+  if (rc) return rc;
   if (log) {
     std::vector<double> h((size_t)nsteps * 4);
     CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -2272,6 +2306,11 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     return MDG_OK;
   }
   return launch_check(c);
+}
+
+int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
+{
+  return run_steps(c, nsteps, dt, epot, etot, true);
 }
 
 int sys_energies(mdg_ctx* c, double* out_dev)
@@ -2292,7 +2331,7 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
   if (rc) return rc;
   rc = autotune(c);
   if (rc) return rc;
-  rc = io_run_start(c, dtf);
+  rc = io_run_start(c, dtf, true);
   if (rc) return rc;
   const int64_t need = (int64_t)nsteps * c->nsys * 4;
   if (c->elog_cap < need) {
@@ -2312,6 +2351,8 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
     rc = sys_energies(c, c->d_elog + (int64_t)s * c->nsys * 4);
     if (rc) return rc;
   }
+  rc = io_run_end(c);
+  if (rc) return rc;
   std::vector<double> h((size_t)need);
   CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   rc = read_status(c);

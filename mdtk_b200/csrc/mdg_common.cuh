@@ -43,6 +43,7 @@ enum StatusBits : unsigned int {
   ST_RECORD_OVERFLOW = 1u << 7, // bond-task or special-pair record capacity exceeded
   ST_SPLINE_DOMAIN = 1u << 8,   // spline argument outside its domain (cubici.hpp:90,211,305)
   ST_CELL_OVERFLOW = 1u << 9,   // cell grid capacity exceeded
+  ST_SNAP_OVERFLOW = 1u << 10,  // snapshot list capacity exceeded
 };
 
 // FP32 scalar of the mixed-precision path: float arithmetic; double operands

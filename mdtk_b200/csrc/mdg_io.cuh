@@ -250,10 +250,13 @@ struct IoState {
   // schedule (SimLoop::iterationFlushStateInterval, simTimeSaveTrajInterval)
   bool on = false;
   std::string dir;
+  std::vector<std::string> dirs;  // per-system directories (batched contexts), else dir/sys%05d
   int64_t flush_interval = 0;
-  double traj_interval_s = 0.0;
+  int ntraj = 0;                  // XVA interval table: traj_int[k] while simTime < traj_until[k] (s)
+  double traj_until[4] = {0, 0, 0, 0}, traj_int[4] = {0, 0, 0, 0};
+  std::vector<char> fin;          // per system: its final state is written
   int zip = MDG_ZIP_NONE;
-  double* h_time = nullptr;    // pinned [3 nsys]: time, dt, dt_prev of adaptive steps
+  double* h_time = nullptr;    // pinned [3 nsys]: time, dt_prev, stop flag of adaptive steps
   int h_time_cap = 0;
   std::chrono::steady_clock::time_point t_run;  // start of the current mdg_run
   double cpu_prev_s = 0.0;     // run time of the earlier runs (SimLoop::CPUTimeUsed_prev)
@@ -657,6 +660,7 @@ static void io_push(mdg_ctx* c, std::vector<IoJob>& jobs)
 
 static std::string sys_dir(mdg_ctx* c, int sys)
 {
+  if ((int)c->io->dirs.size() == c->nsys) return c->io->dirs[sys];
   if (c->nsys == 1) return c->io->dir;
   char b[32];
   std::snprintf(b, sizeof(b), "/sys%05d", sys);
@@ -666,12 +670,16 @@ static std::string sys_dir(mdg_ctx* c, int sys)
 // -------------------------------------------------------------------------
 // SimLoop::executeMain's bookkeeping and output schedule around the steps
 
-int io_run_start(mdg_ctx* c, double dtf)
+int io_run_start(mdg_ctx* c, double dtf, bool fresh)
 {
   if (c->run_t0 <= 0.0) c->run_t0 = wall_s();
   // executeMain takes dt_prev = dt before its loop (SimLoop.cxx:249)
-  if (c->adaptive) {
+  if (!fresh) {
+  } else if (c->adaptive) {
     CK(cudaMemcpyAsync(c->d_dt_prev, c->d_dt, c->nsys * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (c->stop_final)
+      LAUNCH(c, "stop_init", k_stop_init, nblk(c->nsys), kThreads, c->nsys, c->d_time, c->d_stop,
+             c->time_final_s / kFs);
   } else {
     c->dt_s = dtf * kFs;
     c->dt_prev_s = c->dt_s;
@@ -691,44 +699,110 @@ int io_run_start(mdg_ctx* c, double dtf)
 // iterationFlushStateInterval iterations but the first, an XVA frame at the
 // first iteration and whenever simTime has crossed a multiple of
 // simTimeSaveTrajInterval during the last step.
+namespace {
+int snap_write(mdg_ctx* c, int sys, const std::string& path, int zip, bool text);
+}
+
+static double traj_interval(const IoState* io, double t)
+{
+  for (int k = 0; k < io->ntraj; k++)
+    if (t < io->traj_until[k]) return io->traj_int[k];
+  return io->traj_int[io->ntraj - 1];
+}
+
+// Per-system time, dt_prev and stop flag of adaptive steps, read back.
+static int io_read_times(mdg_ctx* c)
+{
+  IoState* io = c->io;
+  if (io->h_time_cap < c->nsys) {
+    if (io->h_time) cudaFreeHost(io->h_time);
+    io->h_time = nullptr;
+    if (cudaHostAlloc((void**)&io->h_time, 3 * c->nsys * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
+      return fail(MDG_ERR_CUDA, "cudaHostAlloc (time readback)");
+    io->h_time_cap = c->nsys;
+  }
+  CK(cudaMemcpyAsync(io->h_time, c->d_time, c->nsys * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(io->h_time + c->nsys, c->d_dt_prev, c->nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  std::vector<int> st((size_t)c->nsys, 0);
+  if (c->stop_final)
+    CK(cudaMemcpyAsync(st.data(), c->d_stop, c->nsys * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < c->nsys; s++) io->h_time[2 * c->nsys + s] = st[s];
+  return MDG_OK;
+}
+
+// Systems that reached simTimeFinal since the last look get executeMain's
+// closing state files (SimLoop.cxx:460-464) at the iteration they ended on.
+static int io_finalize(mdg_ctx* c, std::vector<IoJob>& jobs, int& slot)
+{
+  IoState* io = c->io;
+  if (!c->stop_final || !c->adaptive) return MDG_OK;
+  io->fin.resize(c->nsys, 0);
+  char name[64];
+  for (int s = 0; s < c->nsys; s++) {
+    if (!io->h_time[2 * c->nsys + s] || io->fin[s]) continue;
+    if (slot < 0) {
+      int rc = io_snapshot(c, &slot);
+      if (rc) return rc;
+    }
+    std::snprintf(name, sizeof(name), "/md%010lu", (unsigned long)c->iteration);
+    jobs.push_back(io_job(c, slot, kJobState, s, sys_dir(c, s) + name, io->zip));
+    io->fin[s] = 1;
+  }
+  return MDG_OK;
+}
+
+// The top of an iteration (SimLoop.cxx:263-277, with CustomSimLoop's
+// doBeforeIteration before it, mdtrajsim/main.cpp:59-85): the snapshot list
+// and the state files every iterationFlushStateInterval iterations but the
+// first, an XVA frame at the first iteration and whenever simTime has crossed
+// a multiple of simTimeSaveTrajInterval during the last step.  Systems that
+// reached simTimeFinal write nothing more.
 int io_before_step(mdg_ctx* c)
 {
   if (!c->io || !c->io->on) return MDG_OK;
   IoState* io = c->io;
   const uint64_t it = c->iteration;
-  const bool state = io->flush_interval > 0 && it % (uint64_t)io->flush_interval == 0 && it != 0;
+  const bool flush = io->flush_interval > 0 && it % (uint64_t)io->flush_interval == 0 && it != 0;
+  const bool readback = c->adaptive && (io->ntraj > 0 || c->stop_final);
+  if (readback) {
+    int rc = io_read_times(c);
+    if (rc) return rc;
+  }
+  auto stopped = [&](int s) { return readback && io->h_time[2 * c->nsys + s] != 0.0; };
+  std::vector<IoJob> jobs;
+  int slot = -1;
+  int rc = io_finalize(c, jobs, slot);
+  if (rc) return rc;
   std::vector<char> xva((size_t)c->nsys, 0);
-  bool any_xva = false;
-  if (io->traj_interval_s > 0.0) {
-    if (c->adaptive) {
-      if (io->h_time_cap < c->nsys) {
-        if (io->h_time) cudaFreeHost(io->h_time);
-        io->h_time = nullptr;
-        if (cudaHostAlloc((void**)&io->h_time, 2 * c->nsys * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
-          return fail(MDG_ERR_CUDA, "cudaHostAlloc (time readback)");
-        io->h_time_cap = c->nsys;
-      }
-      CK(cudaMemcpyAsync(io->h_time, c->d_time, c->nsys * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaMemcpyAsync(io->h_time + c->nsys, c->d_dt_prev, c->nsys * sizeof(double), cudaMemcpyDeviceToHost,
-                         c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-    }
-    const double I = io->traj_interval_s;
-    for (int s = 0; s < c->nsys; s++) {
+  bool any = false;
+  for (int s = 0; s < c->nsys; s++) {
+    if (stopped(s)) continue;
+    if (io->ntraj > 0) {
       const double t = c->adaptive ? io->h_time[s] * kFs : c->time_s;
       const double dtp = c->adaptive ? io->h_time[c->nsys + s] * kFs : c->dt_prev_s;
+      const double I = traj_interval(io, t);
       xva[s] = it == 0 || t == 0.0 || (long long)(t / I) != (long long)((t - dtp) / I);
-      any_xva = any_xva || xva[s];
+    }
+    any = any || xva[s] || flush;
+  }
+  if (flush && c->snap) {
+    // CustomSimLoop writes its snapshot list at the same iterations
+    for (int s = 0; s < c->nsys; s++) {
+      if (stopped(s)) continue;
+      rc = snap_write(c, s, sys_dir(c, s) + "/snapshots.conf", io->zip, false);
+      if (rc) return rc;
     }
   }
-  if (!state && !any_xva) return MDG_OK;
-  int slot = 0;
-  int rc = io_snapshot(c, &slot);
-  if (rc) return rc;
-  std::vector<IoJob> jobs;
+  if (any && slot < 0) {
+    rc = io_snapshot(c, &slot);
+    if (rc) return rc;
+  }
   char name[64];
-  for (int s = 0; s < c->nsys; s++) {
-    if (state) {
+  for (int s = 0; s < c->nsys && any; s++) {
+    if (stopped(s)) continue;
+    if (flush) {
       std::snprintf(name, sizeof(name), "/md%010lu", (unsigned long)it);  // SimLoopSaver::generateId
       jobs.push_back(io_job(c, slot, kJobState, s, sys_dir(c, s) + name, io->zip));
     }
@@ -737,7 +811,21 @@ int io_before_step(mdg_ctx* c)
       jobs.push_back(io_job(c, slot, kJobXva, s, sys_dir(c, s) + name, io->zip));
     }
   }
-  io_push(c, jobs);
+  if (!jobs.empty()) io_push(c, jobs);
+  return MDG_OK;
+}
+
+// After the last step of a run: final states of systems that just ended.
+int io_run_end(mdg_ctx* c)
+{
+  if (!c->io || !c->io->on || !c->adaptive || !c->stop_final) return MDG_OK;
+  int rc = io_read_times(c);
+  if (rc) return rc;
+  std::vector<IoJob> jobs;
+  int slot = -1;
+  rc = io_finalize(c, jobs, slot);
+  if (rc) return rc;
+  if (!jobs.empty()) io_push(c, jobs);
   return MDG_OK;
 }
 
@@ -833,10 +921,14 @@ int mdg_set_output(mdg_ctx* c, const char* dir, int64_t flush_interval, double t
   io->dir = dir;
   while (io->dir.size() > 1 && io->dir.back() == '/') io->dir.pop_back();
   ::mkdir(io->dir.c_str(), 0755);
+  if ((int)io->dirs.size() != c->nsys) io->dirs.clear();
   for (int s = 0; s < c->nsys; s++) ::mkdir(sys_dir(c, s).c_str(), 0755);
   io->flush_interval = flush_interval;
-  io->traj_interval_s = (c->prm.units == MDG_UNITS_CGS) ? traj_interval : traj_interval * kFs;
+  io->ntraj = traj_interval > 0.0 ? 1 : 0;
+  io->traj_until[0] = HUGE_VAL;
+  io->traj_int[0] = (c->prm.units == MDG_UNITS_CGS) ? traj_interval : traj_interval * kFs;
   io->zip = zip;
+  io->fin.assign(c->nsys, 0);
   io->on = true;
   return MDG_OK;
 }
@@ -1073,5 +1165,437 @@ int mdg_load_state(mdg_ctx* c, const char* id_c, uint64_t iteration, int* loaded
   c->h_tags = tags;
   c->run_t0 = 0.0;
   if (loaded) *loaded = got;
+  return MDG_OK;
+}
+
+// -------------------------------------------------------------------------
+// SnapshotList (SnapshotList.hpp:38-205) captured on the device: at the top
+// of every iteration, for each system whose simTime has crossed a multiple
+// of the current interval (CustomSimLoop::isItTimeToSave and its interval
+// table, mdtrajsim/main.cpp:52-80), the PBC counters, coordinates and
+// velocities of the atoms tagged projectile or cluster
+// (SnapshotList::initSelectedAtomList) go into a per-system device list, as
+// floats in CGS like SnapshotList::AtomSnapshot.  Both kernels run inside the
+// captured step graph: no host round trip per step.
+
+struct SnapRec {        // SnapshotList::AtomSnapshot: 36 bytes, no padding
+  int32_t pc[3];
+  float p[3];
+  float v[3];
+};
+static_assert(sizeof(SnapRec) == 36, "AtomSnapshot layout");
+
+struct SnapDev {
+  int nsel = 0, nsys = 0, cap = 0, nsched = 0;
+  const int* sel = nullptr;      // [nsel] selected atoms (context indices), grouped by system
+  const int* sel_sys = nullptr;  // [nsel] their systems
+  int* cnt = nullptr;            // [nsys] snapshots taken
+  double* t = nullptr;           // [nsys * cap] their simTime (s)
+  SnapRec* rec = nullptr;        // [cap * nsel]
+  double until[4], interval[4];  // interval while simTime < until (s)
+};
+
+struct SnapState {
+  SnapDev D;
+  std::vector<int64_t> off;      // [nsys + 1] each system's selected atoms in sel
+  std::vector<uint32_t> local;   // [nsel] index within its system (atomsSelectedForSaving)
+  void* mem = nullptr;
+};
+
+MDG_HD bool snap_due(const SnapDev& D, double t, double dtp)
+{
+  double I = D.interval[D.nsched - 1];
+  for (int k = 0; k < D.nsched; k++)
+    if (t < D.until[k]) { I = D.interval[k]; break; }
+  return t == 0.0 || (long long)(t / I) != (long long)((t - dtp) / I);
+}
+
+// k-th snapshot of system s is due now (and not already taken at this time,
+// SnapshotList::getSnapshot's alreadyAccounted)
+MDG_HD int snap_slot(const SnapDev& D, int s, const double* time, const double* dt_prev, const int* stop)
+{
+  if (stop && stop[s]) return -1;
+  const double t = time[s] * kFs, dtp = dt_prev[s] * kFs;
+  if (!snap_due(D, t, dtp)) return -1;
+  const int k = D.cnt[s];
+  if (k > 0 && D.t[(size_t)s * D.cap + k - 1] == t) return -1;
+  return k;
+}
+
+__global__ void k_snap_atoms(State S, SnapDev D, const double* time, const double* dt_prev, const int* stop)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= D.nsel) return;
+  const int s = D.sel_sys[j];
+  const int k = snap_slot(D, s, time, dt_prev, stop);
+  if (k < 0 || k >= D.cap) return;
+  const int a = D.sel[j];
+  const double4 p = S.pos[a], u = S.vel[a];
+  const int4 m = S.image[a];
+  SnapRec r;
+  r.pc[0] = m.x; r.pc[1] = m.y; r.pc[2] = m.z;
+  r.p[0] = (float)(p.x * kCgsLen); r.p[1] = (float)(p.y * kCgsLen); r.p[2] = (float)(p.z * kCgsLen);
+  r.v[0] = (float)(u.x * kCgsVel); r.v[1] = (float)(u.y * kCgsVel); r.v[2] = (float)(u.z * kCgsVel);
+  D.rec[(size_t)k * D.nsel + j] = r;
+}
+
+// after k_snap_atoms (which reads the counts): record the time, count it
+__global__ void k_snap_commit(SnapDev D, const double* time, const double* dt_prev, const int* stop,
+                              unsigned int* status)
+{
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= D.nsys) return;
+  const int k = snap_slot(D, s, time, dt_prev, stop);
+  if (k < 0) return;
+  if (k >= D.cap) { atomicOr(status, ST_SNAP_OVERFLOW); return; }
+  D.t[(size_t)s * D.cap + k] = time[s] * kFs;
+  D.cnt[s] = k + 1;
+}
+
+namespace {  // declared beside free_system
+
+void snap_free(mdg_ctx* c)
+{
+  if (!c->snap) return;
+  if (c->snap->mem) cudaFree(c->snap->mem);
+  delete c->snap;
+  c->snap = nullptr;
+}
+
+int snap_capture(mdg_ctx* c)
+{
+  SnapState* Z = c->snap;
+  if (!Z) return MDG_OK;
+  const int* stop = c->stop_final ? c->d_stop : nullptr;
+  State S = c->S();
+  if (Z->D.nsel > 0)
+    LAUNCH(c, "snap_atoms", k_snap_atoms, nblk(Z->D.nsel), kThreads, S, Z->D, c->d_time, c->d_dt_prev, stop);
+  LAUNCH(c, "snap_commit", k_snap_commit, nblk(c->nsys), kThreads, Z->D, c->d_time, c->d_dt_prev, stop,
+         c->d_status);
+  return MDG_OK;
+}
+
+// Host copy of system sys's snapshots: times (s) and records [nshots][natoms].
+int snap_fetch(mdg_ctx* c, int sys, std::vector<double>& t, std::vector<SnapRec>& rec, int& natoms)
+{
+  SnapState* Z = c->snap;
+  int cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, Z->D.cnt + sys, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  natoms = (int)(Z->off[sys + 1] - Z->off[sys]);
+  t.resize(cnt);
+  rec.resize((size_t)cnt * natoms);
+  if (cnt) CK(cudaMemcpy(t.data(), Z->D.t + (size_t)sys * Z->D.cap, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<SnapRec> all((size_t)cnt * Z->D.nsel);
+  if (cnt && Z->D.nsel)
+    CK(cudaMemcpy(all.data(), Z->D.rec, all.size() * sizeof(SnapRec), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < cnt; k++)
+    for (int j = 0; j < natoms; j++) rec[(size_t)k * natoms + j] = all[(size_t)k * Z->D.nsel + Z->off[sys] + j];
+  return MDG_OK;
+}
+
+// SnapshotList::writestate (binary "snapshots.conf") or saveInText.
+int snap_write(mdg_ctx* c, int sys, const std::string& path, int zip, bool text)
+{
+  std::vector<double> t;
+  std::vector<SnapRec> rec;
+  int na = 0;
+  int rc = snap_fetch(c, sys, t, rec, na);
+  if (rc) return rc;
+  const uint32_t* loc = c->snap->local.data() + c->snap->off[sys];
+  std::string err;
+  if (!text) {
+    Rec b;
+    b.put<uint32_t>((uint32_t)na);
+    for (int j = 0; j < na; j++) b.put<uint32_t>(loc[j]);
+    b.put<uint32_t>((uint32_t)t.size());
+    for (size_t k = 0; k < t.size(); k++) {
+      b.put<double>(t[k]);
+      b.put<uint32_t>((uint32_t)na);
+      b.b.append((const char*)(rec.data() + k * na), sizeof(SnapRec) * na);
+    }
+    if (!write_blob(path, b.b.data(), b.b.size(), zip, err)) return fail(MDG_ERR_IO, err);
+    return MDG_OK;
+  }
+  // saveInText: default ostream formatting (%g)
+  std::string s;
+  for (int j = 0; j < na; j++) appendf(s, "%u ", loc[j]);
+  s += "\n";
+  for (size_t k = 0; k < t.size(); k++) {
+    appendf(s, "%g\n", t[k]);
+    for (int j = 0; j < na; j++) {
+      const SnapRec& r = rec[k * na + j];
+      appendf(s, "%d %d %d \n%g %g %g \n%g %g %g \n", r.pc[0], r.pc[1], r.pc[2], (double)r.p[0], (double)r.p[1],
+              (double)r.p[2], (double)r.v[0], (double)r.v[1], (double)r.v[2]);
+    }
+  }
+  if (!write_blob(path, s.data(), s.size(), zip, err)) return fail(MDG_ERR_IO, err);
+  return MDG_OK;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------------------
+// C ABI: snapshots, simTimeFinal, per-system output
+
+int mdg_snapshots_enable(mdg_ctx* c, int on, int capacity)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  snap_free(c);
+  c->step_cfg++;
+  if (!on) return MDG_OK;
+  if (!c->adaptive) return fail(MDG_ERR_STATE, "snapshots follow simTime: enable the adaptive time step first");
+  if (capacity <= 0 || capacity > (1 << 24)) return fail(MDG_ERR_ARG, "snapshot capacity out of range");
+  SnapState* Z = new SnapState();
+  Z->off.assign(c->nsys + 1, 0);
+  std::vector<int> sel, sys;
+  for (int s = 0; s < c->nsys; s++) {
+    const int64_t b = c->nsys > 1 ? c->h_first[s] : 0, e = c->nsys > 1 ? c->h_first[s + 1] : c->n;
+    for (int64_t i = b; i < e; i++)
+      if (c->h_tags[i] & ((1u << 2) | (1u << 5))) {  // ATOMTAG_PROJECTILE | ATOMTAG_CLUSTER
+        sel.push_back((int)i);
+        sys.push_back(s);
+        Z->local.push_back((uint32_t)(i - b));
+      }
+    Z->off[s + 1] = (int64_t)sel.size();
+  }
+  SnapDev& D = Z->D;
+  D.nsel = (int)sel.size();
+  D.nsys = c->nsys;
+  D.cap = capacity;
+  // CustomSimLoop's intervals (mdtrajsim/main.cpp:62-80), in its own expressions
+  D.nsched = 3;
+  D.until[0] = 2.0 * 1e-12;
+  D.until[1] = 4.0 * 1e-12;
+  D.until[2] = HUGE_VAL;
+  D.interval[0] = 5e-16 * 5 * 4;
+  D.interval[1] = 5e-16 * 25 * 4;
+  D.interval[2] = 5e-16 * 50 * 4;
+  const size_t b_sel = 2 * sizeof(int) * (size_t)D.nsel, b_cnt = sizeof(int) * (size_t)c->nsys,
+               b_t = sizeof(double) * (size_t)c->nsys * capacity, b_rec = sizeof(SnapRec) * (size_t)capacity * D.nsel;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  char* m = nullptr;
+  if (cudaMalloc((void**)&m, up(b_sel) + up(b_cnt) + up(b_t) + up(b_rec) + 256) != cudaSuccess) {
+    delete Z;
+    return fail(MDG_ERR_CUDA, "cudaMalloc (snapshots)");
+  }
+  Z->mem = m;
+  int* dsel = (int*)m;
+  D.sel = dsel;
+  D.sel_sys = dsel + D.nsel;
+  D.cnt = (int*)(m + up(b_sel));
+  D.t = (double*)(m + up(b_sel) + up(b_cnt));
+  D.rec = (SnapRec*)(m + up(b_sel) + up(b_cnt) + up(b_t));
+  c->snap = Z;
+  if (D.nsel) {
+    CK(cudaMemcpy(dsel, sel.data(), D.nsel * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dsel + D.nsel, sys.data(), D.nsel * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemset(D.cnt, 0, b_cnt));
+  return MDG_OK;
+}
+
+int mdg_snapshots_set_schedule(mdg_ctx* c, int n, const double* until, const double* interval)
+{
+  if (!c || !c->snap) return fail(MDG_ERR_STATE, "snapshots are not enabled");
+  if (n < 1 || n > 4 || !until || !interval) return fail(MDG_ERR_ARG, "1 to 4 schedule entries");
+  const double tc = (c->prm.units == MDG_UNITS_CGS) ? 1.0 : kFs;  // time unit -> s
+  for (int k = 0; k < n; k++) {
+    if (!(interval[k] > 0.0)) return fail(MDG_ERR_ARG, "snapshot intervals must be positive");
+    c->snap->D.until[k] = until[k] * tc;
+    c->snap->D.interval[k] = interval[k] * tc;
+  }
+  c->snap->D.nsched = n;
+  c->step_cfg++;
+  return MDG_OK;
+}
+
+int mdg_snapshots_count(mdg_ctx* c, int sys, int* nshots, int* natoms)
+{
+  int rc = check_sys(c, sys);
+  if (rc) return rc;
+  if (!c->snap) return fail(MDG_ERR_STATE, "snapshots are not enabled");
+  int cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, c->snap->D.cnt + sys, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  if (nshots) *nshots = cnt;
+  if (natoms) *natoms = (int)(c->snap->off[sys + 1] - c->snap->off[sys]);
+  return MDG_OK;
+}
+
+int mdg_snapshots_get(mdg_ctx* c, int sys, double* times, uint32_t* indices, int32_t* pbc_count, float* pos,
+                      float* vel)
+{
+  int rc = check_sys(c, sys);
+  if (rc) return rc;
+  if (!c->snap) return fail(MDG_ERR_STATE, "snapshots are not enabled");
+  std::vector<double> t;
+  std::vector<SnapRec> rec;
+  int na = 0;
+  rc = snap_fetch(c, sys, t, rec, na);
+  if (rc) return rc;
+  const double tc = (c->prm.units == MDG_UNITS_CGS) ? 1.0 : 1.0 / kFs;
+  for (size_t k = 0; k < t.size(); k++)
+    if (times) times[k] = t[k] * tc;
+  if (indices)
+    for (int j = 0; j < na; j++) indices[j] = c->snap->local[c->snap->off[sys] + j];
+  for (size_t q = 0; q < rec.size(); q++)
+    for (int a = 0; a < 3; a++) {
+      if (pbc_count) pbc_count[3 * q + a] = rec[q].pc[a];
+      if (pos) pos[3 * q + a] = rec[q].p[a];
+      if (vel) vel[3 * q + a] = rec[q].v[a];
+    }
+  return MDG_OK;
+}
+
+int mdg_snapshots_write(mdg_ctx* c, int sys, const char* path, int zip, int text)
+{
+  int rc = check_sys(c, sys);
+  if (!rc) rc = check_zip(zip);
+  if (rc) return rc;
+  if (!c->snap) return fail(MDG_ERR_STATE, "snapshots are not enabled");
+  if (!path || !*path) return fail(MDG_ERR_ARG, "empty file name");
+  return snap_write(c, sys, path, zip, text != 0);
+}
+
+// SnapshotList::loadstate: earlier snapshots of system sys, so that a resumed
+// trajectory appends to them.
+int mdg_snapshots_load(mdg_ctx* c, int sys, const char* path)
+{
+  int rc = check_sys(c, sys);
+  if (rc) return rc;
+  if (!c->snap) return fail(MDG_ERR_STATE, "snapshots are not enabled");
+  std::string b, err;
+  const int k = read_blob(path, b, err);
+  if (k < 0) return fail(MDG_ERR_IO, err);
+  if (k == 0) return fail(MDG_ERR_ARG, std::string("no snapshot list ") + path);
+  SnapState* Z = c->snap;
+  const int na = (int)(Z->off[sys + 1] - Z->off[sys]);
+  size_t o = 0;
+  auto get = [&](void* dst, size_t n) {
+    if (o + n > b.size()) return false;
+    std::memcpy(dst, b.data() + o, n);
+    o += n;
+    return true;
+  };
+  uint32_t nsel = 0, nshots = 0;
+  if (!get(&nsel, 4) || (int)nsel != na) return fail(MDG_ERR_ARG, "snapshot list: selected atoms differ");
+  for (int j = 0; j < na; j++) {
+    uint32_t v = 0;
+    if (!get(&v, 4) || v != Z->local[Z->off[sys] + j]) return fail(MDG_ERR_ARG, "snapshot list: selected atoms differ");
+  }
+  if (!get(&nshots, 4)) return fail(MDG_ERR_ARG, "snapshot list: truncated");
+  if ((int)nshots > Z->D.cap) return fail(MDG_ERR_CAPACITY, "snapshot list larger than the capacity");
+  std::vector<double> t(nshots);
+  std::vector<SnapRec> all((size_t)nshots * Z->D.nsel);
+  if (nshots && Z->D.nsel)
+    CK(cudaMemcpy(all.data(), Z->D.rec, all.size() * sizeof(SnapRec), cudaMemcpyDeviceToHost));
+  for (uint32_t q = 0; q < nshots; q++) {
+    uint32_t sz = 0;
+    if (!get(&t[q], 8) || !get(&sz, 4) || (int)sz != na) return fail(MDG_ERR_ARG, "snapshot list: truncated");
+    for (int j = 0; j < na; j++)
+      if (!get(&all[(size_t)q * Z->D.nsel + Z->off[sys] + j], sizeof(SnapRec)))
+        return fail(MDG_ERR_ARG, "snapshot list: truncated");
+  }
+  if (nshots && Z->D.nsel)
+    CK(cudaMemcpy(Z->D.rec, all.data(), all.size() * sizeof(SnapRec), cudaMemcpyHostToDevice));
+  if (nshots) CK(cudaMemcpy(Z->D.t + (size_t)sys * Z->D.cap, t.data(), nshots * sizeof(double), cudaMemcpyHostToDevice));
+  const int cnt = (int)nshots;
+  CK(cudaMemcpy(Z->D.cnt + sys, &cnt, sizeof(int), cudaMemcpyHostToDevice));
+  return MDG_OK;
+}
+
+int mdg_set_stop_at_time_final(mdg_ctx* c, int on)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  c->stop_final = on != 0;
+  if (c->n && c->d_stop) CK(cudaMemset(c->d_stop, 0, c->nsys * sizeof(int)));
+  c->step_cfg++;
+  return MDG_OK;
+}
+
+int mdg_run_until_final(mdg_ctx* c, int64_t max_steps, int64_t* steps, int* finished)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (!c->adaptive || !c->stop_final)
+    return fail(MDG_ERR_STATE, "needs the adaptive time step and mdg_set_stop_at_time_final");
+  int64_t done = 0;
+  int all = 0;
+  std::vector<int> st((size_t)c->nsys);
+  while (done < max_steps) {
+    const int chunk = (int)std::min<int64_t>(16, max_steps - done);
+    int rc = run_steps(c, chunk, 0.5, nullptr, nullptr, done == 0);
+    if (rc) return rc;
+    done += chunk;
+    CK(cudaMemcpyAsync(st.data(), c->d_stop, c->nsys * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    rc = read_status(c);
+    if (rc) return rc;
+    all = 1;
+    for (int v : st) all = all && v;
+    if (all) break;
+  }
+  if (steps) *steps = done;
+  if (finished) *finished = all;
+  return io_wait(c);
+}
+
+int mdg_set_time(mdg_ctx* c, const double* sim_time, const double* dt)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (!sim_time || !dt) return fail(MDG_ERR_ARG, "null argument");
+  const double tc = (c->prm.units == MDG_UNITS_CGS) ? 1.0 / kFs : 1.0;  // time unit -> fs
+  std::vector<double> t(c->nsys), d(c->nsys);
+  for (int s = 0; s < c->nsys; s++) {
+    if (!(dt[s] > 0.0) || !std::isfinite(sim_time[s])) return fail(MDG_ERR_ARG, "bad time or dt");
+    t[s] = sim_time[s] * tc;
+    d[s] = std::min(std::max(dt[s] * tc, 1e-5), 0.5);
+  }
+  CK(cudaMemcpy(c->d_time, t.data(), c->nsys * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_dt, d.data(), c->nsys * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_dt_prev, d.data(), c->nsys * sizeof(double), cudaMemcpyHostToDevice));
+  c->time_s = t[0] * kFs;
+  c->dt_s = c->dt_prev_s = d[0] * kFs;
+  return MDG_OK;
+}
+
+int mdg_set_output_dirs(mdg_ctx* c, const char* const* dirs)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  IoState* io = nullptr;
+  int rc = io_get(c, &io);
+  if (!rc) rc = io_wait(c);
+  if (rc) return rc;
+  io->dirs.clear();
+  if (!dirs) return MDG_OK;
+  for (int s = 0; s < c->nsys; s++) {
+    if (!dirs[s] || !*dirs[s]) return fail(MDG_ERR_ARG, "empty directory name");
+    io->dirs.push_back(dirs[s]);
+    ::mkdir(dirs[s], 0755);
+  }
+  return MDG_OK;
+}
+
+int mdg_set_traj_schedule(mdg_ctx* c, int n, const double* until, const double* interval)
+{
+  if (!c || !c->io || !c->io->on) return fail(MDG_ERR_STATE, "call mdg_set_output first");
+  if (n < 0 || n > 4 || (n && (!until || !interval))) return fail(MDG_ERR_ARG, "0 to 4 schedule entries");
+  const double tc = (c->prm.units == MDG_UNITS_CGS) ? 1.0 : kFs;
+  for (int k = 0; k < n; k++) {
+    if (!(interval[k] > 0.0)) return fail(MDG_ERR_ARG, "trajectory intervals must be positive");
+    c->io->traj_until[k] = until[k] * tc;
+    c->io->traj_int[k] = interval[k] * tc;
+  }
+  c->io->ntraj = n;
+  return MDG_OK;
+}
+
+int mdg_set_images(mdg_ctx* c, const int32_t* image)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (!image) return fail(MDG_ERR_ARG, "null argument");
+  std::vector<int4> h(c->n);
+  for (int i = 0; i < c->n; i++) h[i] = make_int4(image[3 * i], image[3 * i + 1], image[3 * i + 2], 0);
+  CK(cudaMemcpy(c->image, h.data(), c->n * sizeof(int4), cudaMemcpyHostToDevice));
   return MDG_OK;
 }

@@ -522,10 +522,17 @@ struct StepDev {
   double4* acc_ntb;               // per atom Atom::an_no_tb, updated in the bath branch only
   double* eb;                     // per atom running sum of Check::energyTransferredFromBath
                                   // (SimLoop.cxx:362-385); both null without a bath
+  const int* stop;                // per system: reached simTimeFinal (SimLoop's loop condition),
+                                  // steps of dt 0 leave it unchanged; or null
 };
 
 MDG_HD int sys_of(const State& S, int i) { return S.sys ? S.sys[i] : 0; }
-MDG_HD double step_dt(const StepDev& P, const State& S, int i) { return P.d_dt ? P.d_dt[sys_of(S, i)] : P.dt; }
+MDG_HD double step_dt(const StepDev& P, const State& S, int i)
+{
+  if (!P.d_dt) return P.dt;
+  const int s = sys_of(S, i);
+  return (P.stop && P.stop[s]) ? 0.0 : P.d_dt[s];
+}
 
 // SimLoop::thermalBathShouldBeApplied (SimLoop.hpp:164-191) at atom i's
 // current coordinates.

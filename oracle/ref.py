@@ -68,6 +68,8 @@ def lib():
         L.ref_set_tags.argtypes = [vp, ub]
         L.ref_get_loop.argtypes = [vp, dp]
         L.ref_set_output.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, ctypes.c_double]
+        L.ref_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_impact_sequence.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
         L.ref_tables.restype = ctypes.c_long
         L.ref_tables.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_long]
         L.ref_spline_eval.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
@@ -184,6 +186,13 @@ class RefSystem:
         return {"pos": pos, "vel": vel, "image": img, "epot": ep, "etot": et, "e0": float(e0[0]), "times": ts}
 
 
+def impact_sequence(potset: int, base_id: str, ionpos_path: str, workdir: str, start: int = 0):
+    """mdtrajsim's impact-sequence mode (main.cpp:113-345) on the reference,
+    with this harness's potential set."""
+    _check(lib().ref_impact_sequence(potset, os.fsencode(base_id), os.fsencode(ionpos_path), os.fsencode(workdir),
+                                     start))
+
+
 def set_zip(mode: int):
     """Compression of the reference's files: 0 plain, 1 .gz, 2 .xz."""
     _check(lib().ref_set_zip(mode))
@@ -243,6 +252,12 @@ def _set_output(self, dir, flush_interval: int = 0, traj_interval_fs: float = 0.
                                 float(traj_interval_fs)))
 
 
+def _set_time(self, time_fs: float, time_final_fs: float, dt_fs: float):
+    """SimLoop::simTime, simTimeFinal, dt."""
+    _check(lib().ref_set_time(self.h, time_fs, time_final_fs, dt_fs))
+
+
+RefSystem.set_time = _set_time
 RefSystem.set_output = _set_output
 RefSystem.write_state = _write_state
 RefSystem.write_xva = _write_xva

@@ -28,6 +28,9 @@
 
 #include <mdtk/SimLoop.hpp>
 #include <mdtk/SimLoopSaver.hpp>
+#include <mdtk/SnapshotList.hpp>
+#include <climits>
+#include <sys/stat.h>
 #include <mdtk/potentials/manybody/AIREBO/REBO.hpp>
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_LJ.hpp>
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_ETors.hpp>
@@ -56,9 +59,38 @@ public:
   bool adaptive;  // leave dt to SimLoop's own adaptation (SimLoop.cxx:405-416)
   int max_iter;   // adaptive runs stop after this many iterations
   std::vector<double> epot_log, etot_log, t_log, dt_log;
-  FixedDtLoop() : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0), adaptive(false), max_iter(0) {}
+  // mdtrajsim's CustomSimLoop (applications/mdtrajsim/main.cpp:36-90): its
+  // SnapshotList and its doBeforeIteration, restated here because the
+  // application's own potential set (applications/common.h:36-77) carries
+  // metal potentials outside this path
+  bool trajsim;
+  SnapshotList snapshotList;
+  FixedDtLoop()
+    : SimLoop(), fixed_dt(0.5 * fs), ekin_before(0.0), adaptive(false), max_iter(0), trajsim(false), snapshotList()
+  {
+  }
+  bool isItTimeToSave(Float interval)
+  {
+    return (simTime == 0.0 || int(simTime / interval) != int((simTime - dt_prev) / interval));
+  }
+  void trajsimBeforeIteration()
+  {
+    if (simTime < 2.0 * ps) simTimeSaveTrajInterval = 1.0 * ps;
+    else simTimeSaveTrajInterval = 5.0 * ps;
+    if (simTime < 2.0 * ps) {
+      if (isItTimeToSave(5e-16 * 5 * 4)) snapshotList.getSnapshot(*this);
+    } else {
+      if (simTime < 4.0 * ps) {
+        if (isItTimeToSave(5e-16 * 25 * 4)) snapshotList.getSnapshot(*this);
+      } else {
+        if (isItTimeToSave(5e-16 * 50 * 4)) snapshotList.getSnapshot(*this);
+      }
+    }
+    if (iteration % iterationFlushStateInterval == 0 && iteration != 0) snapshotList.writestate();
+  }
   virtual void doBeforeIteration()
   {
+    if (trajsim) trajsimBeforeIteration();
     t_log.push_back(wall_now());
     if (!adaptive) dt = fixed_dt;
     dt_log.push_back(dt / fs);
@@ -841,6 +873,114 @@ int ref_set_output(void* h, const char* dir, long flush_interval, double traj_in
   c->out_dir = dir ? dir : "";
   c->flush_interval = flush_interval > 0 ? flush_interval : 1000000;
   c->traj_interval_fs = traj_interval_fs;
+  return 0;
+}
+}  // extern "C"
+
+extern "C" {
+/* mdtrajsim's impact-sequence mode (applications/mdtrajsim/main.cpp:295-345)
+ * with its runTraj (main.cpp:113-180), on this harness's potential set:
+ * load the base state, and for each (x, y) of ionpos.bin from impact
+ * `start` on, in workdir/%08d: place the last atom (the projectile) there,
+ * record ionpos_used.bin/.txt, write the state, run SimLoop (adaptive dt)
+ * to the base's simTimeFinal with CustomSimLoop's snapshots and intervals,
+ * write the final state, snapshots.conf and completed.ok, and keep only the
+ * last state.  Files go through yaatk's streams (compression as ref_set_zip).
+ * Directory changes do not redirect the standard streams (yaatk::ChDir's
+ * stdout.txt/stderr.txt logs are not made). */
+int ref_impact_sequence(int potset, const char* base_id, const char* ionpos_path, const char* workdir, int start)
+{
+  char cwd[4096] = {0};
+  if (!getcwd(cwd, sizeof(cwd))) { g_last_error = "getcwd"; return -1; }
+  RefCtx* base = (RefCtx*)ref_create(potset, 1, 0);
+  if (!base) return -1;
+  int rc = 0;
+  try {
+    mdtk::SimLoopSaver mds(base->loop);
+    int got = mds.load(base_id);
+    REQUIRE(got & mdtk::SimLoopSaver::LOADED_R);
+    double bombX, bombY;
+    yaatk::binary_ifstream ionpos_bin(ionpos_path);
+    int recordLength = ionpos_bin.getDataLength();
+    REQUIRE(recordLength % (sizeof(bombX) + sizeof(bombY)) == 0);
+    int impactCount = recordLength / (sizeof(bombX) + sizeof(bombY));
+    for (int impact = 0; impact < impactCount; ++impact) {
+      YAATK_BIN_READ(ionpos_bin, bombX);
+      YAATK_BIN_READ(ionpos_bin, bombY);
+      Atom& projectile = base->loop.atoms.back();
+      projectile.coords.x = bombX;
+      projectile.coords.y = bombY;
+      if (impact < start) continue;
+      char name[64];
+      sprintf(name, "%08d", impact);
+      const std::string dir = std::string(workdir) + "/" + name;
+      ::mkdir(dir.c_str(), 0755);
+      if (chdir(dir.c_str()) != 0) throw Exception("cannot enter " + dir);
+      if (yaatk::exists("completed.ok") || yaatk::exists("completed.error")) {
+        if (chdir(cwd) != 0) throw Exception("chdir");
+        continue;
+      }
+      {
+        yaatk::binary_ofstream ionpos_used_bin("ionpos_used.bin");
+        yaatk::text_ofstream ionpos_used_txt("ionpos_used.txt");
+        YAATK_BIN_WRITE(ionpos_used_bin, bombX);
+        YAATK_BIN_WRITE(ionpos_used_bin, bombY);
+        ionpos_used_txt << bombX << " " << bombY << "\n";
+        ionpos_used_bin.close();
+        ionpos_used_txt.close();
+      }
+      base->loop.simTimeSaveTrajInterval = 1e6 * ps;
+      mds.write();
+      {
+        // runTraj
+        RefCtx* t = (RefCtx*)ref_create(potset, 1, 0);
+        if (!t) throw Exception(g_last_error);
+        try {
+          mdtk::SimLoopSaver tm(t->loop);
+          if (tm.listIterations().size() > 0) tm.loadIterationLatest();
+          if (yaatk::exists("snapshots.conf")) t->loop.snapshotList.loadstate();
+          t->loop.iterationFlushStateInterval = 1000;
+          t->loop.trajsim = true;
+          t->loop.adaptive = true;
+          t->loop.max_iter = INT_MAX;
+          t->loop.preventFileOutput = false;
+          t->loop.execute();
+          tm.write();
+          t->loop.snapshotList.writestate();
+          if (t->loop.simTime >= t->loop.simTimeFinal) {
+            yaatk::text_ofstream fo2("completed.ok");
+            fo2.close();
+            tm.removeIterations();
+          }
+        } catch (...) {
+          delete t;
+          throw;
+        }
+        delete t;
+      }
+      mds.removeIterations(false, true);
+      if (chdir(cwd) != 0) throw Exception("chdir");
+    }
+    ionpos_bin.close();
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    rc = -1;
+    if (chdir(cwd) != 0) rc = -1;
+  }
+  delete base;
+  return rc;
+}
+}  // extern "C"
+
+extern "C" {
+/* SimLoop::simTime, simTimeFinal and dt (fs), e.g. of a base state to write. */
+int ref_set_time(void* h, double time_fs, double time_final_fs, double dt_fs)
+{
+  RefCtx* c = (RefCtx*)h;
+  c->loop.simTime = time_fs * fs;
+  c->loop.simTimeFinal = time_final_fs * fs;
+  c->loop.dt = dt_fs * fs;
+  c->loop.dt_prev = dt_fs * fs;
   return 0;
 }
 }  // extern "C"
