@@ -46,6 +46,11 @@ typedef struct mdg_ctx mdg_ctx;
 #define MDG_POT_AIREBO_LJ 2   /* AIREBO LJ term (AIREBO/AIREBO_LJ.cxx); needs MDG_POT_REBO */
 #define MDG_POT_ETORS 4       /* AIREBO torsion (AIREBO/AIREBO_ETors.cxx) */
 #define MDG_POT_BRENNER 8     /* first-generation Brenner (Brenner/Brenner.cxx) */
+#define MDG_POT_METAL 16      /* the metal and ion potentials of applications/common.h:36-77:
+                                 FBZL (pairwise/FBZL.cxx: Ar, Xe ions with every element),
+                                 FLJ (pairwise/FLJ.cxx: H, C with Cu, Au) and Ackland
+                                 (manybody/Ackland/Ackland.cxx: Cu, Ag, Au); needed for any
+                                 atom other than H and C */
 #define MDG_POT_AIREBO (MDG_POT_REBO | MDG_POT_AIREBO_LJ | MDG_POT_ETORS)
 
 /* ---- units at this ABI ---- */
@@ -105,6 +110,11 @@ const char* mdg_last_error(void);
 /* Launch all work on this CUDA stream (cudaStream_t passed as void*; NULL =
  * the context's own stream). */
 int mdg_set_stream(mdg_ctx* ctx, void* stream);
+
+/* Elements (z): H 1, C 6 (REBO, AIREBO, Brenner); Cu 29, Ag 47, Au 79 and
+ * the ions Ar 18, Xe 54 (MDG_POT_METAL).  REBO and AIREBO see hydrocarbon
+ * pairs only; the metal potentials every pair with a metal or ion atom.
+ * mdg_compute's e_terms[3] is the metal and ion energy. */
 
 /* Load an atom set (AtomsArray with its PBC, AtomsContainer.hpp:31-104, plus
  * AtomsArray::prepareForSimulatation AtomsContainer.cxx:107-123: positions are

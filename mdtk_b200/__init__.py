@@ -25,6 +25,7 @@ POT_REBO = 1
 POT_AIREBO_LJ = 2
 POT_ETORS = 4
 POT_BRENNER = 8
+POT_METAL = 16  # FBZL, FLJ, Ackland (applications/common.h:36-77): Cu, Ag, Au, Ar, Xe
 POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
 
 # parameters the adjoint differentiates (include/mdg.h MDG_PARAM_*)

@@ -31,8 +31,16 @@ EV_PER_AMU_A2FS2 = EV_ERG / AMU_G * 1e16 / 1e30
 MASS = {6: 12.0, 1: 1.0}
 
 
+# Atom::setAttributesByElementID (mdtk/Atom.hpp:100-115): amu by atomic number
+MASS_AMU = {1: 1.0, 6: 12.0, 29: 63.546, 47: 107.868, 79: 196.967, 18: 39.948, 54: 131.293}
+
+
 def masses(z: np.ndarray) -> np.ndarray:
-    return np.where(np.asarray(z) == 6, 12.0, 1.0)
+    z = np.asarray(z)
+    out = np.empty(z.shape, float)
+    for k, m in MASS_AMU.items():
+        out[z == k] = m
+    return out
 
 
 def temperature(z, vel, fixed=None) -> float:
@@ -350,3 +358,36 @@ def relax_hot(s: Dict[str, np.ndarray], steps: int, temp_k: float, dt: float, po
     out["pos"] = pos
     out["vel"] = v
     return out
+
+
+# fcc lattice constants of the Ackland potential's metals (Ackland.cxx:330, 352, 374)
+FCC_A = {29: 3.615, 47: 4.086, 79: 4.078}
+
+
+def fcc(z: int, nx: int, ny: int = None, nz: int = None, a: float = None, temp_k: float = 0.0,
+        disp_sigma: float = 0.0, pbc=(1, 1, 1), seed: int = 0) -> Dict[str, np.ndarray]:
+    """An fcc metal crystal (Cu 29, Ag 47, Au 79), nx*ny*nz cubic cells of 4 atoms."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    a = FCC_A[z] if a is None else a
+    basis = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]], float) + 0.25
+    cells = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = ((cells[:, None, :] + basis[None, :, :]).reshape(-1, 3)) * a
+    rng = np.random.default_rng(seed)
+    if disp_sigma > 0:
+        pos = pos + rng.normal(scale=disp_sigma, size=pos.shape)
+    box = np.array([nx, ny, nz], float) * a
+    pos = np.where(np.asarray(pbc)[None, :] != 0, np.mod(pos, box), pos)
+    zz = np.full(len(pos), z, np.int32)
+    vel = thermal_velocities(zz, temp_k, rng)
+    return _system(zz, pos, vel, box, list(pbc))
+
+
+def add_atoms(s: Dict[str, np.ndarray], z, pos, vel=None, fixed=None) -> Dict[str, np.ndarray]:
+    """s with more atoms appended (a projectile, an adsorbate)."""
+    z = np.atleast_1d(np.asarray(z, np.int32))
+    pos = np.asarray(pos, float).reshape(-1, 3)
+    vel = np.zeros_like(pos) if vel is None else np.asarray(vel, float).reshape(-1, 3)
+    fx = np.zeros(len(z), np.uint8) if fixed is None else np.asarray(fixed, np.uint8)
+    return _system(np.concatenate([s["z"], z]), np.concatenate([s["pos"], pos]), np.concatenate([s["vel"], vel]),
+                   s["box"], s["pbc"], np.concatenate([s["fixed"], fx]))

@@ -284,6 +284,7 @@ int adj_check(mdg_ctx* c)
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (c->prm.precision != MDG_PREC_FP64) return fail(MDG_ERR_ARG, "the adjoint runs on FP64 contexts");
   if (c->prm.potentials & MDG_POT_BRENNER) return fail(MDG_ERR_ARG, "the adjoint covers REBO, the LJ term and torsion");
+  if (c->has_list[2]) return fail(MDG_ERR_ARG, "the adjoint covers hydrocarbons (no metal or ion atoms)");
   if (c->nsys > 1) return fail(MDG_ERR_ARG, "the adjoint runs on single-system contexts");
   if (c->prm.units != MDG_UNITS_AEVFS) return fail(MDG_ERR_ARG, "the adjoint works in Angstrom / eV / fs units");
   if (c->tb_geom || c->adaptive)

@@ -45,6 +45,9 @@ constexpr int kRedBlocks = 120;
 constexpr double kAo = 1e-8, kEv = 1.6021e-12, kFs = 1e-15;
 
 inline int nblk(int n, int t = kThreads) { return (n + t - 1) / t; }
+}  // namespace
+#include "mdg_metal.cuh"
+namespace {
 
 // ---------------------------------------------------------------- kernels
 
@@ -58,20 +61,24 @@ __device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, do
 // Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
 // of the step) and, per block, the two largest displacements since each
 // list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
-__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, int nl, double* part)
+__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, int mask, double* part)
 {
-  __shared__ double s1[2][kThreads / 32], s2[2][kThreads / 32];
+  __shared__ double s1[3][kThreads / 32], s2[3][kThreads / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
+  double d1[3] = {0.0, 0.0, 0.0}, d2[3] = {0.0, 0.0, 0.0};
   for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
     if (do_pos) verlet_pos_atom(S, step_dt(P, S, a), a);
-    for (int l = 0; l < nl; l++) {
-      const double d = disp_atom(S, l == 0 ? L0 : L1, a);
+#pragma unroll
+    for (int l = 0; l < 3; l++) {
+      if (!((mask >> l) & 1)) continue;
+      const double d = disp_atom(S, l == 0 ? L0 : (l == 1 ? L1 : L2), a);
       if (d >= d1[l]) { d2[l] = d1[l]; d1[l] = d; }
       else if (d >= d2[l]) d2[l] = d;
     }
   }
-  for (int l = 0; l < nl; l++) {
+#pragma unroll
+  for (int l = 0; l < 3; l++) {
+    if (!((mask >> l) & 1)) continue;
     for (int o = 16; o > 0; o >>= 1) {
       const double u1 = __shfl_down_sync(0xffffffffu, d1[l], o), u2 = __shfl_down_sync(0xffffffffu, d2[l], o);
       top2_merge(d1[l], d2[l], u1, u2);
@@ -82,7 +89,7 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
     }
   }
   __syncthreads();
-  if (threadIdx.x < nl) {
+  if (threadIdx.x < 3 && ((mask >> threadIdx.x) & 1)) {
     const int l = threadIdx.x;
     double t1 = 0.0, t2 = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) top2_merge(t1, t2, s1[l][w], s2[l][w]);
@@ -627,11 +634,11 @@ __global__ void k_lj_special_pair(const ReboParams* P, const TB* Tb, LJParams LP
   }
 }
 
-__global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad)
+__global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, const double4* gm)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
-  V3 g = gather_atom(B, O, a, with_lj, nullptr);
+  V3 g = gather_atom(B, O, a, with_lj, gm);
   if (with_lj) g += mid_gather_atom(B, Tk, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
 }
@@ -640,11 +647,11 @@ __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, d
 // gather reads bond records and unit vectors, never positions, so each atom's
 // velocity, acceleration and wrap follow its own gradient at once.
 __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, StepDev P,
-                            double* ekin, unsigned int* status)
+                            double* ekin, const double4* gm, unsigned int* status)
 {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
-  V3 g = gather_atom(B, O, a, with_lj, nullptr);
+  V3 g = gather_atom(B, O, a, with_lj, gm);
   if (with_lj) g += mid_gather_atom(B, Tk, a);
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
   if (P.ekin_pre) {
@@ -778,8 +785,9 @@ __global__ void k_ekin(State S, double* ekin)
 
 // Deterministic sums of up to 4 per-atom arrays: fixed grid, fixed order.
 struct RedArgs {
-  const double* a[4];
-  int narr, n;
+  const double* a[5];
+  int slot[5];  // output slot of each array (the metal energies join another slot or take their own)
+  int narr, nout, n;
 };
 __global__ void k_reduce_partial(RedArgs R, double* part)
 {
@@ -796,14 +804,19 @@ __global__ void k_reduce_partial(RedArgs R, double* part)
   }
   if (threadIdx.x == 0) part[which * gridDim.x + blockIdx.x] = sh[0];
 }
-// out[w] = sum of partials; also a finiteness check on the gradient sum
-__global__ void k_reduce_final(const double* part, int nparts, int narr, double* out, int slot_stride, int slot,
+// out[w] = sum of the partials of the arrays of slot w (in array order)
+__global__ void k_reduce_final(const double* part, int nparts, RedArgs R, double* out, int slot_stride, int slot,
                                unsigned int* status)
 {
   int w = threadIdx.x;
-  if (w >= narr) return;
+  if (w >= R.nout) return;
   double s = 0.0;
-  for (int q = 0; q < nparts; q++) s += part[w * nparts + q];
+  for (int k = 0; k < R.narr; k++) {
+    if (R.slot[k] != w) continue;
+    double t = 0.0;
+    for (int q = 0; q < nparts; q++) t += part[k * nparts + q];
+    s = (k == w) ? t : s + t;
+  }
   out[slot * slot_stride + w] = s;
   if (!isfinite(s)) atomicOr(status, ST_NONFINITE);
 }
@@ -812,7 +825,7 @@ __global__ void k_reduce_final(const double* part, int nparts, int narr, double*
 // thread sums a strided share of the system's atoms, then a fixed tree
 // (deterministic).  out[4 s + {0,1,2,3}] = REBO, LJ, torsion, kinetic.
 __global__ void k_sys_energy(const int64_t* first, int64_t n, const double* er, const double* el, const double* et,
-                             const double* ek, double* out, unsigned int* status)
+                             const double* ek, const double* em, double* out, unsigned int* status)
 {
   __shared__ double sh[4][kThreads];
   const int sy = blockIdx.x;
@@ -823,6 +836,7 @@ __global__ void k_sys_energy(const int64_t* first, int64_t n, const double* er, 
     acc[0] += er[i];
     acc[1] += el[i];
     acc[2] += et[i];
+    if (em) acc[2] += em[i];  // metal and ion energies join the torsion slot in the totals
     acc[3] += ek[i];
   }
   for (int q = 0; q < 4; q++) sh[q][threadIdx.x] = acc[q];
@@ -914,9 +928,9 @@ struct mdg_ctx {
   int* d_sys = nullptr;
   Box* d_boxes = nullptr;
   int64_t* d_first = nullptr;
-  int4* d_snc[2] = {nullptr, nullptr};
-  double4* d_slo[2] = {nullptr, nullptr};
-  double4* d_scs[2] = {nullptr, nullptr};
+  int4* d_snc[3] = {nullptr, nullptr, nullptr};
+  double4* d_slo[3] = {nullptr, nullptr, nullptr};
+  double4* d_scs[3] = {nullptr, nullptr, nullptr};
   double unit_len = 1.0, unit_vel = 1.0, unit_e = 1.0, unit_grad = 1.0;
 
   // state
@@ -927,13 +941,18 @@ struct mdg_ctx {
   bool acc_valid = false;
 
   // lists: 0 = REBO range, 1 = LJ range
-  NList nl[2];
-  Grid grid[2];
-  int* d_need = nullptr;   // [2]
-  int* d_force = nullptr;  // [2]
+  NList nl[3];             // 0 REBO range, 1 AIREBO LJ range, 2 metal and ion pairs
+  Grid grid[3];
+  int* d_need = nullptr;   // [3]
+  int* d_force = nullptr;  // [3]
   double* d_part = nullptr;
-  double rcut[2] = {0, 0};
-  bool has_list[2] = {false, false};
+  double rcut[3] = {0, 0, 0};
+  bool has_list[3] = {false, false, false};
+  // metal and ion potentials (FBZL, FLJ, Ackland)
+  MetalParams* d_metal = nullptr;
+  double* d_fp = nullptr;     // [n] dF/drho of the embedding
+  double* d_em = nullptr;     // [n] metal and ion energies per atom
+  double4* d_gm = nullptr;    // [n] their gradient
 
   // bonds
   int mb = 16;
@@ -1176,7 +1195,7 @@ void free_system(mdg_ctx* c)
                   c->e_kin, c->d_part, c->d_red_part, c->d_elog};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  for (int l = 0; l < 2; l++) {
+  for (int l = 0; l < 3; l++) {
     void* q[] = {c->nl[l].cnt, c->nl[l].list, c->nl[l].pos0, c->grid[l].ccount, c->grid[l].cstart,
                  c->grid[l].ccursor, c->grid[l].catoms};
     for (void* p : q)
@@ -1197,14 +1216,16 @@ void free_system(mdg_ctx* c)
     if (p) cudaFree(p);
   std::memset(&c->cij, 0, sizeof(c->cij));
   std::memset(&c->spc, 0, sizeof(c->spc));
-  void* sq[] = {c->d_sys, c->d_boxes, c->d_first, c->d_snc[0], c->d_snc[1], c->d_slo[0], c->d_slo[1],
-                c->d_scs[0], c->d_scs[1]};
+  void* sq[] = {c->d_sys, c->d_boxes, c->d_first, c->d_snc[0], c->d_snc[1], c->d_snc[2], c->d_slo[0], c->d_slo[1],
+                c->d_slo[2], c->d_scs[0], c->d_scs[1], c->d_scs[2], c->d_fp, c->d_em, c->d_gm};
   for (void* p : sq)
     if (p) cudaFree(p);
   c->d_sys = nullptr;
   c->d_boxes = nullptr;
   c->d_first = nullptr;
-  for (int l = 0; l < 2; l++) { c->d_snc[l] = nullptr; c->d_slo[l] = nullptr; c->d_scs[l] = nullptr; }
+  for (int l = 0; l < 3; l++) { c->d_snc[l] = nullptr; c->d_slo[l] = nullptr; c->d_scs[l] = nullptr; }
+  c->d_fp = c->d_em = nullptr;
+  c->d_gm = nullptr;
   c->nsys = 1;
   c->tuned = false;
   c->overlap = false;
@@ -1355,11 +1376,12 @@ void prof_end(mdg_ctx* c);
 // when a step is given; before it, the bath temperature) in one pass over
 // the atoms.
 constexpr int kDispParts = 296;  // 2 blocks per SM of a B200
+constexpr int kMetalListCap = 320;  // metal / ion list partners per atom (fcc Cu holds ~180 within 7.92 A)
 constexpr int kBathBlocks = 120;
 int step_start(mdg_ctx* c, const StepDev* step)
 {
   State S = c->S();
-  const int nl = c->has_list[1] ? 2 : 1;
+  const int mask = (c->has_list[0] ? 1 : 0) | (c->has_list[1] ? 2 : 0) | (c->has_list[2] ? 4 : 0);
   if (step && step->tb_geom) {
     const int bps = std::max(1, kBathBlocks / c->nsys);
     LAUNCH(c, "bath_temp_partial", k_bath_partial, dim3(bps, c->nsys), kThreads, S, *step,
@@ -1369,7 +1391,7 @@ int step_start(mdg_ctx* c, const StepDev* step)
   StepDev none;
   std::memset(&none, 0, sizeof(none));
   LAUNCH(c, step ? "verlet_pos_disp" : "nl_disp_partial", k_step_start, kDispParts, kThreads, S,
-         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], nl, c->d_part);
+         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], c->nl[2], mask, c->d_part);
   return MDG_OK;
 }
 
@@ -1392,8 +1414,8 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
     LAUNCH_ON(c, st, "nl_cell_fill", k_cell_fill, nblk(c->n), kThreads, S, g, need);
     LAUNCH_ON(c, st, "nl_cell_sort", k_cell_sort, nblk(g.ncell), kThreads, g, need);
   }
-  LAUNCH_ON(c, st, l == 0 ? "nl_build_rebo" : "nl_build_lj", k_nl_build, nblk(c->n), kThreads, S, g, L, need,
-            c->d_status);
+  LAUNCH_ON(c, st, l == 0 ? "nl_build_rebo" : (l == 1 ? "nl_build_lj" : "nl_build_metal"), k_nl_build, nblk(c->n),
+            kThreads, S, g, L, need, c->d_status);
   return MDG_OK;
 }
 
@@ -1402,6 +1424,7 @@ int rebuild_lists(mdg_ctx* c, const StepDev* step = nullptr)
   int rc = step_start(c, step);
   if (!rc) rc = rebuild_list(c, 0, c->stream);
   if (!rc) rc = rebuild_list(c, 1, c->stream);
+  if (!rc) rc = rebuild_list(c, 2, c->stream);
   if (rc) return rc;
   return launch_check(c);
 }
@@ -1522,29 +1545,45 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
   if (tasks || lj)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
+  if (c->has_list[2]) {
+    LAUNCH(c, "eam_density", k_eam_rho, nblk(c->n), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
+           c->d_status);
+    LAUNCH(c, "metal_pairs", k_metal_pairs, nblk(c->n), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
+           c->d_gm);
+  }
   if (step) {
     LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
-           *step, c->e_kin, c->d_status);
+           *step, c->e_kin, c->d_gm, c->d_status);
     if (step->vmax)
       LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_dt_prev, c->d_time,
              c->timeaccel, c->stop_final ? c->d_stop : nullptr, c->time_final_s / kFs);
   }
   else
-    LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad);
+    LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, c->d_gm);
   return launch_check(c);
 }
 
-int reduce_energies(mdg_ctx* c, double* out_dev, int slot_stride, int slot, bool with_kin)
+// Sums of rebo, lj, tors (, kin) into slots 0-3; the metal and ion energies
+// join the torsion slot, or take slot 3 of their own (split_metal, no kin).
+int reduce_energies(mdg_ctx* c, double* out_dev, int slot_stride, int slot, bool with_kin, bool split_metal = false)
 {
   RedArgs R;
   R.a[0] = c->fo.e_rebo;
   R.a[1] = c->fo.e_lj;
   R.a[2] = c->fo.e_tors;
   R.a[3] = c->e_kin;
+  for (int k = 0; k < 5; k++) R.slot[k] = k;
   R.narr = with_kin ? 4 : 3;
+  R.nout = R.narr;
+  if (c->has_list[2]) {
+    R.a[R.narr] = c->d_em;
+    R.slot[R.narr] = split_metal && !with_kin ? 3 : 2;
+    R.narr++;
+    if (split_metal && !with_kin) R.nout = 4;
+  }
   R.n = c->n;
   LAUNCH(c, "energy_partial", k_reduce_partial, dim3(kRedBlocks, R.narr), kThreads, R, c->d_red_part);
-  LAUNCH(c, "energy_final", k_reduce_final, 1, 32, c->d_red_part, kRedBlocks, R.narr, out_dev, slot_stride, slot,
+  LAUNCH(c, "energy_final", k_reduce_final, 1, 32, c->d_red_part, kRedBlocks, R, out_dev, slot_stride, slot,
          c->d_status);
   return launch_check(c);
 }
@@ -1668,13 +1707,13 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   }
   c->stream = c->own_stream;
   c->d_status = dalloc<unsigned int>(1);
-  c->d_need = dalloc<int>(2);
-  c->d_force = dalloc<int>(2);
+  c->d_need = dalloc<int>(3);
+  c->d_force = dalloc<int>(3);
   c->d_energy = dalloc<double>(8);
   if (!c->d_status || !c->d_need || !c->d_force || !c->d_energy) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc"); }
   cudaMemset(c->d_status, 0, sizeof(unsigned int));
-  cudaMemset(c->d_need, 0, 2 * sizeof(int));
-  cudaMemset(c->d_force, 0, 2 * sizeof(int));
+  cudaMemset(c->d_need, 0, 3 * sizeof(int));
+  cudaMemset(c->d_force, 0, 3 * sizeof(int));
   if (cudaGetLastError() != cudaSuccess) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "setup copies failed"); }
   *out = c;
   return MDG_OK;
@@ -1686,7 +1725,8 @@ int mdg_destroy(mdg_ctx* c)
   if (c->stream) cudaStreamSynchronize(c->stream);
   io_free(c);
   free_system(c);
-  void* ptrs[] = {c->d_tables, c->d_tables32, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy};
+  void* ptrs[] = {c->d_tables, c->d_tables32, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy,
+                  c->d_metal};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -1757,11 +1797,26 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   std::vector<double> hm(n), hpos(3 * (size_t)n);
   std::vector<unsigned char> hf(n, 0);
   c->h_type.assign(n, 0);
+  const bool metal = c->prm.potentials & MDG_POT_METAL;
+  int nonch = 0;
+  // Atom::setAttributesByElementID (Atom.hpp:100-115): masses in amu by species
+  const double mass_of[kNSpec] = {12.0, 1.0, 63.546, 107.868, 196.967, 39.948, 131.293};
   for (int i = 0; i < n; i++) {
     int t;
-    if (z[i] == 6) t = kC;
-    else if (z[i] == 1) t = kH;
-    else return fail(MDG_ERR_ARG, "unknown element (REBO::e2i handles only H and C)");
+    switch (z[i]) {
+      case 6: t = kC; break;
+      case 1: t = kH; break;
+      case 29: t = kCu; break;
+      case 47: t = kAg; break;
+      case 79: t = kAu; break;
+      case 18: t = kAr; break;
+      case 54: t = kXe; break;
+      default: return fail(MDG_ERR_ARG, "unknown element (H, C, Cu, Ag, Au, Ar, Xe are on this path)");
+    }
+    if (t > kH) {
+      if (!metal) return fail(MDG_ERR_ARG, "Cu, Ag, Au, Ar and Xe need MDG_POT_METAL (REBO::e2i handles only H and C)");
+      nonch++;
+    }
     double x[3];
     int im[3] = {0, 0, 0};
     const Box& bx = c->h_boxes[c->h_sys[i]];
@@ -1780,11 +1835,12 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
       hv[i] = make_double4(0, 0, 0, 0);
     ha[i] = make_double4(0, 0, 0, 0);
     him[i] = make_int4(im[0], im[1], im[2], 0);
-    hm[i] = (t == kC) ? 12.0 : 1.0;
+    hm[i] = mass_of[t];
   }
   // minimum image needs every period above twice the largest cutoff
   // (SimLoop.cxx:239-245, AtomsArray::checkMIC)
   double rmax = (c->prm.potentials & MDG_POT_AIREBO_LJ) ? c->ljp.R[0][0][1] : 2.0;
+  if (metal && nonch) rmax = std::fmax(rmax, 5.5);  // FBZL / FLJ (Rcutoff 5.5 A, applications/common.h:46-49)
   for (const Box& bx : c->h_boxes)
     for (int a = 0; a < 3; a++)
       if (bx.pbc[a] && !(bx.L[a] > 2.0 * rmax))
@@ -1821,17 +1877,22 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   c->rcut[1] = with_lj ? std::fmax(std::fmax(c->ljp.R[0][0][1], c->ljp.R[0][1][1]), c->ljp.R[1][1][1]) : 0.0;
   c->has_list[0] = true;
   c->has_list[1] = with_lj;
-  for (int l = 0; l < 2; l++) {
+  c->has_list[2] = metal && nonch > 0;
+  c->rcut[2] = 5.5;  // FBZL, FLJ 5.5 A; Ackland's own ranges are below it
+  for (int l = 0; l < 3; l++) {
     if (!c->has_list[l]) continue;
     NList& L = c->nl[l];
     double range = c->prm.nl_skin_mode == 0 ? (1.0 + 0.44) * c->rcut[l] : c->rcut[l] + c->prm.nl_skin;
     L.range2 = range * range;
     L.trigger = c->prm.nl_skin_mode == 0 ? 0.44 * c->rcut[l] : c->prm.nl_skin;
-    L.cap = (l == 0) ? c->prm.cap_rebo_list : c->prm.cap_lj_list;
+    L.cap = (l == 0) ? c->prm.cap_rebo_list : (l == 1 ? c->prm.cap_lj_list : kMetalListCap);
     // The REBO list keeps the reference's ascending order (it fixes the bond
     // slot order, hence every bond-order sum).  The LJ list only orders pair
     // sums, so it stays in (deterministic) cell order and skips the sort.
     L.sorted = (l == 0) ? 1 : 0;
+    // with metal or ion atoms present, REBO and AIREBO see hydrocarbon pairs
+    // only, the metal list every other pair (FGeneral's handled pairs)
+    L.pairs = (l == 2) ? 2 : (nonch ? 1 : 0);
     L.cnt = dalloc<int>(n);
     L.list = dalloc<int>((size_t)n * L.cap);
     L.pos0 = dalloc<double4>(n);
@@ -1844,9 +1905,23 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     int rc = nsys > 1 ? setup_grid_batch(c, l, hpos) : setup_grid(c, l, hpos);
     if (rc) return rc;
   }
-  int one[2] = {1, 1};
+  int one[3] = {1, 1, 1};
   CK(cudaMemcpy(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice));
-  c->d_part = dalloc<double>(2 * 2 * kDispParts);
+  c->d_part = dalloc<double>(2 * 3 * kDispParts);
+  if (c->has_list[2]) {
+    if (!c->d_metal) {
+      MetalParams hmp;
+      make_metal_params(hmp);
+      c->d_metal = dalloc<MetalParams>(1);
+      if (!c->d_metal) return fail(MDG_ERR_CUDA, "cudaMalloc (metal parameters)");
+      CK(cudaMemcpy(c->d_metal, &hmp, sizeof(hmp), cudaMemcpyHostToDevice));
+    }
+    c->d_fp = dalloc<double>(n);
+    c->d_em = dalloc<double>(n);
+    c->d_gm = dalloc<double4>(n);
+    if (!c->d_fp || !c->d_em || !c->d_gm) return fail(MDG_ERR_CUDA, "cudaMalloc (metal forces)");
+    CK(cudaMemset(c->d_em, 0, n * sizeof(double)));
+  }
 
   // bonds and force outputs
   const int mb = c->mb;
@@ -1868,7 +1943,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   c->fo.e_tors = dalloc<double>(n);
   c->fo.e_lj = dalloc<double>(n);
   c->e_kin = dalloc<double>(n);
-  c->d_red_part = dalloc<double>(4 * kRedBlocks);
+  c->d_red_part = dalloc<double>(5 * kRedBlocks);
   if (!c->bb.nb || !c->bb.bj || !c->bb.brev || !c->bb.brv || !c->bb.bu || !c->bb.bd || !c->bb.nco || !c->fo.A ||
       !c->fo.W || !c->fo.gown || !c->fo.glj || !c->fo.e_rebo || !c->fo.e_tors || !c->fo.e_lj || !c->e_kin ||
       !c->d_red_part)
@@ -2042,11 +2117,11 @@ int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   int rc = evaluate(c);
   if (rc) return rc;
-  rc = reduce_energies(c, c->d_energy, 0, 0, false);
+  rc = reduce_energies(c, c->d_energy, 0, 0, false, true);
   if (rc) return rc;
   LAUNCH(c, "finite_check", k_finite, nblk(c->n), kThreads, c->grad, c->n, c->d_status);
   double he[4] = {0, 0, 0, 0};
-  CK(cudaMemcpyAsync(he, c->d_energy, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(he, c->d_energy, (c->has_list[2] ? 4 : 3) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   std::vector<double4> hg;
   if (grad) {
     hg.resize(c->n);
@@ -2055,12 +2130,13 @@ int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
   rc = read_status(c);
   if (rc) return rc;
   double E = (he[0] + he[1]) + he[2];
+  if (c->has_list[2]) E += he[3];
   if (e_total) *e_total = E * c->unit_e;
   if (e_terms) {
     e_terms[0] = he[0] * c->unit_e;
     e_terms[1] = he[1] * c->unit_e;
     e_terms[2] = he[2] * c->unit_e;
-    e_terms[3] = 0.0;
+    e_terms[3] = he[3] * c->unit_e;  // FBZL + FLJ + Ackland
   }
   if (grad)
     for (int i = 0; i < c->n; i++) {
@@ -2185,6 +2261,7 @@ static StepDev step_dev(mdg_ctx* c, double dtf)
   P.vmax = c->adaptive ? c->d_vmax : nullptr;
   P.nlc0 = c->nl[0].cnt;
   P.nlc1 = c->has_list[1] ? c->nl[1].cnt : nullptr;
+  P.nlc2 = c->has_list[2] ? c->nl[2].cnt : nullptr;
   P.ekin_pre = c->d_ekin_pre;
   P.acc_ntb = c->tb_geom ? c->acc_ntb : nullptr;
   P.eb = c->tb_geom ? c->d_eb : nullptr;
@@ -2316,7 +2393,7 @@ int mdg_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
 int sys_energies(mdg_ctx* c, double* out_dev)
 {
   LAUNCH(c, "sys_energy", k_sys_energy, c->nsys, kThreads, c->d_first ? c->d_first : nullptr, (int64_t)c->n, c->fo.e_rebo,
-         c->fo.e_lj, c->fo.e_tors, c->e_kin, out_dev, c->d_status);
+         c->fo.e_lj, c->fo.e_tors, c->e_kin, c->has_list[2] ? c->d_em : nullptr, out_dev, c->d_status);
   return launch_check(c);
 }
 

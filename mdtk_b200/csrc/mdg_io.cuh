@@ -38,7 +38,26 @@ constexpr double kCgsAcc = kAo / (kFs * kFs);   // Angstrom/fs^2 -> cm/s^2
 constexpr double kCgsForce = kEv / kAo;         // eV/Angstrom -> erg/cm
 constexpr double kKbErg = 8.617343E-5 * kEv;    // kb (consts.cxx:32), erg/K
 constexpr double kNoPbcCm = 10000.0 * kAo;      // NO_PBC_L (consts.hpp:96)
-constexpr int kElH = 1, kElC = 12;              // ElementID H_EL, C_EL (consts.hpp:46-49)
+// ElementID (consts.hpp:46-55) by atomic number and back
+inline int element_id(int z)
+{
+  switch (z) {
+    case 1: return 1;
+    case 6: return 12;
+    case 29: return 64;
+    case 47: return 108;
+    case 79: return 197;
+    case 18: return 40;
+    case 54: return 131;
+  }
+  return -1;
+}
+inline int z_of_element(int e)
+{
+  for (int z : {1, 6, 29, 47, 79, 18, 54})
+    if (element_id(z) == e) return z;
+  return -1;
+}
 constexpr int kHdr = 7;                         // per-system header doubles of a snapshot
 
 // Byte offsets of one snapshot (same layout on the device and the host).
@@ -166,7 +185,7 @@ struct Rec {
 // Per atom: coords, V, an, -grad in CGS, PBC_count, and the Check inputs
 // (kinetic energy before the last kick, potential energy, bath energy) in erg.
 __global__ void k_snap_pack(State S, const double4* grad, const double* er, const double* el, const double* et,
-                            const double* ekp, const double* eb, char* out, SnapLayout L)
+                            const double* em, const double* ekp, const double* eb, char* out, SnapLayout L)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
@@ -183,7 +202,7 @@ __global__ void k_snap_pack(State S, const double4* grad, const double* er, cons
   f[0] = -g.x * kCgsForce; f[1] = -g.y * kCgsForce; f[2] = -g.z * kCgsForce;
   im[0] = m.x; im[1] = m.y; im[2] = m.z;
   ((double*)(out + L.ekp))[i] = ekp[i] * kEv;
-  ((double*)(out + L.ep))[i] = ((er[i] + el[i]) + et[i]) * kEv;
+  ((double*)(out + L.ep))[i] = (((er[i] + el[i]) + et[i]) + (em ? em[i] : 0.0)) * kEv;
   ((double*)(out + L.eb))[i] = eb ? eb[i] * kEv : 0.0;
 }
 
@@ -334,7 +353,7 @@ bool write_state_files(const IoJob& J, const char* h, const SnapLayout& L, std::
   auto put = [&](const char* attr, const std::string& b) { return write_blob(id + attr, b.data(), b.size(), J.zip, err); };
   Rec z, pr, cnt, en, idx;
   for (int64_t i = 0; i < n; i++) {
-    z.put<uint8_t>((uint8_t)(J.z[i] == 6 ? kElC : kElH));
+    z.put<uint8_t>((uint8_t)element_id(J.z[i]));
     for (int k = 0; k < 3; k++) cnt.put<int32_t>(im[3 * i + k]);
     for (int k = 0; k < 3; k++) en.put<uint8_t>(J.box.pbc[k] ? 1 : 0);
     idx.put<uint32_t>((uint32_t)i);  // Atom::globalIndex (AtomsContainer.cxx:114)
@@ -591,7 +610,7 @@ static int io_snapshot(mdg_ctx* c, int* slot_out)
   io->lay = L;
   State St = c->S();
   LAUNCH(c, "snap_pack", k_snap_pack, nblk(c->n), kThreads, St, c->grad, c->fo.e_rebo, c->fo.e_lj, c->fo.e_tors,
-         c->d_ekin_pre, c->tb_geom ? c->d_eb : nullptr, S.d, L);
+         c->has_list[2] ? c->d_em : nullptr, c->d_ekin_pre, c->tb_geom ? c->d_eb : nullptr, S.d, L);
   LAUNCH(c, "snap_header", k_snap_header, nblk(c->nsys), kThreads, c->nsys, c->d_time, c->d_dt, c->d_dt_prev,
          c->d_e0, S.d, L);
   CK(cudaEventRecord(S.packed, c->stream));
@@ -983,10 +1002,8 @@ int mdg_load_state(mdg_ctx* c, const char* id_c, uint64_t iteration, int* loaded
   if (n > (1LL << 30)) return fail(MDG_ERR_ARG, "too many atoms");
   std::vector<int32_t> z(n);
   for (int64_t i = 0; i < n; i++) {
-    const int e = (uint8_t)b[i];
-    if (e == kElH) z[i] = 1;
-    else if (e == kElC) z[i] = 6;
-    else return fail(MDG_ERR_ARG, "unknown element in " + id + ".z (only H and C are on this path)");
+    z[i] = z_of_element((uint8_t)b[i]);
+    if (z[i] < 0) return fail(MDG_ERR_ARG, "unknown element in " + id + ".z");
   }
   got |= MDG_LOADED_Z;
   auto sized = [&](const char* attr, size_t rec) -> int {

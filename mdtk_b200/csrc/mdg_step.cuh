@@ -15,6 +15,8 @@ namespace mdg {
 struct NList {
   int cap;
   int sorted;         // 1: ascending partner order (the reference's); 0: cell order (deterministic)
+  int pairs;          // 0: every pair; 1: hydrocarbon pairs only (the REBO/AIREBO lists of a system
+                      // with metal or ion atoms); 2: pairs with a metal or ion atom (their own list)
   int* cnt;
   int* list;
   double range2;      // ((1 + 0.44) * Rcutoff)^2
@@ -122,10 +124,18 @@ MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsign
   const Box& box = box_of(S, i);
   int cnt = 0;
   int* out = L.list + (long)i * L.cap;
+  // FGeneral's handled pairs: REBO and AIREBO never see metal or ion atoms
+  const bool ich = pi.w < 1.5;
+  if (L.pairs == 1 && !ich) {
+    L.cnt[i] = 0;
+    L.pos0[i] = pi;
+    return;
+  }
   if (g.brute && !S.sys) {
     for (int j = 0; j < S.n; j++) {
       if (j == i) continue;
       double4 pj = S.pos[j];
+      if (L.pairs && (L.pairs == 1 ? pj.w > 1.5 : (ich && pj.w < 1.5))) continue;
       V3 d = depos(box, xi, v3(pj.x, pj.y, pj.z));
       if (norm2(d) < L.range2) {
         if (cnt < L.cap) out[cnt] = j;
@@ -159,6 +169,7 @@ MDG_HD void nl_build_atom(const State& S, const Grid& g, NList& L, int i, unsign
             int j = g.catoms[q];
             if (j == i) continue;
             double4 pj = S.pos[j];
+            if (L.pairs && (L.pairs == 1 ? pj.w > 1.5 : (ich && pj.w < 1.5))) continue;
             V3 d = depos(box, xi, v3(pj.x, pj.y, pj.z));
             if (norm2(d) < L.range2) {
               if (cnt < L.cap) out[cnt] = j;
@@ -517,6 +528,7 @@ struct StepDev {
   unsigned long long* vmax;       // per system: bits of the largest |v| (adaptive dt), or null
   const int* nlc0;                // list counts, FProxy::hasNeighbors (FProxy.hpp:99-105)
   const int* nlc1;                // (null when there is no second list)
+  const int* nlc2;                // metal and ion pair list (null when there is none)
   double* ekin_pre;               // per atom M V_n^2 / 2 before the kick (SimLoop::energyKin at
                                   // doEnergyConservationCheck, SimLoop.cxx:337), or null
   double4* acc_ntb;               // per atom Atom::an_no_tb, updated in the bath branch only
@@ -605,7 +617,7 @@ MDG_HD void verlet_vel_ext_atom(State& S, V3 grad, const StepDev& P, int i, unsi
     const V3 vn = v3(vdt2.x + an.x * dt / 2.0, vdt2.y + an.y * dt / 2.0, vdt2.z + an.z * dt / 2.0);
     S.vel[i] = make_double4(vn.x, vn.y, vn.z, 0.0);
 #if defined(__CUDA_ARCH__)
-    if (P.vmax && (P.nlc0[i] > 0 || (P.nlc1 && P.nlc1[i] > 0))) {
+    if (P.vmax && (P.nlc0[i] > 0 || (P.nlc1 && P.nlc1[i] > 0) || (P.nlc2 && P.nlc2[i] > 0))) {
       const double vm = sqrt(vn.x * vn.x + vn.y * vn.y + vn.z * vn.z);
       // non-negative doubles order like their bit patterns: the maximum does
       // not depend on the order of the atomics

@@ -35,7 +35,7 @@ from . import (Context, POT_AIREBO, TB_NONE, TB_UNIVERSE, TB_BOX, TB_SPHERE, ZIP
 
 AO = 1e-8    # Angstrom in cm (consts.cxx:30)
 FS = 1e-15   # fs in s (consts.cxx:36)
-EL_Z = {1: 1, 12: 6}  # ElementID H_EL, C_EL -> atomic number
+EL_Z = {1: 1, 12: 6, 64: 29, 108: 47, 197: 79, 40: 18, 131: 54}  # ElementID (consts.hpp:46-55) -> atomic number
 _EXT = {ZIP_NONE: "", ZIP_GZIP: ".gz", ZIP_XZ: ".xz"}
 
 

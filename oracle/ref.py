@@ -24,6 +24,7 @@ POT_AIREBO_LJ = 2
 POT_ETORS = 4
 POT_BRENNER = 8
 POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
+POT_METAL = 16
 
 _lib = None
 

@@ -35,6 +35,9 @@
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_LJ.hpp>
 #include <mdtk/potentials/manybody/AIREBO/AIREBO_ETors.hpp>
 #include <mdtk/potentials/manybody/Brenner/Brenner.hpp>
+#include <mdtk/potentials/pairwise/FBZL.hpp>
+#include <mdtk/potentials/pairwise/FLJ.hpp>
+#include <mdtk/potentials/manybody/Ackland/Ackland.hpp>
 
 using namespace mdtk;
 
@@ -42,7 +45,7 @@ namespace {
 
 std::string g_last_error;
 
-enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8 };
+enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8, POT_METAL = 16 };
 
 double wall_now()
 {
@@ -130,9 +133,30 @@ struct RefCtx
 
 ElementID el_from_z(int z)
 {
-  if (z == 1) return H_EL;
-  if (z == 6) return C_EL;
-  throw Exception("unknown element (only H=1 and C=6 are on this path)");
+  switch (z) {
+    case 1: return H_EL;
+    case 6: return C_EL;
+    case 29: return Cu_EL;
+    case 47: return Ag_EL;
+    case 79: return Au_EL;
+    case 18: return Ar_EL;
+    case 54: return Xe_EL;
+  }
+  throw Exception("unknown element (H, C, Cu, Ag, Au, Ar, Xe are on this path)");
+}
+
+int z_from_el(ElementID e)
+{
+  switch (e) {
+    case H_EL: return 1;
+    case C_EL: return 6;
+    case Cu_EL: return 29;
+    case Ag_EL: return 47;
+    case Au_EL: return 79;
+    case Ar_EL: return 18;
+    case Xe_EL: return 54;
+    default: return -1;
+  }
 }
 
 void ensure_nl(RefCtx* c)
@@ -171,6 +195,14 @@ void* ref_create(int potset, int brenner_set, int lj_cut_mode)
     c->brenner_set = brenner_set;
     c->lj_cut_mode = lj_cut_mode;
     c->loop.preventFileOutput = true;
+    if (potset & POT_METAL) {
+      // the ion and metal-hydrocarbon pair potentials first, as
+      // setupPotentials adds them (applications/common.h:45-50)
+      c->loop.fpot.addPotential(new FBZL(Rcutoff(5.0 * Ao, 5.5 * Ao)));
+      c->names.push_back("FBZL");
+      c->loop.fpot.addPotential(new FLJ(Rcutoff(5.0 * Ao, 5.5 * Ao)));
+      c->names.push_back("FLJ");
+    }
     if (potset & POT_REBO) {
       c->rebo = new REBO();
       c->loop.fpot.addPotential(c->rebo);
@@ -199,6 +231,10 @@ void* ref_create(int potset, int brenner_set, int lj_cut_mode)
       c->brenner = new Brenner(brenner_set == 2 ? Brenner::POTENTIAL2 : Brenner::POTENTIAL1);
       c->loop.fpot.addPotential(c->brenner);
       c->names.push_back("Brenner");
+    }
+    if (potset & POT_METAL) {
+      c->loop.fpot.addPotential(new Ackland());  // applications/common.h:62-63
+      c->names.push_back("Ackland");
     }
     return c;
   } catch (std::exception& e) {
@@ -799,7 +835,7 @@ int ref_get_atoms(void* h, double* pos, double* vel, double* acc, int* image, un
       for (int k = 0; k < 6; k++) if (a.hasTag(bits[k])) t |= (unsigned char)bits[k];
       tags[i] = t;
     }
-    if (z) z[i] = a.ID == H_EL ? 1 : (a.ID == C_EL ? 6 : -1);
+    if (z) z[i] = z_from_el(a.ID);
   }
   return 0;
 }
