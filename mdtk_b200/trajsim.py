@@ -31,7 +31,7 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
-from . import (Context, POT_AIREBO, TB_NONE, TB_UNIVERSE, TB_BOX, TB_SPHERE, ZIP_NONE, ZIP_GZIP, ZIP_XZ)
+from . import (Context, POT_AIREBO, POT_METAL, TB_NONE, TB_UNIVERSE, TB_BOX, TB_SPHERE, ZIP_NONE, ZIP_GZIP, ZIP_XZ)
 
 AO = 1e-8    # Angstrom in cm (consts.cxx:30)
 FS = 1e-15   # fs in s (consts.cxx:36)
@@ -125,10 +125,13 @@ def remove_iterations(dirname: str, keep_first: bool, keep_last: bool):
 
 
 def impact_sequence(base_id: str, ionpos_path: str, workdir: str, start: int = 0, batch: int = 256,
-                    potentials: int = POT_AIREBO, zip: int = ZIP_NONE, snapshot_capacity: int = 8192,
+                    potentials: int = POT_AIREBO | POT_METAL, zip: int = ZIP_NONE, snapshot_capacity: int = 8192,
                     max_steps: int = 10 ** 9, timeaccel: float = 1.0, task_mode: int = 0) -> List[int]:
     """Runs the impacts of ``ionpos_path`` (pairs of doubles, cm) from impact
-    ``start`` on, ``batch`` at a time; returns the impacts run."""
+    ``start`` on, ``batch`` at a time; returns the impacts run.  The default
+    potentials are the application's (setupPotentials with REBO); the
+    application compresses with yaatk's first working method (``.xz`` where
+    the xz program exists): pass ``zip=ZIP_XZ`` for the same files."""
     base = read_state(base_id)
     raw = read_file(ionpos_path)
     if raw is None or len(raw) % 16:

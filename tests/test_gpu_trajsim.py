@@ -99,6 +99,41 @@ def test_impact_sequence_matches_mdtrajsim(tmp_path):
     assert T.impact_sequence(str(tmp_path / "base"), str(tmp_path / "ionpos.bin"), str(tmp_path / "dev")) == []
 
 
+def test_impact_sequence_matches_the_mdtrajsim_application(tmp_path):
+    """The unmodified mdtrajsim application (applications/mdtrajsim/main.cpp
+    built from its own sources, `mdtrajsim base -i 0`) and the batched driver
+    with the application's potential set and compression."""
+    import subprocess
+    app = os.path.join(os.path.dirname(ref.LIB_PATH), "mdtrajsim")
+    z, pos, vel, box, fixed, tags = base_system()
+    r = ref.RefSystem(ref.POT_AIREBO | ref.POT_METAL)
+    r.set_atoms(z, pos, vel, box, (1, 1, 0), fixed)
+    r.set_tags(tags)
+    r.set_time(0.0, 30.0, 0.2)
+    ref.set_zip(0)
+    os.makedirs(tmp_path / "ref")
+    r.write_state(str(tmp_path / "ref" / "base"))
+    xy = np.array([[2.0e-8, 3.0e-8], [9.5e-8, 11.0e-8]])
+    xy.tofile(str(tmp_path / "ref" / "ionpos.bin"))
+    p = subprocess.run([app, "base", "-i", "0"], cwd=str(tmp_path / "ref"), capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    T.impact_sequence(str(tmp_path / "ref" / "base"), str(tmp_path / "ref" / "ionpos.bin"), str(tmp_path / "dev"),
+                      zip=M.ZIP_XZ, task_mode=1)
+    for k in range(2):
+        dd, rd = tmp_path / "dev" / ("%08d" % k), tmp_path / "ref" / ("%08d" % k)
+        files = sorted(f for f in os.listdir(rd) if f not in ("stdout.txt", "stderr.txt"))
+        assert sorted(os.listdir(dd)) == files and all(f.endswith(".xz") for f in files)
+        assert read(str(dd / "ionpos_used.txt")) == read(str(rd / "ionpos_used.txt"))
+        final = [f[:-5] for f in files if f.endswith(".r.xz")]
+        compare_state(str(dd / final[0]), str(rd / final[0]), adaptive=True)
+        compare_xva(str(dd / "mde0000000000.xva"), str(rd / "mde0000000000.xva"), box=np.asarray(box) * [1, 1, 0],
+                    adaptive=True)
+        ia, ta, ra = read_snapshots(str(dd / "snapshots.conf"))
+        ib, tb, rb = read_snapshots(str(rd / "snapshots.conf"))
+        assert np.array_equal(ia, ib) and len(ta) == len(tb) and np.allclose(ta, tb, rtol=1e-9, atol=0)
+
+
 def test_snapshot_capture_and_reload(tmp_path):
     """The device SnapshotList: snapshots at CustomSimLoop's times, the same
     list through the API and the file, text form, reload, capacity."""
