@@ -2313,7 +2313,8 @@ static int init_first_step(mdg_ctx* c)
   LAUNCH(c, "init_acc", k_init_acc, nblk(c->n), kThreads, S, c->grad, c->acc_ntb, first ? c->d_eb : nullptr);
   if (first) {
     LAUNCH(c, "ekin", k_ekin, nblk(c->n), kThreads, S, c->e_kin);
-    rc = sys_energies(c, c->d_e0);
+    // one system: the grid-wide reduction (the per-system kernel is one block per system)
+    rc = c->nsys == 1 ? reduce_energies(c, c->d_e0, 0, 0, true) : sys_energies(c, c->d_e0);
     if (rc) return rc;
     c->e0_dev = true;
     c->chk_eb0 = 0.0;
