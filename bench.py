@@ -451,6 +451,8 @@ def main():
             "fp64_peak_tflops": fp64_peak,
             "variants": {"fp32_mixed": mixed, "batched": batched, "adjoint": adjoint},
         }
+        if world == 1 and not args.no_variants:
+            line["variants"]["next_rows"] = next_rows(M, s, local, stream, flush, value)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 v, res = cpu_baseline(1, args.cpu_steps)
@@ -468,6 +470,176 @@ def main():
 
 
 ADJ_ATOMS, ADJ_STEPS, ADJ_DT_FS, ADJ_EVERY = 4096, 200, 0.5, 20
+
+
+def next_rows(M, s, local, stream, flush, plain_rate):
+    """Throughput of the rows around the step, one GPU:
+
+    * SimLoop's thermal bath (universe, 300 K, 1e13 / s) with adaptive dt on
+      the headline ethane liquid;
+    * the same liquid writing its files from device snapshots, at
+      mdtrajsim's intervals and at ten times their frequency (wall clock, the
+      files included);
+    * mdtrajsim's impact sequence: 64 impacts of a C projectile on a 900-atom
+      graphite slab to 20 fs, one batched context with the application's
+      files, against the unmodified mdtrajsim application on the host for
+      one impact;
+    * metal and ion potentials: ethane molecules and an Ar ion above an
+      18,432-atom Cu slab (AIREBO + FBZL + FLJ + Ackland), against the
+      reference's own classes on the host (3 steps).
+    CUDA events on the library stream unless said otherwise."""
+    import shutil
+    import tempfile
+    import torch
+    from mdtk_b200 import builders as B
+    from mdtk_b200 import trajsim as T
+    out = {}
+    n = len(s["z"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(c, k, dt):
+        flush.zero_()
+        e0.record(stream)
+        c.run(k, dt, energies=False)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # thermal bath + adaptive dt
+    c = M.Context(potentials=M.POT_AIREBO, device=local)
+    c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    c.set_stream(stream.cuda_stream)
+    c.set_thermal_bath(M.TB_UNIVERSE, 300.0, 1e13 * 1e-15)
+    c.set_adaptive_dt(True, 1.0, DT_FS)
+    c.run(3, DT_FS, energies=False)
+    c.sync()
+    ms = timed(c, 100, DT_FS)
+    out["bath_adaptive_dt"] = {"value": n * 100 / (ms * 1e-3), "unit": "atom-steps/s", "steps": 100,
+                               "over_plain": n * 100 / (ms * 1e-3) / plain_rate,
+                               "workload": "headline liquid, universe bath 300 K, gamma 1e13/s, adaptive dt"}
+    del c
+
+    # files from device snapshots
+    tmp = tempfile.mkdtemp(prefix="mdg_out_")
+    try:
+        c = M.Context(potentials=M.POT_AIREBO, device=local)
+        c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+        c.set_stream(stream.cuda_stream)
+        c.run(3, DT_FS, energies=False)
+        c.sync()
+        for flush_it, traj_fs, label in ((1000, 100.0, "mdtrajsim's intervals: state every 1000 iterations, "
+                                                       "XVA every 0.1 ps (400 steps)"),
+                                         (100, 10.0, "state every 100 iterations, XVA every 10 fs (40 steps)")):
+            c.set_output(os.path.join(tmp, str(flush_it)), flush_it, traj_fs)
+            t0 = time.perf_counter()
+            c.run(2000, DT_FS, energies=False)
+            c.flush_output()
+            wall = time.perf_counter() - t0
+            c.set_output(None)
+            nfiles = len(os.listdir(os.path.join(tmp, str(flush_it))))
+            out["files_every_%d" % flush_it] = {
+                "value": n * 2000 / wall, "unit": "atom-steps/s (wall clock, files written)", "steps": 2000,
+                "files": nfiles, "over_plain": n * 2000 / wall / plain_rate,
+                "workload": "headline liquid, " + label}
+        del c
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+    # mdtrajsim impact sequence
+    tmp = tempfile.mkdtemp(prefix="mdg_traj_")
+    try:
+        slab = B.graphite_slab(2, 8, 4, temp_k=0.0, seed=3)
+        top = slab["pos"][:, 2].max()
+        base = B.add_atoms(slab, [6], [[slab["box"][0] / 2, slab["box"][1] / 2, top + 3.0]], vel=[[0, 0, -0.04]])
+        nb = len(base["z"])
+        bc = M.Context(potentials=M.POT_AIREBO | M.POT_METAL, device=local)
+        bc.set_system(base["z"], base["pos"], base["vel"], base["box"], (1, 1, 0), base["fixed"])
+        tags = np.full(nb, M.TAG_TARGET, np.uint8)
+        tags[-1] = M.TAG_PROJECTILE
+        bc.set_atom_tags(tags)
+        bc.set_adaptive_dt(True, 1.0, 0.2)
+        bc.set_time_final(20.0)
+        bc.write_state(os.path.join(tmp, "base"))
+        del bc
+        rng = np.random.default_rng(7)
+        nimp = 64
+        xy = np.stack([rng.uniform(0, base["box"][0], nimp), rng.uniform(0, base["box"][1], nimp)], 1) * 1e-8
+        xy.tofile(os.path.join(tmp, "ionpos.bin"))
+        t0 = time.perf_counter()
+        T.impact_sequence(os.path.join(tmp, "base"), os.path.join(tmp, "ionpos.bin"), os.path.join(tmp, "dev"),
+                          batch=nimp, task_mode=1)
+        wall = time.perf_counter() - t0
+        iters = []
+        for k in range(nimp):
+            d = os.path.join(tmp, "dev", "%08d" % k)
+            iters += [int(f[2:12]) for f in os.listdir(d) if f.startswith("md") and f.endswith(".r")]
+        row = {"value": nimp / wall, "unit": "impacts/s (wall clock, files included)", "impacts": nimp,
+               "atoms_per_impact": nb, "atom_steps_per_s": nb * sum(iters) / wall,
+               "workload": f"C projectile on a {nb - 1}-atom graphite slab (2 layers) to 20 fs, adaptive dt, "
+                           "application potential set, one batched context"}
+        app = os.path.join(ROOT, "oracle", "_ref", "mdtrajsim")
+        if os.path.exists(app):
+            rd = os.path.join(tmp, "ref")
+            os.makedirs(rd)
+            for f in os.listdir(tmp):
+                if f.startswith("base.") or f == "ionpos.bin":
+                    shutil.copy(os.path.join(tmp, f), rd)
+            xy[:1].tofile(os.path.join(rd, "ionpos.bin"))
+            t0 = time.perf_counter()
+            subprocess.run([app, "base", "-i", "0"], cwd=rd, capture_output=True, check=True)
+            cw = time.perf_counter() - t0
+            row["cpu_baseline"] = {"value": 1.0 / cw, "unit": "impacts/s", "cores": 1, "kind": "reference",
+                                   "sample": "the unmodified mdtrajsim application (oracle build) on one impact "
+                                             "of the same sequence"}
+        out["impact_sequence"] = row
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+    # metal and ion potentials
+    cu = B.fcc(29, 24, 24, 8, pbc=(1, 1, 0), temp_k=300.0, seed=9)
+    top = cu["pos"][:, 2].max()
+    mol = B.c2h6_example()
+    zs, ps = [], []
+    for i in range(10):
+        for j in range(10):
+            zs.append(mol["z"])
+            ps.append(mol["pos"] - mol["pos"].mean(axis=0) + [4.0 + 8.5 * i, 4.0 + 8.5 * j, top + 3.0])
+    zs.append(np.array([18], np.int32))
+    ps.append(np.array([[40.0, 40.0, top + 8.0]]))
+    ms_sys = B.add_atoms(cu, np.concatenate(zs), np.concatenate(ps))
+    ms_sys["vel"][-1] = [0.0, 0.0, -0.05]
+    nm = len(ms_sys["z"])
+    c = M.Context(potentials=M.POT_AIREBO | M.POT_METAL, device=local)
+    c.set_system(ms_sys["z"], ms_sys["pos"], ms_sys["vel"], ms_sys["box"], ms_sys["pbc"], ms_sys["fixed"])
+    c.set_stream(stream.cuda_stream)
+    c.run(3, DT_FS, energies=False)
+    c.sync()
+    ms = timed(c, 100, DT_FS)
+    c.set_profiling(True)
+    for _ in range(5):
+        c.run(1, DT_FS, energies=False)
+    prof = c.profile_read()
+    c.set_profiling(False)
+    ptot = sum(v[0] for v in prof.values()) or 1.0
+    mkern = {k: {"ms_per_launch": v[0] / max(v[1], 1), "share": v[0] / ptot}
+             for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]}
+    row = {"value": nm * 100 / (ms * 1e-3), "unit": "atom-steps/s", "steps": 100, "atoms": nm, "kernels": mkern,
+           "workload": f"{len(cu['z'])} Cu (fcc slab), 100 ethane molecules, an Ar ion; AIREBO + FBZL + FLJ + Ackland, FP64"}
+    del c
+    try:
+        from oracle import ref
+        r = ref.RefSystem(ref.POT_AIREBO | ref.POT_METAL)
+        r.set_atoms(ms_sys["z"], ms_sys["pos"], ms_sys["vel"], ms_sys["box"], ms_sys["pbc"], ms_sys["fixed"])
+        res = r.run(3, DT_FS)
+        ts = res["times"]
+        step_s = (ts[-1] - ts[2]) / 2.0  # iterations 1 and 2, after the list build of iteration 0
+        row["cpu_baseline"] = {"value": nm / step_s, "unit": "atom-steps/s", "cores": 1, "kind": "reference",
+                               "sample": "the reference's FBZL, FLJ, REBO, AIREBO, ETors, Ackland (oracle build), "
+                                         "iterations 1..2 of the same system"}
+    except Exception as e:  # the oracle is test infrastructure; its absence is reported, not fatal
+        row["cpu_baseline"] = {"value": None, "sample": f"unavailable: {e}"}
+    out["metal_ion"] = row
+    return out
 
 # 512,000-atom diamond of the precision study (40^3 cells, a = 3.567 A,
 # Gaussian displacements sigma 0.05 A, 600 K, dt 0.5 fs)

@@ -453,11 +453,29 @@ bool write_xva_file(const IoJob& J, const char* h, const SnapLayout& L, std::str
   std::string s;
   s.reserve((size_t)n * 64 + 512);
   appendf(s, "%g\n%g\n%d\n", vs, ds, (int)n);
-  for (int64_t i = 0; i < n; i++) {
-    appendf(s, "%.2f %.2f %.2f\n", v[3 * i] / vs, v[3 * i + 1] / vs, v[3 * i + 2] / vs);
-    appendf(s, "%.2f %.2f %.2f\n", r[3 * i] / ds, r[3 * i + 1] / ds, r[3 * i + 2] / ds);
-    appendf(s, "%d %d %d\n", im[3 * i], im[3 * i + 1], im[3 * i + 2]);
+  // the atom lines, formatted by several threads over contiguous ranges and
+  // joined in order
+  const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(8, n / 4096));
+  std::vector<std::string> part(nt);
+  auto fmt = [&](int t) {
+    const int64_t b = n * t / nt, e = n * (t + 1) / nt;
+    std::string& q = part[t];
+    q.reserve((size_t)(e - b) * 64);
+    for (int64_t i = b; i < e; i++) {
+      appendf(q, "%.2f %.2f %.2f\n", v[3 * i] / vs, v[3 * i + 1] / vs, v[3 * i + 2] / vs);
+      appendf(q, "%.2f %.2f %.2f\n", r[3 * i] / ds, r[3 * i + 1] / ds, r[3 * i + 2] / ds);
+      appendf(q, "%d %d %d\n", im[3 * i], im[3 * i + 1], im[3 * i + 2]);
+    }
+  };
+  if (nt == 1) {
+    fmt(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(fmt, t);
+    fmt(0);
+    for (auto& x : th) x.join();
   }
+  for (const std::string& q : part) s += q;
   const CheckRec C = job_check(J, h, L);
   double t, dt, dtp;
   job_times(J, h, L, t, dt, dtp);
