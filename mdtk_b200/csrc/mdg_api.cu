@@ -1546,9 +1546,9 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
   if (c->has_list[2]) {
-    LAUNCH(c, "eam_density", k_eam_rho, nblk(c->n), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
+    LAUNCH(c, "eam_density", k_eam_rho, nblk(c->n * 32), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
            c->d_status);
-    LAUNCH(c, "metal_pairs", k_metal_pairs, nblk(c->n), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
+    LAUNCH(c, "metal_pairs", k_metal_pairs, nblk(c->n * 32), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
            c->d_gm);
   }
   if (step) {

@@ -258,19 +258,31 @@ inline void make_metal_params(MetalParams& M)
     }
 }
 
+MDG_HD double warp_sum(double x)
+{
+#if defined(__CUDA_ARCH__)
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+#endif
+  return x;
+}
+
 // Embedding of each metal atom (Ackland::F and rho, Ackland.cxx:208-232):
 // rho_i = sum of g over its metal partners, F_i = -sqrt(rho_i),
-// fp_i = dF/drho = 0.5 / F_i (0 when rho_i = 0); em gets F_i in eV.
+// fp_i = dF/drho = 0.5 / F_i (0 when rho_i = 0); em gets F_i in eV.  One
+// warp per atom: the lanes split the partner list, a fixed butterfly adds
+// their sums (deterministic).
 __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, double* fp, double* em,
                           unsigned int* status)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S.n) return;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= S.n) return;  // uniform per warp
   const double4 pi = S.pos[i];
   const int ti = (int)pi.w;
   if (!spec_metal(ti)) {
-    fp[i] = 0.0;
-    em[i] = 0.0;
+    if (lane == 0) {
+      fp[i] = 0.0;
+      em[i] = 0.0;
+    }
     return;
   }
   const MetalParams& M = *Mp;
@@ -279,7 +291,7 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
   const int* nl = L.list + (long)i * L.cap;
   const int nn = L.cnt[i];
   double rho = 0.0;
-  for (int q = 0; q < nn; q++) {
+  for (int q = lane; q < nn; q += 32) {
     const double4 pj = S.pos[nl[q]];
     const int tj = (int)pj.w;
     if (!spec_metal(tj)) continue;
@@ -287,6 +299,8 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
     double d;
     rho += ack_g(M, ti - kCu, tj - kCu, r, d);
   }
+  rho = warp_sum(rho);
+  if (lane != 0) return;
   if (!(rho >= 0.0)) atomicOr(status, ST_NONFINITE);
   const double F = -sqrt(rho);
   fp[i] = rho != 0.0 ? 0.5 / F : 0.0;
@@ -296,12 +310,13 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
 // Pair terms of every metal or ion pair of atom i (half of each pair's
 // energy to each end) plus the embedding's pair derivative
 // (fp_i + fp_j) dg/dr for metal pairs: gradient gm (eV/A) and energy em (eV)
-// of atom i, summed in list order (deterministic, no atomics).
+// of atom i.  One warp per atom, lanes over the partner list, a fixed
+// butterfly for the sums (deterministic, no atomics).
 __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ Mp, const double* fp, double* em,
                               double4* gm)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S.n) return;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= S.n) return;  // uniform per warp
   const MetalParams& M = *Mp;
   const double4 pi = S.pos[i];
   const int ti = (int)pi.w;
@@ -309,9 +324,9 @@ __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ 
   const V3 xi = v3(pi.x, pi.y, pi.z);
   const int* nl = L.list + (long)i * L.cap;
   const int nn = L.cnt[i];
-  double e = 0.0;
-  V3 g = v3(0.0, 0.0, 0.0);
-  for (int q = 0; q < nn; q++) {
+  const double fpi = fp[i];
+  double e = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  for (int q = lane; q < nn; q += 32) {
     const int j = nl[q];
     const double4 pj = S.pos[j];
     const int tj = (int)pj.w;
@@ -324,14 +339,21 @@ __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ 
     if (spec_metal(ti) && spec_metal(tj)) {
       double dg;
       ack_g(M, ti - kCu, tj - kCu, r, dg);
-      der += (fp[i] + fp[j]) * dg;
+      der += (fpi + fp[j]) * dg;
     }
     e += 0.5 * v;
     const double k = der * kAo / kEv / rA;  // d/dr in eV/A, along the unit vector
-    g += d * k;
+    gx += d.x * k;
+    gy += d.y * k;
+    gz += d.z * k;
   }
+  e = warp_sum(e);
+  gx = warp_sum(gx);
+  gy = warp_sum(gy);
+  gz = warp_sum(gz);
+  if (lane != 0) return;
   em[i] = (spec_metal(ti) ? em[i] : 0.0) + e / kEv;
-  gm[i] = make_double4(g.x, g.y, g.z, 0.0);
+  gm[i] = make_double4(gx, gy, gz, 0.0);
 }
 
 }  // namespace mdg
