@@ -132,3 +132,41 @@ def test_flag_checks():
     c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
     with pytest.raises(M.MdgError):
         c.adjoint_forward(2, 0.5, 1)
+
+
+def test_metal_state_files_both_ways(tmp_path):
+    """Metal and ion atoms in SimLoopSaver's files: ElementID of Cu, Au, Ar in
+    ".z"; the reference loads our state and we load the reference's."""
+    s = hydrocarbon_on_metal(79, seed=31)
+    top = s["pos"][:, 2].max()
+    s = B.add_atoms(s, [18], [[4.0, 4.0, top + 4.0]])
+    c, r = both(s, task_mode=1)
+    c.run(5, 0.25)
+    r.run(5, 0.25)
+    c.write_state(str(tmp_path / "dev"), zip=M.ZIP_GZIP)
+    r2 = ref.RefSystem(RPOT)
+    assert r2.load_state(str(tmp_path / "dev"), 5) == 127
+    a = r2.atoms()
+    pos, vel, img = c.get_state()
+    assert np.array_equal(a["z"], s["z"]) and np.allclose(a["pos"], pos, rtol=1e-14, atol=0)
+    ref.set_zip(0)
+    r.write_state(str(tmp_path / "ref"))
+    d = M.Context(potentials=POT, task_mode=1)
+    assert d.load_state(str(tmp_path / "ref"), 5) == 127
+    e1, _, g1 = d.compute()
+    e0, _, g0 = r.compute()
+    assert abs(e1 - e0) <= 1e-12 * abs(e0) and np.linalg.norm(g1 - g0) <= 1e-10 * np.linalg.norm(g0)
+
+
+def test_fp32_mixed_with_metal():
+    """The mixed mode keeps the metal and ion kernels in FP64; its error stays
+    that of the hydrocarbon terms."""
+    s = hydrocarbon_on_metal(29, seed=32)
+    c64 = M.Context(potentials=POT)
+    c64.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    c32 = M.Context(potentials=POT, precision=M.PREC_FP32_MIXED)
+    c32.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    e64, t64, g64 = c64.compute()
+    e32, t32, g32 = c32.compute()
+    assert t32[3] == t64[3]  # metal and ion energies identical
+    assert np.linalg.norm(g32 - g64) <= 1e-5 * np.linalg.norm(g64)
