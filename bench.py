@@ -144,6 +144,9 @@ def main():
     ap.add_argument("--precision-study", action="store_true",
                     help="instead of the throughput line: the FP32-mixed vs FP64 study on the 512,000-atom diamond")
     ap.add_argument("--study-steps", type=int, default=5000)
+    ap.add_argument("--rows", default=None,
+                    help="instead of the throughput line: only the measurements of the rows around the step "
+                         "(comma-separated subset of bath,files,impacts,metal; 'all')")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -180,6 +183,17 @@ def main():
 
     if args.precision_study:
         return precision_study(args, local, rank)
+    if args.rows:
+        s = build_system(seed=1 + rank)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+        want = None if args.rows == "all" else set(args.rows.split(","))
+        out = next_rows(M, s, local, stream, flush, None, want)
+        if rank == 0:
+            print(json.dumps({"rows": out}))
+        reps.close()
+        return 0
 
     s = build_system(seed=1 + rank)
     n = len(s["z"])
@@ -261,7 +275,7 @@ def main():
     t_e2e = time.perf_counter() - t0
     t_e2e = reps.max(t_e2e)
     e2e = {"value": world * n * args.e2e_steps / t_e2e, "unit": "atom-steps/s",
-           "h2d_bytes_per_step": 2 * 32 * n, "d2h_bytes_per_step": 2 * 32 * n + 16,
+           "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 2 * 24 * n + 4 * 8,
            "steps": args.e2e_steps, "timer": "host wall clock around mdg_step_host calls (each ends synchronised)"}
 
     # FP32-mixed variant on the same workload, from the FP64 run's final state:
@@ -472,7 +486,7 @@ def main():
 ADJ_ATOMS, ADJ_STEPS, ADJ_DT_FS, ADJ_EVERY = 4096, 200, 0.5, 20
 
 
-def next_rows(M, s, local, stream, flush, plain_rate):
+def next_rows(M, s, local, stream, flush, plain_rate, want=None):
     """Throughput of the rows around the step, one GPU:
 
     * SimLoop's thermal bath (universe, 300 K, 1e13 / s) with adaptive dt on
@@ -480,7 +494,7 @@ def next_rows(M, s, local, stream, flush, plain_rate):
     * the same liquid writing its files from device snapshots, at
       mdtrajsim's intervals and at ten times their frequency (wall clock, the
       files included);
-    * mdtrajsim's impact sequence: 64 impacts of a C projectile on a 900-atom
+    * mdtrajsim's impact sequence: 64 impacts of a C projectile on a 256-atom
       graphite slab to 20 fs, one batched context with the application's
       files, against the unmodified mdtrajsim application on the host for
       one impact;
@@ -488,11 +502,7 @@ def next_rows(M, s, local, stream, flush, plain_rate):
       18,432-atom Cu slab (AIREBO + FBZL + FLJ + Ackland), against the
       reference's own classes on the host (3 steps).
     CUDA events on the library stream unless said otherwise."""
-    import shutil
-    import tempfile
     import torch
-    from mdtk_b200 import builders as B
-    from mdtk_b200 import trajsim as T
     out = {}
     n = len(s["z"])
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -505,7 +515,25 @@ def next_rows(M, s, local, stream, flush, plain_rate):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
+    def on(name):
+        return want is None or name in want
+
+    def rel(v):
+        return v / plain_rate if plain_rate else None
+
     # thermal bath + adaptive dt
+    if on("bath"):
+        _row_bath(M, s, local, stream, timed, n, out, rel)
+    if on("files"):
+        _row_files(M, s, local, stream, n, out, rel)
+    if on("impacts"):
+        _row_impacts(M, local, out)
+    if on("metal"):
+        _row_metal(M, local, stream, timed, out)
+    return out
+
+
+def _row_bath(M, s, local, stream, timed, n, out, rel):
     c = M.Context(potentials=M.POT_AIREBO, device=local)
     c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
     c.set_stream(stream.cuda_stream)
@@ -515,11 +543,14 @@ def next_rows(M, s, local, stream, flush, plain_rate):
     c.sync()
     ms = timed(c, 100, DT_FS)
     out["bath_adaptive_dt"] = {"value": n * 100 / (ms * 1e-3), "unit": "atom-steps/s", "steps": 100,
-                               "over_plain": n * 100 / (ms * 1e-3) / plain_rate,
+                               "over_plain": rel(n * 100 / (ms * 1e-3)),
                                "workload": "headline liquid, universe bath 300 K, gamma 1e13/s, adaptive dt"}
     del c
 
-    # files from device snapshots
+
+def _row_files(M, s, local, stream, n, out, rel):
+    import shutil
+    import tempfile
     tmp = tempfile.mkdtemp(prefix="mdg_out_")
     try:
         c = M.Context(potentials=M.POT_AIREBO, device=local)
@@ -539,13 +570,19 @@ def next_rows(M, s, local, stream, flush, plain_rate):
             nfiles = len(os.listdir(os.path.join(tmp, str(flush_it))))
             out["files_every_%d" % flush_it] = {
                 "value": n * 2000 / wall, "unit": "atom-steps/s (wall clock, files written)", "steps": 2000,
-                "files": nfiles, "over_plain": n * 2000 / wall / plain_rate,
+                "files": nfiles, "over_plain": rel(n * 2000 / wall),
                 "workload": "headline liquid, " + label}
         del c
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
-    # mdtrajsim impact sequence
+
+
+def _row_impacts(M, local, out):
+    import shutil
+    import tempfile
+    from mdtk_b200 import builders as B
+    from mdtk_b200 import trajsim as T
     tmp = tempfile.mkdtemp(prefix="mdg_traj_")
     try:
         slab = B.graphite_slab(2, 8, 4, temp_k=0.0, seed=3)
@@ -595,7 +632,10 @@ def next_rows(M, s, local, stream, flush, plain_rate):
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
-    # metal and ion potentials
+
+
+def _row_metal(M, local, stream, timed, out):
+    from mdtk_b200 import builders as B
     cu = B.fcc(29, 24, 24, 8, pbc=(1, 1, 0), temp_k=300.0, seed=9)
     top = cu["pos"][:, 2].max()
     mol = B.c2h6_example()
@@ -639,7 +679,6 @@ def next_rows(M, s, local, stream, flush, plain_rate):
     except Exception as e:  # the oracle is test infrastructure; its absence is reported, not fatal
         row["cpu_baseline"] = {"value": None, "sample": f"unavailable: {e}"}
     out["metal_ion"] = row
-    return out
 
 # 512,000-atom diamond of the precision study (40^3 cells, a = 3.567 A,
 # Gaussian displacements sigma 0.05 A, 600 K, dt 0.5 fs)

@@ -962,6 +962,8 @@ struct mdg_ctx {
   double* d_red_part = nullptr;
   double* d_energy = nullptr;   // [4] rebo, lj, tors, kin of the last evaluation
   double* d_elog = nullptr;     // per-step energy log [cap * 4]
+  double* h_elog = nullptr;     // its pinned host copy
+  int64_t h_elog_cap = 0;
   int64_t elog_cap = 0;
 
   CijTable cij;
@@ -1239,6 +1241,9 @@ void free_system(mdg_ctx* c)
   std::memset(&c->bt, 0, sizeof(c->bt));
   if (c->h_stage) cudaFreeHost(c->h_stage);
   c->h_stage = nullptr;
+  if (c->h_elog) cudaFreeHost(c->h_elog);
+  c->h_elog = nullptr;
+  c->h_elog_cap = 0;
   if (c->d_io) cudaFree(c->d_io);
   c->d_io = nullptr;
   c->pos = c->vel = c->acc = c->grad = nullptr;
@@ -2323,9 +2328,21 @@ static int init_first_step(mdg_ctx* c)
   return MDG_OK;
 }
 
+// Per-step potential and total energies from the pinned log of the last run.
+static void fill_energy_log(mdg_ctx* c, int nsteps, double* epot, double* etot)
+{
+  const double* h = c->h_elog;
+  for (int s = 0; s < nsteps; s++) {
+    double ep = (h[4 * s] + h[4 * s + 1]) + h[4 * s + 2];
+    if (epot) epot[s] = ep * c->unit_e;
+    if (etot) etot[s] = (ep + h[4 * s + 3]) * c->unit_e;
+  }
+}
+
 // fresh: a new SimLoop::execute (dt_prev = dt); else the continuation of
 // the previous call's loop
-static int run_steps(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot, bool fresh)
+static int run_steps(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot, bool fresh,
+                     bool defer_log = false)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
@@ -2372,15 +2389,19 @@ static int run_steps(mdg_ctx* c, int nsteps, double dt, double* epot, double* et
   rc = io_run_end(c);
   if (rc) return rc;
   if (log) {
-    std::vector<double> h((size_t)nsteps * 4);
-    CK(cudaMemcpyAsync(h.data(), c->d_elog, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (c->h_elog_cap < (int64_t)nsteps * 4) {
+      if (c->h_elog) cudaFreeHost(c->h_elog);
+      c->h_elog = nullptr;
+      if (cudaHostAlloc((void**)&c->h_elog, (size_t)nsteps * 4 * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
+        return fail(MDG_ERR_CUDA, "cudaHostAlloc (energy log)");
+      c->h_elog_cap = (int64_t)nsteps * 4;
+    }
+    CK(cudaMemcpyAsync(c->h_elog, c->d_elog, (size_t)nsteps * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    if (defer_log) return MDG_OK;  // the caller synchronises, then calls fill_energy_log
     rc = read_status(c);
     if (rc) return rc;
-    for (int s = 0; s < nsteps; s++) {
-      double ep = (h[4 * s] + h[4 * s + 1]) + h[4 * s + 2];
-      if (epot) epot[s] = ep * c->unit_e;
-      if (etot) etot[s] = (ep + h[4 * s + 3]) * c->unit_e;
-    }
+    fill_energy_log(c, nsteps, epot, etot);
     return MDG_OK;
   }
   return launch_check(c);
@@ -2647,12 +2668,17 @@ int mdg_step_host(mdg_ctx* c, int nsteps, double dt, double* pos, double* vel, d
   CK(cudaMemcpyAsync(io + 3 * (size_t)n, vel, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   State S = c->S();
   LAUNCH(c, "state_unpack", k_state_unpack, nblk(n), kThreads, S, io, c->unit_len, c->unit_vel);
-  int rc = mdg_run(c, nsteps, dt, epot, etot);
+  // one synchronisation for the whole call: the energy log, the state and
+  // the status come back together
+  int rc = run_steps(c, nsteps, dt, epot, etot, true, true);
   if (rc) return rc;
   LAUNCH(c, "state_pack", k_state_pack, nblk(n), kThreads, S, io, c->unit_len, c->unit_vel);
   CK(cudaMemcpyAsync(pos, io, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(vel, io + 3 * (size_t)n, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  return read_status(c);
+  rc = read_status(c);
+  if (rc) return rc;
+  if (epot || etot) fill_energy_log(c, nsteps, epot, etot);
+  return MDG_OK;
 }
 
 int mdg_pipe_peak(int device, int fp32, double* tflops)
