@@ -266,11 +266,51 @@ MDG_HD double warp_sum(double x)
   return x;
 }
 
+// The partners of atom i within the potentials' range, handed to the lanes
+// 32 at a time: each lane tests one list entry, a ballot packs the ones in
+// range into a per-warp queue in list order, and every full queue is
+// processed with all lanes busy (two thirds of a Verlet list lie in its
+// skin).  f(j, lane) is called once per queued partner; deterministic.
+template <class F>
+__device__ void for_partners(const State& S, const NList& L, int i, const V3& xi, const Box& box, double rcut_A,
+                             bool metal_only, int* wq, F&& f)
+{
+  const int lane = threadIdx.x & 31;
+  const int* nl = L.list + (long)i * L.cap;
+  const int nn = L.cnt[i];
+  int cnt = 0;  // queued, the same in every lane
+  for (int base = 0; base < nn; base += 32) {
+    const int q = base + lane;
+    bool keep = false;
+    int j = -1;
+    if (q < nn) {
+      j = nl[q];
+      const double4 pj = S.pos[j];
+      if (!metal_only || spec_metal((int)pj.w)) keep = norm2(depos(box, xi, v3(pj.x, pj.y, pj.z))) < rcut_A * rcut_A;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+    if (keep && pos < 32) wq[pos] = j;
+    const int total = cnt + __popc(m);
+    __syncwarp();
+    if (total >= 32) {
+      f(wq[lane]);
+      __syncwarp();
+      if (keep && pos >= 32) wq[pos - 32] = j;
+      __syncwarp();
+      cnt = total - 32;
+    } else {
+      cnt = total;
+    }
+  }
+  if (lane < cnt) f(wq[lane]);
+  __syncwarp();
+}
+
 // Embedding of each metal atom (Ackland::F and rho, Ackland.cxx:208-232):
 // rho_i = sum of g over its metal partners, F_i = -sqrt(rho_i),
 // fp_i = dF/drho = 0.5 / F_i (0 when rho_i = 0); em gets F_i in eV.  One
-// warp per atom: the lanes split the partner list, a fixed butterfly adds
-// their sums (deterministic).
+// warp per atom, a fixed butterfly for the sum.
 __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, double* fp, double* em,
                           unsigned int* status)
 {
@@ -288,6 +328,8 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
   const MetalParams& M = *Mp;
   const Box& box = box_of(S, i);
   const V3 xi = v3(pi.x, pi.y, pi.z);
+  // (the density terms are cheap: the lanes take the list entries in turn;
+  // queueing the partners in range, as the pair kernel does, cost more here)
   const int* nl = L.list + (long)i * L.cap;
   const int nn = L.cnt[i];
   double rho = 0.0;
@@ -310,11 +352,12 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
 // Pair terms of every metal or ion pair of atom i (half of each pair's
 // energy to each end) plus the embedding's pair derivative
 // (fp_i + fp_j) dg/dr for metal pairs: gradient gm (eV/A) and energy em (eV)
-// of atom i.  One warp per atom, lanes over the partner list, a fixed
+// of atom i.  One warp per atom over the partners in range, a fixed
 // butterfly for the sums (deterministic, no atomics).
 __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ Mp, const double* fp, double* em,
                               double4* gm)
 {
+  __shared__ int qbuf[kThreads];
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= S.n) return;  // uniform per warp
   const MetalParams& M = *Mp;
@@ -322,18 +365,14 @@ __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ 
   const int ti = (int)pi.w;
   const Box& box = box_of(S, i);
   const V3 xi = v3(pi.x, pi.y, pi.z);
-  const int* nl = L.list + (long)i * L.cap;
-  const int nn = L.cnt[i];
   const double fpi = fp[i];
   double e = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-  for (int q = lane; q < nn; q += 32) {
-    const int j = nl[q];
+  for_partners(S, L, i, xi, box, M.rcut / kAo, false, qbuf + (threadIdx.x & ~31), [&](int j) {
     const double4 pj = S.pos[j];
     const int tj = (int)pj.w;
     const V3 d = depos(box, xi, v3(pj.x, pj.y, pj.z));
     const double rA = sqrt(norm2(d));
     const double r = rA * kAo;
-    if (r >= M.rcut) continue;
     double der;
     const double v = metal_pair(M, ti, tj, r, der);
     if (spec_metal(ti) && spec_metal(tj)) {
@@ -346,7 +385,7 @@ __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ 
     gx += d.x * k;
     gy += d.y * k;
     gz += d.z * k;
-  }
+  });
   e = warp_sum(e);
   gx = warp_sum(gx);
   gy = warp_sum(gy);
