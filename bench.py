@@ -207,6 +207,10 @@ def main():
     # warm-up (also builds the lists and the initial accelerations)
     ctx.run(max(args.warmup, 3), DT_FS, energies=False)
     ctx.sync()
+    mode, ms_dir, ms_pair = ctx.task_mode()
+    ovl, rblocks = ctx.tuned_launch()
+    tuned = {"rebo_task_mode": "per bond" if mode == 2 else "directed", "eval_ms_directed": ms_dir,
+             "eval_ms_per_bond": ms_pair, "overlap": bool(ovl), "rebo_blocks": rblocks}
 
     # L2 flush buffer (the per-step working set is below the 126 MB L2)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -462,6 +466,7 @@ def main():
                        "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches, "clocks": clk, "kernels": kern, "roofline": roof, "e2e": e2e,
+            "autotuner": tuned,
             "fp64_peak_tflops": fp64_peak,
             "variants": {"fp32_mixed": mixed, "batched": batched, "adjoint": adjoint},
         }
