@@ -426,21 +426,27 @@ __global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NLi
 // round with every lane busy (the last round excepted).  Pairs that need
 // b*_ij or a connectivity gradient are compacted, in list order, into the
 // atom's special list.
+constexpr int kLjGroup = 16;  // lanes per atom in the plain LJ pair kernel (a divisor of 32)
 template <class Real>
 __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* inr,
                                                        const int* inr_cnt, const int* nbonds, ForceOut O,
                                                        SpecialTasks Tk, unsigned int* status)
 {
   if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
-  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (a >= S.n) return;  // whole warps
+  // kLjGroup lanes per atom: an atom has ~30 in-range partners, so a group
+  // of 16 keeps more lanes busy than a whole warp would
+  const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLjGroup;
+  const int lane = threadIdx.x & 31, gl = lane % kLjGroup, gbase = lane - gl;
+  const bool live = gid < S.n;
+  if (__all_sync(0xffffffffu, !live)) return;  // whole warps
+  const int a = live ? gid : S.n - 1;
   const double4 pa = S.pos[a];
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
-  const int cnt = inr_cnt[a];
+  const int cnt = live ? inr_cnt[a] : 0;
   const int* q = inr + (long)a * L.cap;
-  const unsigned below = (1u << lane) - 1u;
+  const unsigned gmask = (kLjGroup == 32) ? 0xffffffffu : (((1u << kLjGroup) - 1u) << gbase);
+  const unsigned below = ((1u << lane) - 1u) & gmask;
   SinkT<Real> sk;
   sk.a = a;
   sk.g = v3(0, 0, 0);
@@ -448,10 +454,12 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
   sk.W = nullptr;
   double e = 0.0;
   int nsp = 0;
-  for (int base = 0; base < cnt; base += 32) {
+  int wcnt = cnt;  // the warp's longest list bounds its loop
+  for (int o = 16; o > 0; o >>= 1) wcnt = max(wcnt, __shfl_xor_sync(0xffffffffu, wcnt, o));
+  for (int base = 0; base < wcnt; base += kLjGroup) {
     int kind = 0, b = -1;
-    if (base + lane < cnt) {
-      b = q[base + lane];
+    if (base + gl < cnt) {
+      b = q[base + gl];
       kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
     }
     const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
@@ -459,16 +467,16 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
       const int pos = nsp + __popc(m & below);
       if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
     }
-    nsp += __popc(m);
+    nsp += __popc(m & gmask);
   }
   double gx = sk.g.x, gy = sk.g.y, gz = sk.g.z;
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = kLjGroup / 2; o > 0; o >>= 1) {
     gx += __shfl_xor_sync(0xffffffffu, gx, o);
     gy += __shfl_xor_sync(0xffffffffu, gy, o);
     gz += __shfl_xor_sync(0xffffffffu, gz, o);
     e += __shfl_xor_sync(0xffffffffu, e, o);
   }
-  if (lane == 0) {
+  if (live && gl == 0) {
     O.glj[a] = make_double4(gx, gy, gz, 0.0);
     O.e_lj[a] = e;
     if (nsp > Tk.cap) {
@@ -1514,10 +1522,10 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
     if (ovl) CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
     if (f32p)
-      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
+      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * kLjGroup), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
              c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
     else
-      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * 32), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
+      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * kLjGroup), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
              c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
     ScanPair sp;
     sp.in[0] = c->spc.cnt;
