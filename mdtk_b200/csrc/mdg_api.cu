@@ -642,25 +642,111 @@ __global__ void k_lj_special_pair(const ReboParams* P, const TB* Tb, LJParams LP
   }
 }
 
+// The gather split over kGatherLanes lanes per atom: lane l takes the bond
+// slots l, l + kGatherLanes, ... of both the bond-record gather and the LJ
+// middle-bond gather (the same terms as gather_atom + mid_gather_atom); lane 0
+// adds the atom's own gradients.  The lanes' sums are combined by a fixed
+// butterfly, so every lane holds the same, deterministic total.
+constexpr int kGatherLanes = 4;
+__device__ V3 gather_lanes(const BondList& B, const ForceOut& O, const SpecialTasks& X, int a, int with_lj,
+                           const double4* gextra, int l)
+{
+  V3 g = v3(0.0, 0.0, 0.0);
+  if (l == 0) {
+    const double4 g0 = O.gown[a];
+    g = v3(g0.x, g0.y, g0.z);
+    if (with_lj) {
+      const double4 g1 = O.glj[a];
+      g += v3(g1.x, g1.y, g1.z);
+    }
+    if (gextra) {
+      const double4 g2 = gextra[a];
+      g += v3(g2.x, g2.y, g2.z);
+    }
+  }
+  const int nb = B.nb[a];
+  for (int s = l; s < nb; s += kGatherLanes) {
+    const int q = a * B.mb + s;
+    const int k = B.bj[q];
+    const int r = B.brev[q];
+    if (r >= 0) {  // (a partner list truncated by an overflow is already flagged)
+      const double* Ak = O.A + ((long)k * O.mb + r) * 3;
+      g += v3(Ak[0], Ak[1], Ak[2]);
+    }
+    const double df = B.bd[q].x;
+    if (df != 0.0) {
+      double wa = 0.0;
+      for (int t = 0; t < nb; t++) {
+        if (t == s) continue;
+        const int qt = a * B.mb + t;
+        if (B.brev[qt] < 0) continue;
+        wa += O.W[(long)B.bj[qt] * O.mb + B.brev[qt]];
+      }
+      double wm = 0.0;
+      const int nbm = B.nb[k];
+      for (int t = 0; t < nbm; t++) {
+        const int qt = k * B.mb + t;
+        const int cc = B.bj[qt];
+        if (cc == a || B.brev[qt] < 0) continue;
+        wm += O.W[(long)cc * O.mb + B.brev[qt]];
+      }
+      const double4 u = B.bu[q];
+      g += v3(u.x, u.y, u.z) * (df * (wa + wm));
+    }
+    if (with_lj) {
+      // middle-bond terms of the LJ special pairs (mid_gather_atom)
+      const int t0 = X.off[k], t1 = X.off[k + 1] < X.task_cap ? X.off[k + 1] : X.task_cap;
+      for (int t = t0; t < t1; t++) {
+        const int4 e = X.mid[t];
+        if (!e.w || e.x != a) continue;
+        const double4 u = B.bu[a * B.mb + e.y];
+        g += v3(u.x, u.y, u.z) * X.midc[t];
+      }
+      const double4 ua = B.bu[q];
+      const int nbk = B.nb[k];
+      for (int qq = 0; qq < nbk; qq++) {
+        const int lo = B.bj[k * B.mb + qq];
+        const int u0 = X.off[lo], u1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+        for (int t = u0; t < u1; t++) {
+          const int4 e = X.mid[t];
+          if (!e.w || e.x != k || e.z != a) continue;
+          g += v3(ua.x, ua.y, ua.z) * X.midc[t];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = kGatherLanes / 2; o > 0; o >>= 1) {
+    g.x += __shfl_xor_sync(0xffffffffu, g.x, o);
+    g.y += __shfl_xor_sync(0xffffffffu, g.y, o);
+    g.z += __shfl_xor_sync(0xffffffffu, g.z, o);
+  }
+  return g;
+}
+
 __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, const double4* gm)
 {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= B.n) return;
-  V3 g = gather_atom(B, O, a, with_lj, gm);
-  if (with_lj) g += mid_gather_atom(B, Tk, a);
-  grad[a] = make_double4(g.x, g.y, g.z, 0.0);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = t / kGatherLanes, l = t % kGatherLanes;
+  if (__all_sync(0xffffffffu, a >= B.n)) return;  // whole warps
+  const int aa = a < B.n ? a : B.n - 1;
+  const V3 g = gather_lanes(B, O, Tk, aa, with_lj, gm, l);
+  if (a < B.n && l == 0) grad[a] = make_double4(g.x, g.y, g.z, 0.0);
 }
 
 // The gather and the end of a step in one pass (eq 2-4 and applyPBC): the
 // gather reads bond records and unit vectors, never positions, so each atom's
-// velocity, acceleration and wrap follow its own gradient at once.
+// velocity, acceleration and wrap follow its own gradient at once (on the
+// atom's first lane).
 __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, StepDev P,
                             double* ekin, const double4* gm, unsigned int* status)
 {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= B.n) return;
-  V3 g = gather_atom(B, O, a, with_lj, gm);
-  if (with_lj) g += mid_gather_atom(B, Tk, a);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = t / kGatherLanes, l = t % kGatherLanes;
+  if (__all_sync(0xffffffffu, a >= B.n)) return;  // whole warps
+  const int aa = a < B.n ? a : B.n - 1;
+  const V3 g = gather_lanes(B, O, Tk, aa, with_lj, gm, l);
+  if (a >= B.n || l != 0) return;
   grad[a] = make_double4(g.x, g.y, g.z, 0.0);
   if (P.ekin_pre) {
     const double4 v0 = S.vel[a];
@@ -1565,14 +1651,14 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
            c->d_gm);
   }
   if (step) {
-    LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
+    LAUNCH(c, "gather_verlet_vel", k_gather_vv, nblk(c->n * kGatherLanes), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, S,
            *step, c->e_kin, c->d_gm, c->d_status);
     if (step->vmax)
       LAUNCH(c, "dt_update", k_dt_update, nblk(c->nsys), kThreads, c->nsys, c->d_vmax, c->d_dt, c->d_dt_prev, c->d_time,
              c->timeaccel, c->stop_final ? c->d_stop : nullptr, c->time_final_s / kFs);
   }
   else
-    LAUNCH(c, "gather", k_gather, nblk(c->n), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, c->d_gm);
+    LAUNCH(c, "gather", k_gather, nblk(c->n * kGatherLanes), kThreads, B, c->fo, lj ? 1 : 0, c->spc, c->grad, c->d_gm);
   return launch_check(c);
 }
 
