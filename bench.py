@@ -235,6 +235,22 @@ def main():
     total_ms = reps.max(total_ms)
     value = aggregate_rate(n * args.steps, world, total_ms * 1e-3)
 
+    # the same steps with ordinary launches (programmatic dependent launch off), for comparison
+    ctx.set_dependent_launch(False)
+    ctx.run(3, DT_FS, energies=False)
+    nab = min(args.steps, 100)
+    torch.cuda.synchronize()
+    for k in range(nab):
+        flush.zero_()
+        ev[k][0].record(stream)
+        ctx.run(1, DT_FS, energies=False)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    tuned["dependent_launch"] = True
+    tuned["ms_per_step_ordinary_launch"] = sum(a.elapsed_time(b) for a, b in ev[:nab]) / nab
+    ctx.set_dependent_launch(True)
+    ctx.run(1, DT_FS, energies=False)
+
     # per-kernel device times over a short profiled window (same stream)
     ctx.set_profiling(True)
     prof_steps = 20

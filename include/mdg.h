@@ -408,6 +408,13 @@ int mdg_snapshots_load(mdg_ctx* ctx, int sys, const char* path);
  * counterpart. */
 int mdg_tuned_launch(mdg_ctx* ctx, int* overlap, int* rebo_blocks);
 
+/* Programmatic dependent launch of the step's kernels (default on): each
+ * kernel may be scheduled while the one before it on its stream drains and
+ * waits on the device for that kernel's completion before its first read, so
+ * results are those of ordinary launches; on = 0 launches them ordinarily.
+ * No reference counterpart. */
+int mdg_set_dependent_launch(mdg_ctx* ctx, int on);
+
 /* ---- Batched systems ----
  * Many independent systems of uneven size in one context (the reference runs
  * impacts one after another, mdtrajsim/main.cpp:295-345): atoms of system s

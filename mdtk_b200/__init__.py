@@ -110,6 +110,7 @@ def lib():
                                     ctypes.POINTER(ctypes.c_float)]
         L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_tuned_launch.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.mdg_set_dependent_launch.argtypes = [vp, ctypes.c_int]
         L.mdg_set_thermal_bath.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp,
                                            ctypes.POINTER(ctypes.c_uint8)]
         L.mdg_set_adaptive_dt.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
@@ -423,6 +424,10 @@ class Context:
         b = ctypes.c_int()
         _check(lib().mdg_tuned_launch(self.h, ctypes.byref(o), ctypes.byref(b)))
         return o.value, b.value
+
+    def set_dependent_launch(self, on: bool):
+        """Programmatic dependent launch of the step's kernels (default on)."""
+        _check(lib().mdg_set_dependent_launch(self.h, 1 if on else 0))
 
     def batch_energies(self) -> np.ndarray:
         """[nsys, 4]: REBO, LJ, torsion, kinetic energy of each system."""

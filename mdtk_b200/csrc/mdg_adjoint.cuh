@@ -75,6 +75,7 @@ struct DualBonds {
 // rebuilt on duals whose positions carry tan.
 __global__ void k_adj_bonds(State S, const double4* tan, ReboParams P, BondList B, DualBonds D)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= S.n) return;
   const double4 pa = S.pos[a], ua = tan[a];
@@ -111,6 +112,7 @@ __global__ void k_adj_bonds(State S, const double4* tan, ReboParams P, BondList 
 __global__ void k_adj_rebo(const ReboParams* P, const ReboTables* T, BondListT<dual> B, TorsParams TP, int do_rebo,
                            int do_tors, ForceOutT<dual> O, unsigned int* status)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   ReboT<dual, ReboTables> R{*P, *T, B, status};
@@ -121,6 +123,7 @@ __global__ void k_adj_rebo(const ReboParams* P, const ReboTables* T, BondListT<d
 // (the products in the order cij_build_atom forms them).
 __global__ void k_adj_cij(BondListT<dual> B, CijTable T, dual* w)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   auto fb = [&](int c, int o) -> dual {
@@ -143,6 +146,7 @@ __global__ void k_adj_cij(BondListT<dual> B, CijTable T, dual* w)
 __global__ void k_adj_lj_plain(LJParams P, CijTableT<dual> T, State S, NList L, const double4* tan,
                                ForceOutT<dual> O)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= S.n) return;
   const double4 pa = S.pos[a];
@@ -167,6 +171,7 @@ __global__ void k_adj_lj_special(const ReboParams* P, const ReboTables* Tb, LJPa
                                  CijTableT<dual> T, State S, SpecialTasksT<dual> Tk, const double4* tan,
                                  unsigned int* status)
 {
+  pdl_enter();
   const int total = min(Tk.off[S.n], Tk.task_cap);
   ReboT<dual, ReboTables> R{*P, *Tb, B, status};
   LJT<dual, ReboTables> X{LP, R, T};
@@ -176,12 +181,14 @@ __global__ void k_adj_lj_special(const ReboParams* P, const ReboTables* Tb, LJPa
 
 __global__ void k_adj_lj_reduce(BondListT<dual> B, SpecialTasksT<dual> Tk, ForceOutT<dual> O)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a < B.n) lj_reduce_atom(B, Tk, O, a);
 }
 
 __global__ void k_adj_gather(BondListT<dual> B, ForceOutT<dual> O, int with_lj, SpecialTasksT<dual> Tk, dual4* g)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   V3T<dual> gg = gather_atom(B, O, a, with_lj, (const dual4*)nullptr);
@@ -193,6 +200,7 @@ __global__ void k_adj_gather(BondListT<dual> B, ForceOutT<dual> O, int with_lj, 
 // A_0/m (mode 1, the initial accelerations); 0 for fixed atoms.
 __global__ void k_adj_dir(State S, const double4* lv, const double4* la, double dt, int mode, double4* tan)
 {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   if (S.fixed && S.fixed[i]) { tan[i] = make_double4(0.0, 0.0, 0.0, 0.0); return; }
@@ -212,6 +220,7 @@ __global__ void k_adj_dir(State S, const double4* lv, const double4* la, double 
 __global__ void k_adj_update(State S, const dual4* g, double4* lx, double4* lv, double4* la, double dt, int mode,
                              double seed_e)
 {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   const dual4 gi = g[i];
@@ -231,6 +240,7 @@ __global__ void k_adj_update(State S, const dual4* g, double4* lx, double4* lv, 
 // per parameter in a fixed order; theta += scale_t * tangent + scale_v * value.
 __global__ void k_adj_par(const dual* dp, int n, double scale_t, double scale_v, double* theta, double* last)
 {
+  pdl_enter();
   __shared__ double sv[128], sd[128];
   const int k = blockIdx.x;
   double a = 0.0, b = 0.0;

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mdg.h"
@@ -63,6 +64,7 @@ __device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, do
 // list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
 __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, int mask, double* part)
 {
+  pdl_enter();
   __shared__ double s1[3][kThreads / 32], s2[3][kThreads / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double d1[3] = {0.0, 0.0, 0.0}, d2[3] = {0.0, 0.0, 0.0};
@@ -104,6 +106,7 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
 // not depend on the order they are met in).
 __global__ void k_disp_final(const double* part, int nparts, double trigger, int* need, int* force)
 {
+  pdl_enter();
   const int lane = threadIdx.x;
   if (lane >= 32) return;
   double t1 = 0.0, t2 = 0.0;
@@ -125,6 +128,7 @@ __global__ void k_disp_final(const double* part, int nparts, double trigger, int
 
 __global__ void k_cell_clear(Grid g, const int* need)
 {
+  pdl_enter();
   if (!*need) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < g.ncell) { g.ccount[c] = 0; g.ccursor[c] = 0; }
@@ -132,6 +136,7 @@ __global__ void k_cell_clear(Grid g, const int* need)
 
 __global__ void k_cell_count(State S, Grid g, const int* need)
 {
+  pdl_enter();
   if (!*need) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < S.n) atomicAdd(&g.ccount[cell_of(g, S, i)], 1);
@@ -140,6 +145,7 @@ __global__ void k_cell_count(State S, Grid g, const int* need)
 // single-block exclusive scan of the cell counts
 __global__ void k_cell_scan(Grid g, const int* need)
 {
+  pdl_enter();
   if (!*need) return;
   __shared__ int part[1024];
   int t = threadIdx.x, nt = blockDim.x;
@@ -161,6 +167,7 @@ __global__ void k_cell_scan(Grid g, const int* need)
 
 __global__ void k_cell_fill(State S, Grid g, const int* need)
 {
+  pdl_enter();
   if (!*need) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
@@ -172,6 +179,7 @@ __global__ void k_cell_fill(State S, Grid g, const int* need)
 // ascending atom order inside each cell (the fill order is racy)
 __global__ void k_cell_sort(Grid g, const int* need)
 {
+  pdl_enter();
   if (!*need) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.ncell) return;
@@ -181,6 +189,7 @@ __global__ void k_cell_sort(Grid g, const int* need)
 
 __global__ void k_nl_build(State S, Grid g, NList L, const int* need, unsigned int* status)
 {
+  pdl_enter();
   if (!*need) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < S.n) nl_build_atom(S, g, L, i, status);
@@ -188,6 +197,7 @@ __global__ void k_nl_build(State S, Grid g, NList L, const int* need, unsigned i
 
 __global__ void k_bonds(State S, NList L, ReboParams P, BondBuild B, BondTasks K, unsigned int* status)
 {
+  pdl_enter();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a == 0 && K.ctr) K.ctr[0] = K.ctr[1] = K.ctr[2] = 0;
   if (a < S.n) bonds_atom(S, L, P, B, a, status);
@@ -215,6 +225,7 @@ __device__ unsigned long long warp_alloc(unsigned long long v, unsigned long lon
 // written to each slot's record do not.
 __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const bool ok = a < B.n;
   int nb = 0, ncc = 0;
@@ -261,6 +272,7 @@ __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
 __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, TorsParams TP, int do_rebo,
                        int do_tors, ForceOut O, unsigned int* status)
 {
+  pdl_enter();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   Rebo R{*P, *T, B, status};
@@ -273,6 +285,7 @@ template <class Real, class TB>
 __global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const TB* T, BondList B, TorsParams TP,
                                                    int do_rebo, int do_tors, BondTasks K, unsigned int* status)
 {
+  pdl_enter();
   const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
   ReboT<Real, TB> R{*P, *T, B, status};
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
@@ -290,6 +303,7 @@ __global__ void __launch_bounds__(128) k_rebo_pair_task(const ReboParams* P, con
                                                         int do_rebo, int do_tors, BondTasks K,
                                                         unsigned int* status)
 {
+  pdl_enter();
   const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
   ReboT<Real, TB> R{*P, *T, B, status};
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
@@ -313,6 +327,7 @@ __global__ void __launch_bounds__(128) k_rebo_pair_task(const ReboParams* P, con
 template <int G>
 __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTasks Tk, int with_lj, ForceOut O)
 {
+  pdl_enter();
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = gid / G, l = gid - (gid / G) * G;
   if (a >= B.n) return;
@@ -370,6 +385,7 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
 __global__ void k_brenner(const BrennerParams* P, const BrennerTables* T, BondList B, ForceOut O,
                           unsigned int* status)
 {
+  pdl_enter();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= B.n) return;
   Brenner R{*P, *T, B, status};
@@ -380,6 +396,7 @@ constexpr int kCijLocal = 128;  // per-thread connectivity table capacity
 
 __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
 {
+  pdl_enter();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
@@ -392,6 +409,7 @@ __global__ void k_cij(BondList B, CijTable T, unsigned int* status)
 // hide the position gathers.
 __global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NList L, int* inr, int* inr_cnt)
 {
+  pdl_enter();
   const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (a >= S.n) return;  // whole warps
@@ -432,6 +450,7 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
                                                        const int* inr_cnt, const int* nbonds, ForceOut O,
                                                        SpecialTasks Tk, unsigned int* status)
 {
+  pdl_enter();
   if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
   // kLjGroup lanes per atom: an atom has ~30 in-range partners, so a group
   // of 16 keeps more lanes busy than a whole warp would
@@ -491,6 +510,7 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
 // Single-block exclusive scan: off[i] = sum cnt[0..i), off[n] = total.
 __global__ void k_exscan(const int* cnt, int n, int* off)
 {
+  pdl_enter();
   __shared__ int part[1024];
   int t = threadIdx.x, nt = blockDim.x;
   int chunk = (n + nt - 1) / nt;
@@ -523,6 +543,7 @@ constexpr int kReduceLanes = 8;
 
 __global__ void k_scan_tiles(ScanPair P)
 {
+  pdl_enter();
   __shared__ int wsum[32];
   const int y = blockIdx.y;
   const int i = blockIdx.x * kScanTile + threadIdx.x;
@@ -551,6 +572,7 @@ __global__ void k_scan_tiles(ScanPair P)
 
 __global__ void k_scan_top(ScanPair P)
 {
+  pdl_enter();
   const int y = blockIdx.y;
   if (threadIdx.x != 0) return;
   int acc = 0;
@@ -564,6 +586,7 @@ __global__ void k_scan_top(ScanPair P)
 
 __global__ void k_scan_add(ScanPair P)
 {
+  pdl_enter();
   const int y = blockIdx.y;
   const int i = blockIdx.x * kScanTile + threadIdx.x;
   if (i < P.n && blockIdx.x > 0) P.out[y][i] += P.tile[y][blockIdx.x];
@@ -574,6 +597,7 @@ __global__ void k_scan_add(ScanPair P)
 // the partner's task of the same pair (a linear search in its special list).
 __global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, int pairs, unsigned int* status)
 {
+  pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const bool ok = a < n;
   int c = 0, o = 0, nhi = 0;
@@ -619,6 +643,7 @@ template <class Real, class TB>
 __global__ void k_lj_special(const ReboParams* P, const TB* Tb, LJParams LP, BondList B, CijTable T, State S,
                              SpecialTasks Tk, unsigned int* status)
 {
+  pdl_enter();
   const int total = min(Tk.off[S.n], Tk.task_cap);
   ReboT<Real, TB> R{*P, *Tb, B, status};
   LJT<Real, TB> X{LP, R, T};
@@ -631,6 +656,7 @@ template <class Real, class TB>
 __global__ void k_lj_special_pair(const ReboParams* P, const TB* Tb, LJParams LP, BondList B, CijTable T, State S,
                                   SpecialTasks Tk, unsigned int* status)
 {
+  pdl_enter();
   const long total = (long)*Tk.wcnt;
   ReboT<Real, TB> R{*P, *Tb, B, status};
   LJT<Real, TB> X{LP, R, T};
@@ -726,6 +752,7 @@ __device__ V3 gather_lanes(const BondList& B, const ForceOut& O, const SpecialTa
 
 __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, const double4* gm)
 {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = t / kGatherLanes, l = t % kGatherLanes;
   if (__all_sync(0xffffffffu, a >= B.n)) return;  // whole warps
@@ -741,6 +768,7 @@ __global__ void k_gather(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, d
 __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk, double4* grad, State S, StepDev P,
                             double* ekin, const double4* gm, unsigned int* status)
 {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = t / kGatherLanes, l = t % kGatherLanes;
   if (__all_sync(0xffffffffu, a >= B.n)) return;  // whole warps
@@ -763,6 +791,7 @@ __global__ void k_gather_vv(BondList B, ForceOut O, int with_lj, SpecialTasks Tk
 // [system][block][2], summed in a fixed order by k_bath_final.
 __global__ void k_bath_partial(State S, StepDev P, const int64_t* first, double* part)
 {
+  pdl_enter();
   __shared__ double se[kThreads], sn[kThreads];
   const int sy = blockIdx.y;
   const long b = first ? first[sy] : 0, e = first ? first[sy + 1] : S.n;
@@ -791,6 +820,7 @@ __global__ void k_bath_partial(State S, StepDev P, const int64_t* first, double*
 }
 __global__ void k_bath_final(const double* part, int nblk_sys, int nsys, double* T)
 {
+  pdl_enter();
   const int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= nsys) return;
   double ek = 0.0, cnt = 0.0;
@@ -807,6 +837,7 @@ __global__ void k_bath_final(const double* part, int nblk_sys, int nsys, double*
 __global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, double* dt_prev, double* time,
                             double timeaccel, int* stop, double time_final)
 {
+  pdl_enter();
   const int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= nsys) return;
   if (stop && stop[sy]) {  // finished: time and dt stay as the last step left them
@@ -829,6 +860,7 @@ __global__ void k_dt_update(int nsys, unsigned long long* vmax, double* dt, doub
 // Systems already at or past simTimeFinal take no step.
 __global__ void k_stop_init(int nsys, const double* time, int* stop, double time_final)
 {
+  pdl_enter();
   const int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy < nsys) stop[sy] = !(time[sy] < time_final);
 }
@@ -837,6 +869,7 @@ __global__ void k_stop_init(int nsys, const double* time, int* stop, double time
 // units; the species in pos.w is kept.
 __global__ void k_state_unpack(State S, const double* io, double ul, double uv)
 {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   const double* p = io + 3 * (long)i;
@@ -846,6 +879,7 @@ __global__ void k_state_unpack(State S, const double* io, double ul, double uv)
 }
 __global__ void k_state_pack(State S, double* io, double ul, double uv)
 {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   const double4 p = S.pos[i], v = S.vel[i];
@@ -859,6 +893,7 @@ __global__ void k_state_pack(State S, double* io, double ul, double uv)
 // (and Atom::an_no_tb, Check::energyTransferredFromBath = 0, SimLoop.cxx:1137)
 __global__ void k_init_acc(State S, const double4* grad, double4* acc_ntb, double* eb)
 {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   if (eb) eb[i] = 0.0;
@@ -871,6 +906,7 @@ __global__ void k_init_acc(State S, const double4* grad, double4* acc_ntb, doubl
 
 __global__ void k_ekin(State S, double* ekin)
 {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   double4 v = S.vel[i];
@@ -885,6 +921,7 @@ struct RedArgs {
 };
 __global__ void k_reduce_partial(RedArgs R, double* part)
 {
+  pdl_enter();
   __shared__ double sh[kThreads];
   int which = blockIdx.y;
   const double* x = R.a[which];
@@ -902,6 +939,7 @@ __global__ void k_reduce_partial(RedArgs R, double* part)
 __global__ void k_reduce_final(const double* part, int nparts, RedArgs R, double* out, int slot_stride, int slot,
                                unsigned int* status)
 {
+  pdl_enter();
   int w = threadIdx.x;
   if (w >= R.nout) return;
   double s = 0.0;
@@ -921,6 +959,7 @@ __global__ void k_reduce_final(const double* part, int nparts, RedArgs R, double
 __global__ void k_sys_energy(const int64_t* first, int64_t n, const double* er, const double* el, const double* et,
                              const double* ek, const double* em, double* out, unsigned int* status)
 {
+  pdl_enter();
   __shared__ double sh[4][kThreads];
   const int sy = blockIdx.x;
   // a single-system context has no offsets array: its one system is [0, n)
@@ -949,6 +988,7 @@ __global__ void k_sys_energy(const int64_t* first, int64_t n, const double* er, 
 
 __global__ void k_finite(const double4* g, int n, unsigned int* status)
 {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double4 v = g[i];
@@ -1086,6 +1126,7 @@ struct mdg_ctx {
   cudaGraphExec_t step_graph = nullptr;
   double graph_dt = 0.0;
   int graph_cfg = -1;           // step_cfg the graph was captured with
+  bool pdl = true;              // programmatic dependent launches (mdg_set_dependent_launch)
   int step_cfg = 0;             // bumped when the thermal bath or the dt mode changes
 
   // thermal bath (SimLoop::thermalBath*, SimLoop.hpp:96-191) and adaptive dt
@@ -1455,20 +1496,38 @@ int setup_grid_batch(mdg_ctx* c, int l, const std::vector<double>& hpos)
 // profiling is on, brackets it with CUDA events on the launch stream.
 void prof_begin(mdg_ctx* c, const char* name);
 void prof_end(mdg_ctx* c);
-#define LAUNCH(c, NAME, KERNEL, GRID, BLOCK, ...)                     \
-  do {                                                                \
-    prof_begin(c, NAME);                                              \
-    KERNEL<<<(GRID), (BLOCK), 0, (c)->stream>>>(__VA_ARGS__);         \
-    prof_end(c);                                                      \
-    (c)->launches++;                                                  \
+// With pdl set, the launch carries the programmatic stream-serialisation
+// attribute: the kernel's blocks may be scheduled while the grid before it
+// drains, and wait in pdl_enter() (their first statement) for its completion.
+template <typename... P, typename... A>
+inline void launch_kernel(bool pdl, cudaStream_t st, void (*k)(P...), dim3 grid, dim3 block, A&&... args)
+{
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at.val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = &at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+#define LAUNCH(c, NAME, KERNEL, GRID, BLOCK, ...)                           \
+  do {                                                                      \
+    prof_begin(c, NAME);                                                    \
+    launch_kernel((c)->pdl, (c)->stream, KERNEL, GRID, BLOCK, __VA_ARGS__); \
+    prof_end(c);                                                            \
+    (c)->launches++;                                                        \
   } while (0)
 // The same on another stream (never while profiling: the events are on c->stream).
-#define LAUNCH_ON(c, STREAM, NAME, KERNEL, GRID, BLOCK, ...)          \
-  do {                                                                \
-    prof_begin(c, NAME);                                              \
-    KERNEL<<<(GRID), (BLOCK), 0, (STREAM)>>>(__VA_ARGS__);            \
-    prof_end(c);                                                      \
-    (c)->launches++;                                                  \
+#define LAUNCH_ON(c, STREAM, NAME, KERNEL, GRID, BLOCK, ...)               \
+  do {                                                                      \
+    prof_begin(c, NAME);                                                    \
+    launch_kernel((c)->pdl, (STREAM), KERNEL, GRID, BLOCK, __VA_ARGS__);    \
+    prof_end(c);                                                            \
+    (c)->launches++;                                                        \
   } while (0)
 
 // The displacement partials of both lists (after the step's position update
@@ -2670,6 +2729,14 @@ int mdg_tuned_launch(mdg_ctx* c, int* overlap, int* rebo_blocks)
   if (!c) return fail(MDG_ERR_ARG, "null context");
   if (overlap) *overlap = c->overlap ? 1 : 0;
   if (rebo_blocks) *rebo_blocks = c->rebo_grid > 0 ? c->rebo_grid : c->rebo_task_blocks;
+  return MDG_OK;
+}
+
+int mdg_set_dependent_launch(mdg_ctx* c, int on)
+{
+  if (!c) return fail(MDG_ERR_ARG, "null context");
+  c->pdl = on != 0;
+  c->step_cfg++;  // recapture the step graph with the new launch attribute
   return MDG_OK;
 }
 

@@ -46,6 +46,21 @@ enum StatusBits : unsigned int {
   ST_SNAP_OVERFLOW = 1u << 10,  // snapshot list capacity exceeded
 };
 
+#if defined(__CUDACC__)
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialisation attribute may be scheduled while the grid before it on
+// the stream is still draining; the first statement of every such kernel is
+// this call, which waits until that grid has completed and its memory writes
+// are visible (griddepcontrol.wait, a no-op for a kernel launched without the
+// attribute), and then lets the next grid be scheduled in turn.  Completion
+// is thereby transitive along the stream, as with ordinary launches.
+__device__ __forceinline__ void pdl_enter()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+
 // FP32 scalar of the mixed-precision path: float arithmetic; double operands
 // (parameters, literals, loads from the FP64 bond list) convert to float
 // implicitly, conversion back to double is explicit (dbl()).

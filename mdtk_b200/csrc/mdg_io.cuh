@@ -187,6 +187,7 @@ struct Rec {
 __global__ void k_snap_pack(State S, const double4* grad, const double* er, const double* el, const double* et,
                             const double* em, const double* ekp, const double* eb, char* out, SnapLayout L)
 {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.n) return;
   double* r = (double*)(out + L.r) + 3 * (size_t)i;
@@ -211,6 +212,7 @@ __global__ void k_snap_pack(State S, const double4* grad, const double* er, cons
 __global__ void k_snap_header(int nsys, const double* time, const double* dt, const double* dt_prev, const double* e0,
                               char* out, SnapLayout L)
 {
+  pdl_enter();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   double* h = (double*)(out + L.hdr) + kHdr * (size_t)s;
@@ -1259,6 +1261,7 @@ MDG_HD int snap_slot(const SnapDev& D, int s, const double* time, const double* 
 
 __global__ void k_snap_atoms(State S, SnapDev D, const double* time, const double* dt_prev, const int* stop)
 {
+  pdl_enter();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= D.nsel) return;
   const int s = D.sel_sys[j];
@@ -1278,6 +1281,7 @@ __global__ void k_snap_atoms(State S, SnapDev D, const double* time, const doubl
 __global__ void k_snap_commit(SnapDev D, const double* time, const double* dt_prev, const int* stop,
                               unsigned int* status)
 {
+  pdl_enter();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= D.nsys) return;
   const int k = snap_slot(D, s, time, dt_prev, stop);

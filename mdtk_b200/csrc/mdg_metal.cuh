@@ -314,6 +314,7 @@ __device__ void for_partners(const State& S, const NList& L, int i, const V3& xi
 __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, double* fp, double* em,
                           unsigned int* status)
 {
+  pdl_enter();
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= S.n) return;  // uniform per warp
   const double4 pi = S.pos[i];
@@ -357,6 +358,7 @@ __global__ void k_eam_rho(State S, NList L, const MetalParams* __restrict__ Mp, 
 __global__ void k_metal_pairs(State S, NList L, const MetalParams* __restrict__ Mp, const double* fp, double* em,
                               double4* gm)
 {
+  pdl_enter();
   __shared__ int qbuf[kThreads];
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= S.n) return;  // uniform per warp
