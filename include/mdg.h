@@ -88,7 +88,9 @@ typedef struct mdg_params {
                          records (half the work); 0 = timed once per system on the first mdg_run
                          (the autotuner) and the faster kept.  Both route the same terms into the
                          same records; results agree to rounding (the two kernels may contract
-                         multiply-adds differently). */
+                         multiply-adds differently).  With the LJ term the launch configuration
+                         (stream overlap, REBO grid) is timed on the first mdg_run in every mode;
+                         it never changes results. */
 } mdg_params;
 
 /* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */
@@ -402,7 +404,7 @@ int mdg_snapshots_write(mdg_ctx* ctx, int sys, const char* path, int zip, int te
 /* SnapshotList::loadstate: earlier snapshots of system sys (same selection). */
 int mdg_snapshots_load(mdg_ctx* ctx, int sys, const char* path);
 
-/* The launch configuration the autotuner chose (task_mode 0): overlap = 1
+/* The launch configuration the autotuner chose (with the LJ term): overlap = 1
  * when the REBO tasks run on a second stream concurrently with the LJ
  * kernels, rebo_blocks = the REBO task kernel's grid.  No reference
  * counterpart. */

@@ -507,44 +507,28 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
   }
 }
 
-// Single-block exclusive scan: off[i] = sum cnt[0..i), off[n] = total.
-__global__ void k_exscan(const int* cnt, int n, int* off)
-{
-  pdl_enter();
-  __shared__ int part[1024];
-  int t = threadIdx.x, nt = blockDim.x;
-  int chunk = (n + nt - 1) / nt;
-  int b = t * chunk, e = min(n, b + chunk);
-  int s = 0;
-  for (int c = b; c < e; c++) s += cnt[c];
-  part[t] = s;
-  __syncthreads();
-  if (t == 0) {
-    int acc = 0;
-    for (int q = 0; q < nt; q++) { int v = part[q]; part[q] = acc; acc += v; }
-    off[n] = acc;
-  }
-  __syncthreads();
-  int acc = part[t];
-  for (int c = b; c < e; c++) { off[c] = acc; acc += cnt[c]; }
-}
-
-// Tiled exclusive scan of up to two int arrays at once (blockIdx.y picks the
-// array): per-tile block scan, a scan of the tile sums, then the tile offsets
-// added back.  off has n + 1 entries; off[n] = total.
+// Tiled exclusive scan of two int arrays at once (blockIdx.y picks the
+// array) in one launch: each tile block scans its tile into part (offsets
+// within the tile) and stores the tile's sum; the last block to finish (a
+// counter, no waiting) turns the tile sums into tile offsets and writes the
+// totals out[y][n].  The element offset is part[y][i] + tile[y][i / kScanTile],
+// added by the compaction kernel that follows.
 struct ScanPair {
   const int* in[2];
-  int* out[2];
-  int* tile[2];   // [ntiles + 1] tile sums, then tile offsets
+  int* out[2];    // [n + 1]: only out[y][n] (the total) is written here
+  int* part[2];   // [n] offsets within the tile
+  int* tile[2];   // [ntiles] tile sums, then tile offsets
+  unsigned int* done;  // tile blocks finished (back to 0 by the last one)
   int n, ntiles;
 };
 constexpr int kScanTile = 1024;
 constexpr int kReduceLanes = 8;
 
-__global__ void k_scan_tiles(ScanPair P)
+__global__ void __launch_bounds__(kScanTile) k_scan_tiles(ScanPair P)
 {
   pdl_enter();
   __shared__ int wsum[32];
+  __shared__ int last;
   const int y = blockIdx.y;
   const int i = blockIdx.x * kScanTile + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -566,36 +550,37 @@ __global__ void k_scan_tiles(ScanPair P)
   }
   __syncthreads();
   const int incl = x + (wid > 0 ? wsum[wid - 1] : 0);
-  if (i < P.n) P.out[y][i] = incl - v;
+  if (i < P.n) P.part[y][i] = incl - v;
   if (threadIdx.x == kScanTile - 1) P.tile[y][blockIdx.x] = incl;
-}
-
-__global__ void k_scan_top(ScanPair P)
-{
-  pdl_enter();
-  const int y = blockIdx.y;
-  if (threadIdx.x != 0) return;
-  int acc = 0;
-  for (int t = 0; t < P.ntiles; t++) {
-    int v = P.tile[y][t];
-    P.tile[y][t] = acc;
-    acc += v;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(P.done, 1u) == gridDim.x * gridDim.y - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (wid < 2) {  // warp yy scans the tile sums of array yy, 32 at a time
+    const int yy = wid;
+    int carry = 0;
+    for (int t0 = 0; t0 < P.ntiles; t0 += 32) {
+      const int t = t0 + lane;
+      const int u = t < P.ntiles ? __ldcg(P.tile[yy] + t) : 0;
+      int z = u;
+      for (int o = 1; o < 32; o <<= 1) {
+        int q = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += q;
+      }
+      if (t < P.ntiles) P.tile[yy][t] = carry + z - u;
+      carry += __shfl_sync(0xffffffffu, z, 31);
+    }
+    if (lane == 0) P.out[yy][P.n] = carry;
   }
-  P.out[y][P.n] = acc;
-}
-
-__global__ void k_scan_add(ScanPair P)
-{
-  pdl_enter();
-  const int y = blockIdx.y;
-  const int i = blockIdx.x * kScanTile + threadIdx.x;
-  if (i < P.n && blockIdx.x > 0) P.out[y][i] += P.tile[y][blockIdx.x];
+  if (threadIdx.x == 0) *P.done = 0u;
 }
 
 // Flat task list (atom, partner) and record offsets; with `pairs`, also the
 // work list of tasks owned by the lower index of their pair and, for each,
 // the partner's task of the same pair (a linear search in its special list).
-__global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, int pairs, unsigned int* status)
+__global__ void k_spc_compact(SpecialTasks Tk, ScanPair P, const int* nbonds, int n, int pairs, unsigned int* status)
 {
   pdl_enter();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -603,11 +588,14 @@ __global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, int pai
   int c = 0, o = 0, nhi = 0;
   if (ok) {
     c = Tk.cnt[a];
-    o = Tk.off[a];
+    o = P.part[0][a] + P.tile[0][a / kScanTile];
+    const int ra = P.part[1][a] + P.tile[1][a / kScanTile];
+    Tk.off[a] = o;
+    Tk.roff[a] = ra;
     const int rs = rec_size(nbonds[a]);
     for (int q = 0; q < c; q++) {
       const int t = o + q;
-      const long ro = (long)Tk.roff[a] + (long)q * rs;
+      const long ro = (long)ra + (long)q * rs;
       const int b = Tk.part[(long)a * Tk.cap + q];
       if (t < Tk.task_cap) {
         Tk.flat[t] = make_int2(a, b);
@@ -629,7 +617,7 @@ __global__ void k_spc_compact(SpecialTasks Tk, const int* nbonds, int n, int pai
     const int b = Tk.part[(long)a * Tk.cap + q];
     if (b < a) continue;
     int t2 = -1;
-    const int cb = Tk.cnt[b], ob = Tk.off[b];
+    const int cb = Tk.cnt[b], ob = P.part[0][b] + P.tile[0][b / kScanTile];
     for (int u = 0; u < cb; u++)
       if (Tk.part[(long)b * Tk.cap + u] == a) { t2 = ob + u; break; }
     if (t2 >= Tk.task_cap) t2 = -1;
@@ -1120,7 +1108,7 @@ struct mdg_ctx {
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
-  int* scan_tiles = nullptr;  // 2 * (n / 1024 + 2)
+  int* scan_tiles = nullptr;  // 2 (n / 1024 + 2) tile sums, a counter, 2 n offsets within tiles
 
   // one MD step captured as a CUDA graph (replayed when no per-step energies are wanted)
   cudaGraphExec_t step_graph = nullptr;
@@ -1677,15 +1665,17 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     sp.in[1] = c->spc.rsz;
     sp.out[0] = c->spc.off;
     sp.out[1] = c->spc.roff;
+    const int tstride = c->n / kScanTile + 2;
     sp.tile[0] = c->scan_tiles;
-    sp.tile[1] = c->scan_tiles + (c->n / kScanTile + 2);
+    sp.tile[1] = c->scan_tiles + tstride;
+    sp.done = (unsigned int*)(c->scan_tiles + 2 * tstride);
+    sp.part[0] = c->scan_tiles + 2 * tstride + 1;
+    sp.part[1] = sp.part[0] + c->n;
     sp.n = c->n;
     sp.ntiles = (c->n + kScanTile - 1) / kScanTile;
     LAUNCH(c, "lj_scan_tiles", k_scan_tiles, dim3(sp.ntiles, 2), kScanTile, sp);
-    LAUNCH(c, "lj_scan_top", k_scan_top, dim3(1, 2), 32, sp);
-    LAUNCH(c, "lj_scan_add", k_scan_add, dim3(sp.ntiles, 2), kScanTile, sp);
     const int pairs = (c->bt.ctr && c->bt.pairs) ? 1 : 0;
-    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, c->bb.nb, c->n, pairs, c->d_status);
+    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, sp, c->bb.nb, c->n, pairs, c->d_status);
     // b*_ij of close non-bonded pairs stays FP64 in the mixed mode too: the
     // S(t_b) window (0.04 wide for C-C) multiplies an error of b* by up to
     // 1/0.04^2 in the pair force, beyond what float b* can carry.
@@ -2159,8 +2149,11 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
     CK(cudaMemset(X.cnt, 0, n * sizeof(int)));
     CK(cudaMemset(X.off, 0, (n + 1) * sizeof(int)));
-    c->scan_tiles = dalloc<int>(2 * (n / kScanTile + 2));
+    // tile sums of both arrays, the finished-tiles counter, offsets within the tiles
+    const size_t scan_ints = 2 * (size_t)(n / kScanTile + 2) + 1 + 2 * (size_t)n;
+    c->scan_tiles = dalloc<int>(scan_ints);
     if (!c->scan_tiles) return fail(MDG_ERR_CUDA, "cudaMalloc (scan)");
+    CK(cudaMemset(c->scan_tiles, 0, scan_ints * sizeof(int)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2348,8 +2341,12 @@ static int autotune(mdg_ctx* c)
 {
   if (c->tuned || !c->bt.ctr) return MDG_OK;
   c->tuned = true;
-  if (c->prm.task_mode != 0) return MDG_OK;
   const bool lj = c->prm.potentials & MDG_POT_AIREBO_LJ;
+  // a fixed task mode (task_mode 1 or 2) keeps its split; the launch
+  // configuration, which never changes results, is still chosen
+  if (c->prm.task_mode != 0 && !lj) return MDG_OK;
+  const int mode0 = c->prm.task_mode ? c->prm.task_mode - 1 : 0;
+  const int mode1 = c->prm.task_mode ? c->prm.task_mode : 2;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2363,9 +2360,9 @@ static int autotune(mdg_ctx* c)
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best_all = 1e30f;
-  int best_mode = 0;
+  int best_mode = mode0;
   Cfg best_cfg = cfgs[0];
-  for (int mode = 0; mode < 2; mode++) {
+  for (int mode = mode0; mode < mode1; mode++) {
     c->bt.pairs = mode;
     c->tune_ms[mode] = 1e30f;
     for (const Cfg& g : cfgs) {

@@ -115,6 +115,26 @@ def test_record_capacity_overflow_is_reported():
     assert e.value.code == -8
 
 
+def test_dependent_launch_matches_ordinary_launch():
+    """Programmatic dependent launch changes when blocks are scheduled, never
+    what they compute: the same trajectory bit for bit, list rebuilds and the
+    three streams included, through the graph and through host steps."""
+    s = B.ethane_liquid(400, seed=40, temp_k=1500.0)
+    out = []
+    for pdl in (True, False):
+        c = _gpu(s, task_mode=2)  # the launch configuration is still tuned (overlap)
+        c.set_dependent_launch(pdl)
+        _, et = c.run(120, 0.5)
+        c.run(60, 0.5, energies=False)
+        c.sync()
+        p, v, img = c.get_state()
+        out.append((et, p, v, img, c.compute()))
+        assert c.task_mode()[0] == 2
+    (ea, pa, va, ia, (ga, ta, fa)), (eb, pb, vb, ib, (gb, tb, fb)) = out
+    assert np.array_equal(ea, eb) and np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(ia, ib) and ga == gb and np.array_equal(ta, tb) and np.array_equal(fa, fb)
+
+
 def test_graph_replay_matches_eager_steps():
     s = B.ethane_liquid(30, seed=39, temp_k=300.0)
     a = _gpu(s)
