@@ -62,7 +62,11 @@ __device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, do
 // Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
 // of the step) and, per block, the two largest displacements since each
 // list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
-__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, int mask, double* part)
+// The last block to finish (a counter, no waiting) reduces the partials of
+// each list to its rebuild flag: need[l] = force[l] || top1 + top2 > trigger
+// (NeighbourList::MovedTooMuch, NeighbourList.cxx:109-133), then clears force[l].
+__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, int mask, double* part,
+                             int* need, int* force, unsigned int* done)
 {
   pdl_enter();
   __shared__ double s1[3][kThreads / 32], s2[3][kThreads / 32];
@@ -98,40 +102,32 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
     part[2 * gridDim.x * l + 2 * blockIdx.x] = t1;
     part[2 * gridDim.x * l + 2 * blockIdx.x + 1] = t2;
   }
-}
-
-// need = force || top1 + top2 > trigger (NeighbourList::MovedTooMuch); one
-// warp: each lane keeps the two largest of a strided share of the partials,
-// then the lanes' pairs are merged by shuffles (the two largest of a set do
-// not depend on the order they are met in).
-__global__ void k_disp_final(const double* part, int nparts, double trigger, int* need, int* force)
-{
-  pdl_enter();
-  const int lane = threadIdx.x;
-  if (lane >= 32) return;
-  double t1 = 0.0, t2 = 0.0;
-  for (int q = lane; q < 2 * nparts; q += 32) {
-    const double x = part[q];
-    if (x >= t1) { t2 = t1; t1 = x; }
-    else if (x >= t2) t2 = x;
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // warp l: each lane keeps the two largest of a strided share of the
+  // partials, then the lanes' pairs are merged by shuffles (the two largest
+  // of a set do not depend on the order they are met in)
+  if (wid < 3 && ((mask >> wid) & 1)) {
+    const int l = wid;
+    const double* pl = part + 2 * gridDim.x * l;
+    double t1 = 0.0, t2 = 0.0;
+    for (int q = lane; q < (int)gridDim.x; q += 32) top2_merge(t1, t2, __ldcg(pl + 2 * q), __ldcg(pl + 2 * q + 1));
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u1 = __shfl_down_sync(0xffffffffu, t1, o), u2 = __shfl_down_sync(0xffffffffu, t2, o);
+      top2_merge(t1, t2, u1, u2);
+    }
+    if (lane == 0) {
+      const double trig = l == 0 ? L0.trigger : (l == 1 ? L1.trigger : L2.trigger);
+      need[l] = force[l] || (t1 + t2 > trig);
+      force[l] = 0;
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const double u1 = __shfl_down_sync(0xffffffffu, t1, o), u2 = __shfl_down_sync(0xffffffffu, t2, o);
-    top2_merge(t1, t2, u1, u2);
-  }
-  if (lane == 0) {
-    const int nd = (*force) || (t1 + t2 > trigger);
-    *need = nd;
-    *force = 0;
-  }
-}
-
-__global__ void k_cell_clear(Grid g, const int* need)
-{
-  pdl_enter();
-  if (!*need) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < g.ncell) { g.ccount[c] = 0; g.ccursor[c] = 0; }
+  if (threadIdx.x == 0) *done = 0u;
 }
 
 __global__ void k_cell_count(State S, Grid g, const int* need)
@@ -176,7 +172,8 @@ __global__ void k_cell_fill(State S, Grid g, const int* need)
   g.catoms[g.cstart[c] + slot] = i;
 }
 
-// ascending atom order inside each cell (the fill order is racy)
+// ascending atom order inside each cell (the fill order is racy); the cell's
+// count and fill cursor, used up by now, go back to zero for the next build
 __global__ void k_cell_sort(Grid g, const int* need)
 {
   pdl_enter();
@@ -185,6 +182,8 @@ __global__ void k_cell_sort(Grid g, const int* need)
   if (c >= g.ncell) return;
   int b = g.cstart[c], e = g.cstart[c + 1];
   isort(g.catoms + b, e - b);
+  g.ccount[c] = 0;
+  g.ccursor[c] = 0;
 }
 
 __global__ void k_nl_build(State S, Grid g, NList L, const int* need, unsigned int* status)
@@ -1067,6 +1066,7 @@ struct mdg_ctx {
   Grid grid[3];
   int* d_need = nullptr;   // [3]
   int* d_force = nullptr;  // [3]
+  unsigned int* d_disp_done = nullptr;  // blocks of step_start finished (back to 0 by the last)
   double* d_part = nullptr;
   double rcut[3] = {0, 0, 0};
   bool has_list[3] = {false, false, false};
@@ -1418,6 +1418,9 @@ int setup_grid(mdg_ctx* c, int l, const std::vector<double>& hpos)
   g.ccursor = dalloc<int>(nc);
   g.catoms = dalloc<int>(c->n);
   if (!g.ccount || !g.cstart || !g.ccursor || !g.catoms) return fail(MDG_ERR_CUDA, "cudaMalloc (cell grid)");
+  // counts and cursors start at zero; each build's sort returns them there
+  CK(cudaMemset(g.ccount, 0, (size_t)nc * sizeof(int)));
+  CK(cudaMemset(g.ccursor, 0, (size_t)nc * sizeof(int)));
   return MDG_OK;
 }
 
@@ -1471,6 +1474,8 @@ int setup_grid_batch(mdg_ctx* c, int l, const std::vector<double>& hpos)
   c->d_scs[l] = dalloc<double4>(c->nsys);
   if (!g.ccount || !g.cstart || !g.ccursor || !g.catoms || !c->d_snc[l] || !c->d_slo[l] || !c->d_scs[l])
     return fail(MDG_ERR_CUDA, "cudaMalloc (cell grids)");
+  CK(cudaMemset(g.ccount, 0, (size_t)total * sizeof(int)));
+  CK(cudaMemset(g.ccursor, 0, (size_t)total * sizeof(int)));
   CK(cudaMemcpy(c->d_snc[l], snc.data(), c->nsys * sizeof(int4), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_slo[l], slo.data(), c->nsys * sizeof(double4), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_scs[l], scs.data(), c->nsys * sizeof(double4), cudaMemcpyHostToDevice));
@@ -1536,14 +1541,15 @@ int step_start(mdg_ctx* c, const StepDev* step)
   }
   StepDev none;
   std::memset(&none, 0, sizeof(none));
-  LAUNCH(c, step ? "verlet_pos_disp" : "nl_disp_partial", k_step_start, kDispParts, kThreads, S,
-         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], c->nl[2], mask, c->d_part);
+  LAUNCH(c, step ? "verlet_pos_disp" : "nl_disp", k_step_start, kDispParts, kThreads, S,
+         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], c->nl[2], mask, c->d_part, c->d_need, c->d_force,
+         c->d_disp_done);
   return MDG_OK;
 }
 
-// Displacement decision and (when it fires) cell-list rebuild of list l on
-// stream st, from the partials of step_start; each list has its own
-// partials, flags and grid, so the two lists can run on different streams.
+// Cell-list rebuild of list l on stream st when step_start's flag for it is
+// set (each kernel returns at once otherwise); each list has its own flag
+// and grid, so the lists can be rebuilt on different streams.
 int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
 {
   if (!c->has_list[l]) return MDG_OK;
@@ -1551,10 +1557,7 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
   NList& L = c->nl[l];
   Grid& g = c->grid[l];
   int* need = c->d_need + l;
-  double* part = c->d_part + 2 * kDispParts * l;
-  LAUNCH_ON(c, st, "nl_disp_final", k_disp_final, 1, 32, part, kDispParts, L.trigger, need, c->d_force + l);
   if (!g.brute) {
-    LAUNCH_ON(c, st, "nl_cell_clear", k_cell_clear, nblk(g.ncell), kThreads, g, need);
     LAUNCH_ON(c, st, "nl_cell_count", k_cell_count, nblk(c->n), kThreads, S, g, need);
     LAUNCH_ON(c, st, "nl_cell_scan", k_cell_scan, 1, 1024, g, need);
     LAUNCH_ON(c, st, "nl_cell_fill", k_cell_fill, nblk(c->n), kThreads, S, g, need);
@@ -1857,11 +1860,16 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   c->d_status = dalloc<unsigned int>(1);
   c->d_need = dalloc<int>(3);
   c->d_force = dalloc<int>(3);
+  c->d_disp_done = dalloc<unsigned int>(1);
   c->d_energy = dalloc<double>(8);
-  if (!c->d_status || !c->d_need || !c->d_force || !c->d_energy) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "cudaMalloc"); }
+  if (!c->d_status || !c->d_need || !c->d_force || !c->d_disp_done || !c->d_energy) {
+    mdg_destroy(c);
+    return fail(MDG_ERR_CUDA, "cudaMalloc");
+  }
   cudaMemset(c->d_status, 0, sizeof(unsigned int));
   cudaMemset(c->d_need, 0, 3 * sizeof(int));
   cudaMemset(c->d_force, 0, 3 * sizeof(int));
+  cudaMemset(c->d_disp_done, 0, sizeof(unsigned int));
   if (cudaGetLastError() != cudaSuccess) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "setup copies failed"); }
   *out = c;
   return MDG_OK;
@@ -1874,7 +1882,7 @@ int mdg_destroy(mdg_ctx* c)
   io_free(c);
   free_system(c);
   void* ptrs[] = {c->d_tables, c->d_tables32, c->d_rp, c->d_btables, c->d_bp, c->d_status, c->d_need, c->d_force, c->d_energy,
-                  c->d_metal};
+                  c->d_metal, c->d_disp_done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
