@@ -141,6 +141,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--task-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="REBO work split of the headline context: 0 autotuned, 1 directed, 2 per bond")
     ap.add_argument("--precision-study", action="store_true",
                     help="instead of the throughput line: the FP32-mixed vs FP64 study on the 512,000-atom diamond")
     ap.add_argument("--study-steps", type=int, default=5000)
@@ -197,7 +199,7 @@ def main():
 
     s = build_system(seed=1 + rank)
     n = len(s["z"])
-    ctx = M.Context(potentials=M.POT_AIREBO, device=local)
+    ctx = M.Context(potentials=M.POT_AIREBO, device=local, task_mode=args.task_mode)
     ctx.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
     # one explicit stream for the library's kernels, the L2 flush and the events
     stream = torch.cuda.Stream()
