@@ -529,9 +529,14 @@ __global__ void __launch_bounds__(kScanTile) k_scan_tiles(ScanPair P)
   __shared__ int wsum[32];
   __shared__ int last;
   const int y = blockIdx.y;
+  // the array's pointers by selection (an index into the parameter arrays
+  // would copy them to local memory)
+  const int* in = y ? P.in[1] : P.in[0];
+  int* part = y ? P.part[1] : P.part[0];
+  int* tile = y ? P.tile[1] : P.tile[0];
   const int i = blockIdx.x * kScanTile + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int v = (i < P.n) ? P.in[y][i] : 0;
+  int v = (i < P.n) ? in[i] : 0;
   int x = v;
   for (int o = 1; o < 32; o <<= 1) {
     int t = __shfl_up_sync(0xffffffffu, x, o);
@@ -549,29 +554,29 @@ __global__ void __launch_bounds__(kScanTile) k_scan_tiles(ScanPair P)
   }
   __syncthreads();
   const int incl = x + (wid > 0 ? wsum[wid - 1] : 0);
-  if (i < P.n) P.part[y][i] = incl - v;
-  if (threadIdx.x == kScanTile - 1) P.tile[y][blockIdx.x] = incl;
+  if (i < P.n) part[i] = incl - v;
+  if (threadIdx.x == kScanTile - 1) tile[blockIdx.x] = incl;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(P.done, 1u) == gridDim.x * gridDim.y - 1;
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (wid < 2) {  // warp yy scans the tile sums of array yy, 32 at a time
-    const int yy = wid;
+  if (wid < 2) {  // warp 0 / 1 scans the tile sums of array 0 / 1, 32 at a time
+    int* ty = wid ? P.tile[1] : P.tile[0];
     int carry = 0;
     for (int t0 = 0; t0 < P.ntiles; t0 += 32) {
       const int t = t0 + lane;
-      const int u = t < P.ntiles ? __ldcg(P.tile[yy] + t) : 0;
+      const int u = t < P.ntiles ? __ldcg(ty + t) : 0;
       int z = u;
       for (int o = 1; o < 32; o <<= 1) {
         int q = __shfl_up_sync(0xffffffffu, z, o);
         if (lane >= o) z += q;
       }
-      if (t < P.ntiles) P.tile[yy][t] = carry + z - u;
+      if (t < P.ntiles) ty[t] = carry + z - u;
       carry += __shfl_sync(0xffffffffu, z, 31);
     }
-    if (lane == 0) P.out[yy][P.n] = carry;
+    if (lane == 0) (wid ? P.out[1] : P.out[0])[P.n] = carry;
   }
   if (threadIdx.x == 0) *P.done = 0u;
 }
