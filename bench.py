@@ -120,6 +120,20 @@ def cpu_baseline(procs: int, nsteps: int):
     return atoms / window, res
 
 
+def usable_cores() -> int:
+    """Host cores this process may run on: its CPU affinity, lowered to the
+    cgroup's CPU quota when one is set (a container may see every core of the
+    machine but be granted fewer)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(float(quota) / float(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
+
+
 def cpu_model() -> str:
     try:
         for line in open("/proc/cpuinfo"):
@@ -139,6 +153,8 @@ def main():
     ap.add_argument("--impl", default="mdg", choices=["mdg", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-procs", type=int, default=0,
+                    help="processes of the reference arm (default: every usable host core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--task-mode", type=int, default=0, choices=[0, 1, 2],
@@ -158,7 +174,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        procs = min(os.cpu_count() or 1, 16)
+        procs = args.cpu_procs if args.cpu_procs > 0 else usable_cores()
         value, res = cpu_baseline(procs, args.cpu_steps)
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-steps/s",

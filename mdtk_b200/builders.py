@@ -157,37 +157,22 @@ def ethane_liquid(n_mol: int, density_g_cm3: float = 0.55, temp_k: float = 300.0
     a = L / ncell
     cells = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell), indexing="ij"), -1).reshape(-1, 3)
     sites = ((cells[:, None, :] + basis[None]).reshape(-1, 3) + 0.25) * a
-    sites = sites[rng.permutation(len(sites))[:n_mol]]
+    order = sites[rng.permutation(len(sites))]
+    # the first n_mol sites of the permutation are used in turn; a site where no
+    # orientation fits (its neighbours jammed it) is given up for the next
+    # unused site, so every seed builds while the lattice has spare sites
+    spare = list(order[n_mol:][::-1])
     tmpl = _ethane_template()
     ng = max(1, int(L // min_dist))
     csz = L / ng
     grid: Dict[tuple, list] = {}
     placed = []
-    for center0 in sites:
-        for attempt in range(5000):
-            R = _random_rotations(rng, 1)[0]
-            center = center0 + rng.uniform(-jitter, jitter, size=3)
-            at = np.mod((tmpl @ R.T) + center, L)
-            keys = [tuple((p // csz).astype(int) % ng) for p in at]
-            ok = True
-            for p, ci in zip(at, keys):
-                near = []
-                for dx in (-1, 0, 1):
-                    for dy in (-1, 0, 1):
-                        for dz in (-1, 0, 1):
-                            lst = grid.get(((ci[0] + dx) % ng, (ci[1] + dy) % ng, (ci[2] + dz) % ng))
-                            if lst:
-                                near.extend(lst)
-                if near:
-                    d = p - np.array(near)
-                    d -= L * np.round(d / L)
-                    if np.min(np.einsum("ij,ij->i", d, d)) < min_dist * min_dist:
-                        ok = False
-                        break
-            if ok:
-                break
-        else:
-            raise RuntimeError("ethane_liquid: no clash-free orientation; lower the density or min_dist")
+    for center0 in order[:n_mol]:
+        at, keys = _place_ethane(rng, tmpl, center0, L, jitter, min_dist, grid, csz, ng)
+        while at is None:
+            if not spare:
+                raise RuntimeError("ethane_liquid: no clash-free orientation; lower the density or min_dist")
+            at, keys = _place_ethane(rng, tmpl, spare.pop(), L, jitter, min_dist, grid, csz, ng)
         for p, k in zip(at, keys):
             grid.setdefault(k, []).append(p)
         placed.append(at)
@@ -195,6 +180,35 @@ def ethane_liquid(n_mol: int, density_g_cm3: float = 0.55, temp_k: float = 300.0
     z = np.tile(np.array([6, 6, 1, 1, 1, 1, 1, 1], np.int32), n_mol)
     vel = thermal_velocities(z, temp_k, rng)
     return _system(z, pos, vel, [L, L, L], [1, 1, 1])
+
+
+def _place_ethane(rng, tmpl, center0, L, jitter, min_dist, grid, csz, ng, attempts: int = 5000):
+    """A random orientation and jitter of one ethane molecule about a lattice
+    site with every atom at least min_dist from the atoms already placed:
+    (atoms, their grid cells), or (None, None) when `attempts` draws all clash."""
+    for _ in range(attempts):
+        R = _random_rotations(rng, 1)[0]
+        center = center0 + rng.uniform(-jitter, jitter, size=3)
+        at = np.mod((tmpl @ R.T) + center, L)
+        keys = [tuple((p // csz).astype(int) % ng) for p in at]
+        ok = True
+        for p, ci in zip(at, keys):
+            near = []
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        lst = grid.get(((ci[0] + dx) % ng, (ci[1] + dy) % ng, (ci[2] + dz) % ng))
+                        if lst:
+                            near.extend(lst)
+            if near:
+                d = p - np.array(near)
+                d -= L * np.round(d / L)
+                if np.min(np.einsum("ij,ij->i", d, d)) < min_dist * min_dist:
+                    ok = False
+                    break
+        if ok:
+            return at, keys
+    return None, None
 
 
 def amorphous_carbon(n: int, density_g_cm3: float = 2.0, min_sep: float = 1.2, temp_k: float = 0.0,

@@ -1,6 +1,6 @@
 """NVE energy behaviour over long runs: the GPU FP64 path against the
-reference's own SimLoop over 10^4 steps, and the FP32-mixed path against
-FP64.  Trajectories decorrelate after a few hundred steps (chaos), so the
+reference's own SimLoop (AIREBO here; REBO over 10^4 steps of the 1,728-atom
+diamond in test_gpu_configs.py), and the FP32-mixed path against FP64.  Trajectories decorrelate after a few hundred steps (chaos), so the
 long-run comparison is statistical: the linear drift of E_total after the
 first 1% of the steps and the RMS fluctuation about that line."""
 import numpy as np
@@ -20,29 +20,6 @@ def drift_stats(etot, n_atoms, dt_fs):
     t = (np.arange(k0, len(etot)) + 1) * dt_fs * 1e-3
     a, b = np.polyfit(t, e, 1)
     return float(a), float(np.sqrt(np.mean((e - (a * t + b)) ** 2)))
-
-
-def test_nve_drift_matches_reference_over_1e4_steps():
-    """REBO diamond (216 C, 300 K, dt 0.5 fs), 10^4 steps on both."""
-    s = B.diamond(3, temp_k=300.0, seed=101)
-    n = len(s["z"])
-    ctx = M.Context(potentials=M.POT_REBO)
-    ctx.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
-    _, et = ctx.run(10000, 0.5)
-    r = ref.RefSystem(ref.POT_REBO)
-    r.set_atoms(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
-    out = r.run(10000, 0.5)
-    # identical trajectories before they decorrelate
-    assert np.max(np.abs(et[:50] - out["etot"][:50])) / n < 1e-9
-    sg, fg = drift_stats(et, n, 0.5)
-    sr, fr = drift_stats(out["etot"], n, 0.5)
-    T = 10000 * 0.5e-3  # ps
-    # no secular drift on either: a slope below (fluctuation / run length)
-    # is indistinguishable from the fluctuation itself; the same slope within
-    # that resolution and the same fluctuation amplitude
-    assert abs(sr) < 10 * fr / T and abs(sg) < 10 * fr / T, (sg, sr, fr)
-    assert abs(sg - sr) < 10 * fr / T, (sg, sr, fr)
-    assert 0.8 < fg / fr < 1.25, (fg, fr)
 
 
 def test_airebo_drift_matches_reference():

@@ -66,11 +66,28 @@ def test_reference_arm_under_torchrun_two_ranks():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--cpu-steps", "2", "--steps", "2", "--warmup", "3"]
+           "--impl", "reference", "--gpus", "2", "--cpu-steps", "2", "--cpu-procs", "16", "--steps", "2",
+           "--warmup", "3"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-3000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 2
+    assert d["cpu_baseline"]["cores"] == 16
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def _build_headline(seed):
+    sys.path.insert(0, ROOT)
+    from bench import build_system
+    return seed, len(build_system(seed)["z"])
+
+
+def test_headline_system_builds_for_every_reference_arm_seed():
+    """The reference arm gives its k-th process seed k (1..cores); each must
+    build (a jammed lattice site moves to a spare one instead of raising)."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(8, os.cpu_count() or 1)) as pool:
+        out = pool.map(_build_headline, range(1, 17))
+    assert [n for _, n in out] == [43688] * 16
