@@ -132,6 +132,16 @@ int mdg_set_system(mdg_ctx* ctx, int n, const int32_t* z, const double* pos, con
  * NeighbourList.cxx:109-133). */
 int mdg_set_positions(mdg_ctx* ctx, const double* pos);
 
+/* Verlet-list maintenance at the current positions (FGeneral::NL_init,
+ * NL_checkRequestUpdate and NL_UpdateIfNeeded, FGeneral.hpp:71-91, over
+ * NeighbourList::Update / MovedTooMuch, NeighbourList.cxx:32-133).  force = 0:
+ * each list is rebuilt when the two largest displacements since its last
+ * build exceed its trigger (0.44 Rcut, or the absolute skin); force != 0:
+ * every list is rebuilt.  Displacements are measured on the device from the
+ * positions themselves, so FGeneral::incDisplacement has no counterpart.
+ * mdg_compute and mdg_run perform the same check on their own. */
+int mdg_nl_update(mdg_ctx* ctx, int force);
+
 /* Energy and gradient of the configured potentials at the current positions
  * (FProxy::operator(), FProxy.cxx:46-61).  e_total: total energy; e_terms
  * (NULL or [4]): REBO or Brenner, AIREBO LJ, torsion, 0; grad (NULL or [n*3]):

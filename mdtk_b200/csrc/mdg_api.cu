@@ -2311,6 +2311,18 @@ int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
   return MDG_OK;
 }
 
+int mdg_nl_update(mdg_ctx* c, int force)
+{
+  if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
+  if (force) {
+    const int one[3] = {1, 1, 1};
+    CK(cudaMemcpyAsync(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
+  }
+  int rc = rebuild_lists(c);
+  if (rc) return rc;
+  return read_status(c);
+}
+
 int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* count)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");

@@ -25,6 +25,10 @@ POT_ETORS = 4
 POT_BRENNER = 8
 POT_AIREBO = POT_REBO | POT_AIREBO_LJ | POT_ETORS
 POT_METAL = 16
+# the drop-in GPU classes (mdtk_b200/mdtk/GpuPotentials.hpp) in the FProxy in
+# place of the reference's own; needs install_gpu_shim() first
+POT_GPU = 64
+SHIM_PATH = os.path.join(HERE, "_ref", "libmdtkshim.so")
 
 _lib = None
 
@@ -78,6 +82,26 @@ def lib():
     return _lib
 
 
+_shim = None
+
+
+def install_gpu_shim():
+    """Load oracle/_ref/libmdtkshim.so (the GPU classes compiled against the
+    reference headers) and install its factory, so RefSystem(potset | POT_GPU)
+    holds GpuREBO / GpuAIREBO / GpuETors / GpuBrenner."""
+    global _shim
+    if _shim is None:
+        lib()
+        if not os.path.exists(SHIM_PATH):
+            raise RuntimeError(f"shim library missing: {SHIM_PATH} (run `make -C oracle`)")
+        S = ctypes.CDLL(SHIM_PATH)
+        S.shim_last_error.restype = ctypes.c_char_p
+        if S.shim_install() != 0:
+            raise RuntimeError("shim_install failed")
+        _shim = S
+    return _shim
+
+
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -98,7 +122,10 @@ class RefSystem:
     def __init__(self, potset: int, brenner_set: int = 1, lj_cut_mode: int = 0):
         h = lib().ref_create(potset, brenner_set, lj_cut_mode)
         if not h:
-            raise RuntimeError("oracle: " + lib().ref_last_error().decode())
+            msg = lib().ref_last_error().decode()
+            if potset & POT_GPU and _shim is not None:
+                msg += ": " + _shim.shim_last_error().decode()
+            raise RuntimeError("oracle: " + msg)
         self.h = ctypes.c_void_p(h)
         self.n = 0
         self.npot = lib().ref_num_potentials(self.h)

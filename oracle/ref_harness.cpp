@@ -45,7 +45,16 @@ namespace {
 
 std::string g_last_error;
 
-enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8, POT_METAL = 16 };
+enum { POT_REBO = 1, POT_AIREBO_LJ = 2, POT_ETORS = 4, POT_BRENNER = 8, POT_METAL = 16, POT_GPU = 64 };
+
+// Test support for the drop-in GPU classes (mdtk_b200/mdtk/GpuPotentials.hpp):
+// the library that binds them (oracle/shim_harness.cpp) installs a factory
+// here, and ref_create with POT_GPU builds its potential stack from it, in
+// place of the reference's own classes, so that the unmodified FProxy and
+// SimLoop drive the GPU path.  The factory adds the potentials to fpot and
+// returns their names (comma-separated).
+typedef const char* (*ref_gpu_factory_fn)(int potset, int brenner_set, int lj_cut_mode, mdtk::FProxy* fpot);
+ref_gpu_factory_fn g_gpu_factory = 0;
 
 double wall_now()
 {
@@ -180,6 +189,12 @@ extern "C" {
 
 const char* ref_last_error() { return g_last_error.c_str(); }
 
+int ref_set_gpu_factory(ref_gpu_factory_fn f)
+{
+  g_gpu_factory = f;
+  return 0;
+}
+
 void ref_set_verbose(int on) { yaatk::verboseTrace = (on != 0); }
 
 /* potset: bitmask of REBO(1) | AIREBO_LJ(2) | ETORS(4) | BRENNER(8).
@@ -195,6 +210,13 @@ void* ref_create(int potset, int brenner_set, int lj_cut_mode)
     c->brenner_set = brenner_set;
     c->lj_cut_mode = lj_cut_mode;
     c->loop.preventFileOutput = true;
+    if (potset & POT_GPU) {
+      if (!g_gpu_factory) throw Exception("no GPU potential factory installed");
+      const char* names = g_gpu_factory(potset & ~POT_GPU, brenner_set, lj_cut_mode, &c->loop.fpot);
+      if (!names) throw Exception("GPU potential factory failed");
+      c->names.push_back(names);
+      return c;
+    }
     if (potset & POT_METAL) {
       // the ion and metal-hydrocarbon pair potentials first, as
       // setupPotentials adds them (applications/common.h:45-50)
@@ -240,6 +262,9 @@ void* ref_create(int potset, int brenner_set, int lj_cut_mode)
   } catch (std::exception& e) {
     g_last_error = e.what();
     return 0;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return 0;
   }
 }
 
@@ -272,6 +297,9 @@ int ref_set_atoms(void* h, int n, const int* z, const double* pos, const double*
     c->nl_ready = false;
     return 0;
   } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  } catch (yaatk::Exception& e) {
     g_last_error = e.what();
     return -1;
   }
@@ -317,6 +345,9 @@ int ref_compute(void* h, double* e_total, double* e_terms, double* grad, double*
   } catch (std::exception& e) {
     g_last_error = e.what();
     return -1;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return -1;
   }
 }
 
@@ -337,6 +368,9 @@ int ref_energy_proxy(void* h, double* e_total, double* grad)
       }
     return 0;
   } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  } catch (yaatk::Exception& e) {
     g_last_error = e.what();
     return -1;
   }
@@ -364,6 +398,9 @@ long ref_nl_pairs(void* h, int index, int* pairs, long cap)
     }
     return cnt;
   } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  } catch (yaatk::Exception& e) {
     g_last_error = e.what();
     return -1;
   }
@@ -540,6 +577,9 @@ int ref_run(void* h, int nsteps, double dt_fs, double* pos, double* vel, int* im
   } catch (std::exception& e) {
     g_last_error = e.what();
     return -1;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return -1;
   }
 }
 
@@ -691,6 +731,9 @@ long ref_tables(int which, int brenner_set, double* out, long cap)
   } catch (std::exception& e) {
     g_last_error = e.what();
     return -1;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return -1;
   }
 }
 
@@ -736,6 +779,9 @@ int ref_spline_eval(int fn, int n, const double* x, double* out)
   } catch (std::exception& e) {
     g_last_error = e.what();
     return -1;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return -1;
   }
 }
 
@@ -764,6 +810,9 @@ int ref_write_state(void* h, const char* id)
   } catch (std::exception& e) {
     g_last_error = e.what();
     return -1;
+  } catch (yaatk::Exception& e) {
+    g_last_error = e.what();
+    return -1;
   }
 }
 
@@ -782,6 +831,10 @@ int ref_write_xva(void* h, const char* path)
     c->loop.preventFileOutput = true;
     return 0;
   } catch (std::exception& e) {
+    c->loop.preventFileOutput = true;
+    g_last_error = e.what();
+    return -1;
+  } catch (yaatk::Exception& e) {
     c->loop.preventFileOutput = true;
     g_last_error = e.what();
     return -1;
@@ -804,6 +857,9 @@ int ref_load_state(void* h, const char* id, unsigned long iteration)
     c->keep_time = true;
     return got;
   } catch (std::exception& e) {
+    g_last_error = e.what();
+    return -1;
+  } catch (yaatk::Exception& e) {
     g_last_error = e.what();
     return -1;
   }
@@ -999,6 +1055,10 @@ int ref_impact_sequence(int potset, const char* base_id, const char* ionpos_path
     }
     ionpos_bin.close();
   } catch (std::exception& e) {
+    g_last_error = e.what();
+    rc = -1;
+    if (chdir(cwd) != 0) rc = -1;
+  } catch (yaatk::Exception& e) {
     g_last_error = e.what();
     rc = -1;
     if (chdir(cwd) != 0) rc = -1;

@@ -217,3 +217,17 @@ def test_reference_xva_layout(tmp_path):
     tail = lines[3 + 3 * n:]
     assert tail[0] == "1" and tail[2] == "1" and tail[1].endswith(" ") and tail[9] == "4"
     assert all(len(t.split("e")) == 2 for t in tail[3:9] + [tail[10]])
+
+
+@pytest.mark.skipif(not os.path.exists(ref.SHIM_PATH), reason="shim library not built")
+def test_gpu_classes_load_and_fail_loudly_without_a_device():
+    """The drop-in GPU classes compiled against the reference headers load
+    beside the oracle; without a CUDA device their construction reports the
+    C ABI's error through the reference's own exception type instead of
+    falling back to anything."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    ref.install_gpu_shim()
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        ref.RefSystem(ref.POT_AIREBO | ref.POT_GPU)
