@@ -139,8 +139,10 @@ int mdg_set_positions(mdg_ctx* ctx, const double* pos);
  * build exceed its trigger (0.44 Rcut, or the absolute skin); force != 0:
  * every list is rebuilt.  Displacements are measured on the device from the
  * positions themselves, so FGeneral::incDisplacement has no counterpart.
- * mdg_compute and mdg_run perform the same check on their own. */
-int mdg_nl_update(mdg_ctx* ctx, int force);
+ * rebuilt: NULL or [3], set to 1 for each list (0 REBO/Brenner/torsion,
+ * 1 AIREBO LJ, 2 metal) that was rebuilt, else 0.  mdg_compute and mdg_run
+ * perform the same check on their own. */
+int mdg_nl_update(mdg_ctx* ctx, int force, int32_t* rebuilt);
 
 /* Energy and gradient of the configured potentials at the current positions
  * (FProxy::operator(), FProxy.cxx:46-61).  e_total: total energy; e_terms

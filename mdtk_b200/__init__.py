@@ -102,7 +102,7 @@ def lib():
         L.mdg_set_state.argtypes = [vp, dp, dp]
         L.mdg_compute.argtypes = [vp, dp, dp, dp]
         L.mdg_nl_pairs.argtypes = [vp, ctypes.c_int, i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
-        L.mdg_nl_update.argtypes = [vp, ctypes.c_int]
+        L.mdg_nl_update.argtypes = [vp, ctypes.c_int, i32p]
         L.mdg_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_set_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), i32p, dp, dp, dp, i32p,
                                     ctypes.POINTER(ctypes.c_uint8)]
@@ -455,9 +455,12 @@ class Context:
         _check(lib().mdg_compute(self.h, _dp(e), _dp(et), _dp(g)))
         return float(e[0]), et, g
 
-    def nl_update(self, force: bool = False):
-        """Rebuild the Verlet lists if the displacement criterion fires (or always, with force)."""
-        _check(lib().mdg_nl_update(self.h, 1 if force else 0))
+    def nl_update(self, force: bool = False) -> np.ndarray:
+        """Rebuild the Verlet lists if the displacement criterion fires (or
+        always, with force); returns which of the three lists were rebuilt."""
+        out = np.zeros(3, np.int32)
+        _check(lib().mdg_nl_update(self.h, 1 if force else 0, _ip(out)))
+        return out
 
     def nl_pairs(self, list_id: int) -> np.ndarray:
         cnt = ctypes.c_int64()

@@ -24,11 +24,13 @@
  * are used together, in one FProxy, as the reference uses REBO with AIREBO.
  *
  * Neighbour lists live on the device: NL_init loads the atoms and builds the
- * lists, NL_UpdateIfNeeded loads the current positions and rebuilds where
- * the device's displacement check (NeighbourList::MovedTooMuch,
+ * lists, NL_checkRequestUpdate loads the current positions and rebuilds the
+ * lists whose displacement check (NeighbourList::MovedTooMuch,
  * NeighbourList.cxx:109-133) fires (mdg_nl_update); the device measures the
- * displacements from the positions, so NL_checkRequestUpdate and
- * incDisplacement have nothing to do.  Errors come back as yaatk::Exception,
+ * displacements from the positions, so incDisplacement has nothing to do.
+ * After each device build a term copies its list into its NeighbourList, so
+ * FGeneral::NL and FProxy::hasNeighbors (SimLoop.cxx:394-398) see the
+ * reference's lists.  Errors come back as yaatk::Exception,
  * the reference's own (REQUIRE), which SimLoop::execute catches
  * (SimLoop.cxx:176-205).
  *
@@ -71,6 +73,7 @@ public:
     p.units = MDG_UNITS_CGS;
     if (mdg_create(&p, &ctx_) != MDG_OK) throw yaatk::Exception(mdg_last_error());
     for (int t = 0; t < 4; t++) eterms_[t] = 0.0;
+    for (int l = 0; l < 3; l++) builds_[l] = 0;
   }
 
   // the device context (for the C ABI's other entry points)
@@ -93,16 +96,45 @@ public:
     return 2.0 * Ao;
   }
 
+  // NL_init: load the atoms and build every list
   void nl_init(AtomsArray& atoms)
   {
     load(atoms, true);
-    check(mdg_nl_update(ctx_, 1));
+    int32_t rebuilt[3];
+    check(mdg_nl_update(ctx_, 1, rebuilt));
+    for (int l = 0; l < 3; l++) builds_[l]++;
   }
 
+  // NL_checkRequestUpdate / NL_UpdateIfNeeded: load the current positions
+  // and rebuild the lists whose displacement check fires
   void nl_update(AtomsArray& atoms)
   {
     load(atoms, false);
-    check(mdg_nl_update(ctx_, 0));
+    int32_t rebuilt[3] = {0, 0, 0};
+    check(mdg_nl_update(ctx_, 0, rebuilt));
+    for (int l = 0; l < 3; l++) builds_[l] += rebuilt[l];
+  }
+
+  // how many times list l (0: REBO / Brenner / torsion, 1: AIREBO LJ) was built
+  unsigned long builds(int l) const { return builds_[l]; }
+
+  // the device's list l as the reference's NeighbourList holds it:
+  // nl[i] = the partners of atom i in ascending order (NeighbourList.cxx:73-106
+  // pushes them so), so that FGeneral::NL and FProxy::hasNeighbors read
+  // what they read from the reference's own lists
+  void export_list(AtomsArray& atoms, int l, std::vector<AtomRefsContainer>& nl)
+  {
+    int64_t cnt = 0;
+    check(mdg_nl_pairs(ctx_, l, 0, 0, &cnt));
+    std::vector<int32_t> pairs(2 * (size_t)cnt + 2);
+    check(mdg_nl_pairs(ctx_, l, &pairs[0], cnt, &cnt));
+    nl.resize(atoms.size());
+    for (size_t i = 0; i < nl.size(); i++) nl[i].clear();
+    for (int64_t q = 0; q < cnt; q++) {
+      const int32_t i = pairs[2 * q], j = pairs[2 * q + 1];
+      nl[i].push_back(&atoms[j]);
+      nl[j].push_back(&atoms[i]);
+    }
   }
 
   // FGeneral::operator() of term t
@@ -189,13 +221,14 @@ private:
   bool loaded_, evaluated_, grad_pending_;
   std::vector<double> pos_, uploaded_, at_eval_, grad_;
   double eterms_[4];
+  unsigned long builds_[3];
 };
 
 // One term of a GpuStack, with FGeneral's interface (FGeneral.hpp:54-114).
 class GpuTerm : public FManybody
 {
 public:
-  GpuTerm(GpuStack* stack, GpuStack::Term term) : FManybody(), stack_(stack), term_(term)
+  GpuTerm(GpuStack* stack, GpuStack::Term term) : FManybody(), stack_(stack), term_(term), seen_(0)
   {
     stack_->attach();
     handledElements.insert(H_EL);
@@ -209,23 +242,42 @@ public:
   Float operator()(AtomsArray& atoms) { return stack_->energy(atoms, term_); }
   Float getRcutoff() const { return stack_->rcutoff(term_); }
 
-  // FProxy forwards each of these to every potential; the stack's first
-  // term does the work and the others find nothing left to do
+  // FProxy::NL_init and NL_checkRequestUpdate call these on every potential
+  // in order (FProxy.hpp:59-71); the stack's first term (REBO or Brenner)
+  // does the device work and every term then copies its own list out when
+  // the device rebuilt it.  nl.ListUpdateRequested stays false, so
+  // FProxy::NL_UpdateIfNeeded never runs the CPU list build on these terms.
   void NL_init(AtomsArray& atoms)
   {
+    nl.init(atoms);
+    nl.ListUpdateRequested = false;
     if (first()) stack_->nl_init(atoms);
+    refresh(atoms);
   }
-  void NL_checkRequestUpdate(AtomsArray&) {}
-  void NL_UpdateIfNeeded(AtomsArray& atoms)
+  void NL_checkRequestUpdate(AtomsArray& atoms)
   {
     if (first()) stack_->nl_update(atoms);
+    refresh(atoms);
+    nl.ListUpdateRequested = false;
   }
+  void NL_UpdateIfNeeded(AtomsArray& atoms) { NL_checkRequestUpdate(atoms); }
+  // the device measures displacements from the positions themselves
   void incDisplacement(Atom&, Vector3D) {}
 
 private:
   bool first() const { return term_ == GpuStack::TERM_REBO || term_ == GpuStack::TERM_BRENNER; }
+  int list_id() const { return term_ == GpuStack::TERM_LJ ? 1 : 0; }
+  void refresh(AtomsArray& atoms)
+  {
+    const unsigned long b = stack_->builds(list_id());
+    if (b != seen_) {
+      stack_->export_list(atoms, list_id(), nl.nl);
+      seen_ = b;
+    }
+  }
   GpuStack* stack_;
   GpuStack::Term term_;
+  unsigned long seen_;  // the stack's build count of this term's list when nl.nl was copied
 };
 
 // REBO (AIREBO/REBO.hpp) on the device

@@ -56,6 +56,9 @@ def test_fproxy_over_gpu_classes_matches_reference_classes(name):
     gp = np.zeros((len(s["z"]), 3))
     ref._check(ref.lib().ref_energy_proxy(gpu.h, ref._dp(ep), ref._dp(gp)))
     assert_parity(float(ep[0]), gp, eo, go, floor, label=f"shim FProxy {name}")
+    # each class's NeighbourList holds the device's list, as FGeneral::NL reads it
+    for k in range(cpu.npot):
+        assert np.array_equal(gpu.nl_pairs(k), cpu.nl_pairs(k)), k
 
 
 @pytest.mark.parametrize("name", ["ethane30", "diamond3_rebo_tors", "ac300_brenner1"])
