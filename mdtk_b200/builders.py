@@ -352,13 +352,15 @@ def relax_hot(s: Dict[str, np.ndarray], steps: int, temp_k: float, dt: float, po
     """Pre-relaxation of a random packing: `steps` velocity-Verlet steps on
     the GPU (mdg) with the velocities rescaled to temp_k after every step (a
     seeded Maxwell-Boltzmann start).  Returns a copy of s with the relaxed,
-    wrapped positions and the final velocities."""
+    wrapped positions and the final velocities; the same on every run."""
     from mdtk_b200 import Context
 
     rng = np.random.default_rng(seed)
     out = dict(s)
     vel = thermal_velocities(s["z"], temp_k, rng, s.get("fixed"))
-    ctx = Context(potentials=potentials, device=device)
+    # one fixed REBO work split: the two splits agree to rounding only, and
+    # 500 hot steps would turn a timing-dependent choice into a different state
+    ctx = Context(potentials=potentials, device=device, task_mode=1)
     ctx.set_system(s["z"], s["pos"], vel, s["box"], s["pbc"], s.get("fixed"))
     for _ in range(steps):
         ctx.run(1, dt, energies=False)

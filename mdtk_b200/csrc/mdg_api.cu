@@ -278,6 +278,18 @@ __global__ void k_rebo(const ReboParams* P, const ReboTables* T, BondList B, Tor
   rebo_atom(R, TP, do_rebo, do_tors, O, a);
 }
 
+// Task index of this thread in a grid-stride loop over a queue whose front
+// holds the heaviest tasks (C-C bonds): consecutive warps of tasks go to
+// consecutive blocks (warp w of block b takes task warp w * gridDim.x + b),
+// so the heavy front of the queue is spread one warp per block over every SM
+// instead of filling the first few blocks (and SMs).  A permutation of
+// 0 .. gridDim.x * blockDim.x - 1.
+__device__ __forceinline__ long spread_task_index()
+{
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  return ((long)w * gridDim.x + blockIdx.x) * 32 + lane;
+}
+
 // REBO + torsion, one thread per directed bond slot, over a grid sized to the
 // resident capacity of the GPU (grid-stride over the queue).
 template <class Real, class TB>
@@ -287,7 +299,7 @@ __global__ void __launch_bounds__(128) k_rebo_task(const ReboParams* P, const TB
   pdl_enter();
   const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
   ReboT<Real, TB> R{*P, *T, B, status};
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
+  for (long t = spread_task_index(); t < nt; t += (long)gridDim.x * blockDim.x) {
     const int q = t < n0 ? K.q[t] : K.q[K.cap - 1 - (t - n0)];
     const int a = q / B.mb, s = q - a * B.mb;
     const long rb = K.rbase[a];
@@ -305,7 +317,7 @@ __global__ void __launch_bounds__(128) k_rebo_pair_task(const ReboParams* P, con
   pdl_enter();
   const long n0 = (long)K.ctr[0], nt = n0 + (long)K.ctr[1];
   ReboT<Real, TB> R{*P, *T, B, status};
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nt; t += (long)gridDim.x * blockDim.x) {
+  for (long t = spread_task_index(); t < nt; t += (long)gridDim.x * blockDim.x) {
     const int q = t < n0 ? K.q[t] : K.q[K.cap - 1 - (t - n0)];
     const int lo = q / B.mb, s = q - lo * B.mb;
     const int hi = B.bj[q], sh = B.brev[q];
@@ -339,6 +351,9 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
     t0 = Tk.off[a];
     t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
   }
+  // the LJ pass over REBO sums already in place: an atom without special
+  // pair records keeps every element as it is
+  if (!rebo_tasks && with_lj && t1 <= t0) return;
   for (int e = l; e < nel; e += G) {
     int roff = -1, loff = -1;
     double* dst;
@@ -1623,15 +1638,17 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
              c->lj_inr_cnt);
   }
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
-  LAUNCH(c, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
   const bool f32p = c->prm.precision == MDG_PREC_FP32_MIXED;
   cudaStream_t rs = c->stream;
   if (ovl) {
+    // the reverse slots, the REBO bond tasks and the reduction of their
+    // records on the second stream: none of the LJ kernels reads them
     CK(cudaEventRecord(c->ev_fork, c->stream));
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     rs = c->side;
   }
+  LAUNCH_ON(c, rs, "bonds_rev", k_brev, nblk(c->n), kThreads, c->bb, c->bt, c->d_status);
   if (tasks) {
     const int ir = rebo ? 1 : 0, it = tors ? 1 : 0;
     const int grid = c->rebo_grid > 0 ? c->rebo_grid : c->rebo_task_blocks;
@@ -1656,7 +1673,13 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
   else
     LAUNCH(c, "rebo_tors", k_rebo, nblk(c->n), kThreads, c->d_rp, c->d_tables, B, c->tp, rebo ? 1 : 0,
            tors ? 1 : 0, c->fo, c->d_status);
-  if (ovl) CK(cudaEventRecord(c->ev_join, c->side));
+  if (ovl) {
+    // the REBO half of the record sums; the LJ half adds to it after the join
+    // (the same additions in the same order as one combined pass)
+    LAUNCH_ON(c, rs, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt, 1,
+              c->spc, 0, c->fo);
+    CK(cudaEventRecord(c->ev_join, c->side));
+  }
   if (pot & MDG_POT_BRENNER)
     LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
@@ -1697,10 +1720,14 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
              c->spc, c->d_status);
     }
   }
-  if (ovl) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
-  if (tasks || lj)
+  if (ovl) {
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    LAUNCH(c, "lj_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt, 0, c->spc,
+           1, c->fo);
+  } else if (tasks || lj) {
     LAUNCH(c, "bond_reduce", k_bond_reduce<kReduceLanes>, nblk(c->n * kReduceLanes), kThreads, B, c->bt,
            tasks ? 1 : 0, c->spc, lj ? 1 : 0, c->fo);
+  }
   if (c->has_list[2]) {
     LAUNCH(c, "eam_density", k_eam_rho, nblk(c->n * 32), kThreads, S, c->nl[2], c->d_metal, c->d_fp, c->d_em,
            c->d_status);
@@ -2311,7 +2338,7 @@ int mdg_compute(mdg_ctx* c, double* e_total, double* e_terms, double* grad)
   return MDG_OK;
 }
 
-int mdg_nl_update(mdg_ctx* c, int force)
+int mdg_nl_update(mdg_ctx* c, int force, int32_t* rebuilt)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (force) {
@@ -2320,7 +2347,13 @@ int mdg_nl_update(mdg_ctx* c, int force)
   }
   int rc = rebuild_lists(c);
   if (rc) return rc;
-  return read_status(c);
+  int need[3] = {0, 0, 0};
+  CK(cudaMemcpyAsync(need, c->d_need, sizeof(need), cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  if (rebuilt)
+    for (int l = 0; l < 3; l++) rebuilt[l] = (c->has_list[l] && need[l]) ? 1 : 0;
+  return MDG_OK;
 }
 
 int mdg_nl_pairs(mdg_ctx* c, int list_id, int32_t* pairs, int64_t cap, int64_t* count)

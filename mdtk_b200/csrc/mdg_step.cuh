@@ -55,7 +55,14 @@ struct State {
 };
 
 // The periodic box atom a lives in.
-MDG_HD const Box& box_of(const State& S, int a) { return S.sys ? S.boxes[S.sys[a]] : S.box; }
+// By value: a reference that may point at the kernel parameter S.box would
+// make every thread copy the parameter to local memory.
+MDG_HD Box box_of(const State& S, int a)
+{
+  Box b = S.box;  // loaded field by field: no pointer to the parameter is formed
+  if (S.sys) b = S.boxes[S.sys[a]];
+  return b;
+}
 
 // The cell grid of atom a's system.
 struct GridView {
