@@ -151,7 +151,9 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mdg", choices=["mdg", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps-per-call", type=int, default=10,
+                    help="steps per mdg_step_host call in the end-to-end measurement")
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--cpu-procs", type=int, default=0,
                     help="processes of the reference arm (default: every usable host core)")
@@ -292,29 +294,44 @@ def main():
     if flops_per_atom:
         achieved = flops_per_atom * n / (kern[top]["ms_per_launch"] * 1e-3) / 1e12
         roof = {"kernel": top, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak, "traffic": TRAFFIC_PER_LAUNCH.get(top),
+                "frac": achieved / fp64_peak, "traffic": TRAFFIC_PER_LAUNCH.get((top, tuned["rebo_task_mode"])),
+                "traffic_split": tuned["rebo_task_mode"],
                 "peak_source": "measured FP64 FMA probe (mdg_pipe_peak) on this GPU",
                 "flops_per_atom": flops_per_atom,
                 "step": {"flops_per_atom": STEP_FLOPS_PER_ATOM,
                          "achieved": STEP_FLOPS_PER_ATOM * n / (total_ms / args.steps * 1e-3) / 1e12,
                          "frac": STEP_FLOPS_PER_ATOM * n / (total_ms / args.steps * 1e-3) / 1e12 / fp64_peak}}
 
-    # end to end through the C ABI with host buffers (pinned), one step per call
+    # end to end through the C ABI with host buffers (pinned): each
+    # mdg_step_host call takes the state (positions, velocities) from the
+    # caller's arrays, advances k steps and returns the state and every step's
+    # potential and total energy.  The headline calls k = --e2e-steps-per-call
+    # steps at a time; beside it, k = 1 (the state crosses PCIe every step).
     pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     vel = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     p0, v0, _ = ctx.get_state()
     pos[:] = p0
     vel[:] = v0
-    ctx.step_host(1, DT_FS, pos, vel)
-    barrier()
-    t0 = time.perf_counter()
-    for k in range(args.e2e_steps):
-        ctx.step_host(1, DT_FS, pos, vel)
-    t_e2e = time.perf_counter() - t0
-    t_e2e = reps.max(t_e2e)
-    e2e = {"value": world * n * args.e2e_steps / t_e2e, "unit": "atom-steps/s",
-           "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 2 * 24 * n + 4 * 8,
-           "steps": args.e2e_steps, "timer": "host wall clock around mdg_step_host calls (each ends synchronised)"}
+
+    def e2e_rate(k, calls):
+        ctx.step_host(k, DT_FS, pos, vel)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            ctx.step_host(k, DT_FS, pos, vel)
+        t = reps.max(time.perf_counter() - t0)
+        return world * n * k * calls / t
+
+    kc = max(1, args.e2e_steps_per_call)
+    calls = max(1, args.e2e_steps // kc)
+    state_bytes = 2 * 24 * n  # [n*3] positions and velocities, FP64
+    e2e = {"value": e2e_rate(kc, calls), "unit": "atom-steps/s",
+           "h2d_bytes_per_step": state_bytes / kc, "d2h_bytes_per_step": state_bytes / kc + 2 * 8,
+           "steps": kc * calls, "steps_per_call": kc,
+           "timer": "host wall clock around mdg_step_host calls (each ends synchronised)"}
+    e2e["one_step_per_call"] = {"value": e2e_rate(1, args.e2e_steps), "unit": "atom-steps/s",
+                                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes + 2 * 8,
+                                "steps": args.e2e_steps}
 
     # FP32-mixed variant on the same workload, from the FP64 run's final state:
     # device time per step (same protocol) and its force error against the
@@ -786,9 +803,17 @@ def precision_study(args, local, rank):
 # products); lj_special = the b*_ij bond orders of close non-bonded pairs.
 FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_plain": 5151.5, "lj_special": 5205.5}
 STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
-# dram read+write bytes per launch from an ncu capture of the same workload
-# (`ncu --set full`, one launch of each kernel), or None.
-TRAFFIC_PER_LAUNCH = {"rebo_tors": 22.84e6, "lj_plain": 22.85e6, "lj_special": 22.70e6, "lj_filter": 36.49e6}
+# DRAM read + write bytes per launch of each kernel on this workload, from
+# one ncu capture of the kernel (profiles/, captured with
+#   ncu --set full --clock-control none -k regex:<kernel> -c <few> ...
+# on one GPU), keyed by the REBO work split the timed step ran (the
+# autotuner's choice: "per bond" or "directed"); None when not captured.
+TRAFFIC_PER_LAUNCH = {
+    ("rebo_tors", "per bond"): 10.95e6, ("rebo_tors", "directed"): 22.83e6,
+    ("lj_special", "per bond"): 25.68e6, ("lj_special", "directed"): 22.89e6,
+    ("lj_plain", "per bond"): 22.89e6, ("lj_plain", "directed"): 22.89e6,
+    ("lj_filter", "per bond"): 36.64e6, ("lj_filter", "directed"): 36.64e6,
+}
 
 
 if __name__ == "__main__":

@@ -1248,37 +1248,6 @@ void prof_end(mdg_ctx* c)
   cudaEventRecord(pool_event(c), c->stream);
 }
 
-void set_rebo_params(ReboParams& p)
-{
-  std::memset(&p, 0, sizeof(p));
-  const int C = kC, H = kH;
-  // REBO::setupPotential1 (REBO.cxx:857-938), converted to A / eV
-  p.Q[C][C] = 0.313460; p.Q[C][H] = p.Q[H][C] = 0.340776; p.Q[H][H] = 0.370471;
-  p.alpha[C][C] = 4.7465391; p.alpha[C][H] = p.alpha[H][C] = 4.1025498; p.alpha[H][H] = 3.5362986;
-  p.A[C][C] = 10953.544; p.A[C][H] = p.A[H][C] = 149.94099; p.A[H][H] = 32.817356;
-  p.B[0][C][C] = 12388.792; p.B[0][C][H] = p.B[0][H][C] = 32.355187; p.B[0][H][H] = 29.632593;
-  p.B[1][C][C] = 17.567065;
-  p.B[2][C][C] = 30.714932;
-  p.beta[0][C][C] = 4.7204523; p.beta[0][C][H] = p.beta[0][H][C] = 1.4344581; p.beta[0][H][H] = 1.7158922;
-  p.beta[1][C][C] = 1.4332132;
-  p.beta[2][C][C] = 1.3826913;
-  p.rho[C][H] = p.rho[H][C] = 1.09; p.rho[H][H] = 0.7415887;
-  p.R[C][C][0] = 1.7; p.R[H][H][0] = 1.1; p.R[C][H][0] = p.R[H][C][0] = 1.3;
-  p.R[C][C][1] = 2.0; p.R[H][H][1] = 1.7; p.R[C][H][1] = p.R[H][C][1] = 1.8;
-  p.Rp[C][C][0] = 1.7; p.Rp[H][H][0] = 1.1; p.Rp[C][H][0] = p.Rp[H][C][0] = 1.3;
-  p.Rp[C][C][1] = 2.0; p.Rp[H][H][1] = 1.7; p.Rp[C][H][1] = p.Rp[H][C][1] = 1.6;
-  p.Ntot[0] = 2;
-  p.Ntot[1] = 3;
-}
-
-void set_tors_params(TorsParams& t)
-{
-  // ETors::setupPotential (AIREBO_ETors.cxx:125-133)
-  t.eps[kC][kC] = 0.3079;
-  t.eps[kH][kH] = 0.1250;
-  t.eps[kC][kH] = t.eps[kH][kC] = 0.1787;
-}
-
 int launch_check(mdg_ctx* c)
 {
   cudaError_t e = cudaGetLastError();
@@ -1838,8 +1807,8 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   if (c->prm.cap_special <= 0) c->prm.cap_special = 64;
   if (c->prm.special_avg <= 0) c->prm.special_avg = 48;
   c->mb = c->prm.cap_bonds;
-  set_rebo_params(c->rp);
-  set_tors_params(c->tp);
+  fill_rebo_params(c->rp);
+  fill_tors_params(c->tp);
   set_lj_params(c->ljp, c->prm.lj_cut_mode);
   if (p->units == MDG_UNITS_CGS) {
     c->unit_len = 1.0 / kAo;          // cm -> A

@@ -86,29 +86,6 @@ int na_fail(int code, const std::string& msg)
   return code;
 }
 
-void na_rebo_params(ReboParams& p)
-{
-  // REBO::setupPotential1 (REBO.cxx:857-938), A / eV
-  std::memset(&p, 0, sizeof(p));
-  const int C = kC, H = kH;
-  p.Q[C][C] = 0.313460; p.Q[C][H] = p.Q[H][C] = 0.340776; p.Q[H][H] = 0.370471;
-  p.alpha[C][C] = 4.7465391; p.alpha[C][H] = p.alpha[H][C] = 4.1025498; p.alpha[H][H] = 3.5362986;
-  p.A[C][C] = 10953.544; p.A[C][H] = p.A[H][C] = 149.94099; p.A[H][H] = 32.817356;
-  p.B[0][C][C] = 12388.792; p.B[0][C][H] = p.B[0][H][C] = 32.355187; p.B[0][H][H] = 29.632593;
-  p.B[1][C][C] = 17.567065;
-  p.B[2][C][C] = 30.714932;
-  p.beta[0][C][C] = 4.7204523; p.beta[0][C][H] = p.beta[0][H][C] = 1.4344581; p.beta[0][H][H] = 1.7158922;
-  p.beta[1][C][C] = 1.4332132;
-  p.beta[2][C][C] = 1.3826913;
-  p.rho[C][H] = p.rho[H][C] = 1.09; p.rho[H][H] = 0.7415887;
-  p.R[C][C][0] = 1.7; p.R[H][H][0] = 1.1; p.R[C][H][0] = p.R[H][C][0] = 1.3;
-  p.R[C][C][1] = 2.0; p.R[H][H][1] = 1.7; p.R[C][H][1] = p.R[H][C][1] = 1.8;
-  p.Rp[C][C][0] = 1.7; p.Rp[H][H][0] = 1.1; p.Rp[C][H][0] = p.Rp[H][C][0] = 1.3;
-  p.Rp[C][C][1] = 2.0; p.Rp[H][H][1] = 1.7; p.Rp[C][H][1] = p.Rp[H][C][1] = 1.6;
-  p.Ntot[0] = 2;
-  p.Ntot[1] = 3;
-}
-
 // Once per device, with that device current: resolve the device addresses of
 // the static arrays (their host-side names are only stand-ins) and upload the
 // spline tables and parameters.
@@ -131,7 +108,7 @@ int na_setup(int dev, DeviceSetup** out)
       built = true;
     }
     ReboParams hp;
-    na_rebo_params(hp);
+    fill_rebo_params(hp);
     e = cudaMemcpyToSymbol(g_noalloc_tables, &host_tables, sizeof(ReboTables));
     if (e != cudaSuccess) return na_fail(MDG_ERR_CUDA, std::string("cudaMemcpyToSymbol: ") + cudaGetErrorString(e));
     e = cudaMemcpyToSymbol(g_noalloc_params, &hp, sizeof(ReboParams));
@@ -313,9 +290,7 @@ int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const d
   e = cudaMemsetAsync(v.status, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess) return na_fail(MDG_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   TorsParams tp;
-  tp.eps[kC][kC] = 0.3079;  // ETors::setupPotential (AIREBO_ETors.cxx:125-133)
-  tp.eps[kH][kH] = 0.1250;
-  tp.eps[kC][kH] = tp.eps[kH][kC] = 0.1787;
+  fill_tors_params(tp);
   const int T = 128, B = (n + T - 1) / T;
   k_na_pack<<<B, T, 0, st>>>(v, pos, z);
   k_na_nl<<<B, T, 0, st>>>(v);

@@ -15,6 +15,11 @@ void build_rebo_tables(ReboTables* tb, std::vector<double>* flat_out);
 // re-expanded about each cell's lower corner, rounded to float.
 void build_rebo_tables32(const ReboTables& d, ReboTables32* f);
 
+// REBO::setupPotential1 (REBO.cxx:857-938) and ETors::setupPotential
+// (AIREBO_ETors.cxx:125-133) parameters, Angstrom / eV.
+void fill_rebo_params(ReboParams& p);
+void fill_tors_params(TorsParams& t);
+
 struct BrennerTables;
 // Brenner H_CC / H_CH / F tables of parameter set 1 or 2, same layout rules.
 void build_brenner_tables(int set, BrennerTables* tb, std::vector<double>* flat_out);
