@@ -34,6 +34,7 @@ N_MOL = 5461
 DT_FS = 0.25
 BATCH_SYSTEMS = 256
 BATCH_DT_FS = 0.2
+TASK_MODE_NAMES = {1: "directed", 2: "per bond", 3: "lane pairs"}
 WORKLOAD = (f"FP64 AIREBO ethane liquid: {N_MOL} C2H6 ({8 * N_MOL} atoms), 0.55 g/cm^3, 300 K, "
             f"dt {DT_FS} fs, reference cutoffs and 0.44 Rcut skin")
 
@@ -159,8 +160,9 @@ def main():
                     help="processes of the reference arm (default: every usable host core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
-    ap.add_argument("--task-mode", type=int, default=0, choices=[0, 1, 2],
-                    help="REBO work split of the headline context: 0 autotuned, 1 directed, 2 per bond")
+    ap.add_argument("--task-mode", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="REBO work split of the headline context: 0 autotuned, 1 directed, 2 per bond, "
+                         "3 per bond on lane pairs")
     ap.add_argument("--precision-study", action="store_true",
                     help="instead of the throughput line: the FP32-mixed vs FP64 study on the 512,000-atom diamond")
     ap.add_argument("--study-steps", type=int, default=5000)
@@ -227,10 +229,10 @@ def main():
     # warm-up (also builds the lists and the initial accelerations)
     ctx.run(max(args.warmup, 3), DT_FS, energies=False)
     ctx.sync()
-    mode, ms_dir, ms_pair = ctx.task_mode()
+    mode, ms_dir, ms_pair, ms_split = ctx.task_mode()
     ovl, rblocks = ctx.tuned_launch()
-    tuned = {"rebo_task_mode": "per bond" if mode == 2 else "directed", "eval_ms_directed": ms_dir,
-             "eval_ms_per_bond": ms_pair, "overlap": bool(ovl), "rebo_blocks": rblocks}
+    tuned = {"rebo_task_mode": TASK_MODE_NAMES[mode], "eval_ms_directed": ms_dir, "eval_ms_per_bond": ms_pair,
+             "eval_ms_lane_pairs": ms_split, "overlap": bool(ovl), "rebo_blocks": rblocks}
 
     # L2 flush buffer (the per-step working set is below the 126 MB L2)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")

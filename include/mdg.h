@@ -85,12 +85,15 @@ typedef struct mdg_params {
                          0 = default (174: six bonds per atom) */
   int task_mode;      /* REBO work split: 1 = one task per directed bond (both ends evaluate each
                          bond, shortest critical path), 2 = one task per bond writing both ends'
-                         records (half the work); 0 = timed once per system on the first mdg_run
-                         (the autotuner) and the faster kept.  Both route the same terms into the
-                         same records; results agree to rounding (the two kernels may contract
-                         multiply-adds differently).  With the LJ term the launch configuration
-                         (stream overlap, REBO grid) is timed on the first mdg_run in every mode;
-                         it never changes results. */
+                         records (half the work), 3 = per bond on a pair of lanes, each lane the
+                         bond-order terms of one end, and the torsion of each C-C bond a task of
+                         its own (a bond's serial chain about halved); 0 = timed once per system
+                         on the first mdg_run (the autotuner) and the fastest kept.  All route the
+                         same terms into the same records; results agree to rounding (the kernels
+                         may contract multiply-adds differently and mode 3 adds an end's pieces in
+                         two sums).  With the LJ term the launch configuration (stream overlap,
+                         REBO grid) is timed on the first mdg_run in every mode; it never changes
+                         results. */
 } mdg_params;
 
 /* Fill *p with the defaults: REBO only, FP64, Angstrom/eV/fs, reference cutoffs and skin. */
@@ -267,9 +270,10 @@ int mdg_adjoint_backward(mdg_ctx* ctx, const double* seed_pos, const double* see
 int mdg_rebo_compute_noalloc(int n, const double* pos, const int32_t* z, const double box[3], const int32_t pbc[3],
                              int with_torsion, double* energy, double* grad, void* stream);
 
-/* The REBO task mode in use (1 directed, 2 per bond) and, when the autotuner
- * ran, its timings of one force evaluation in each mode (ms; 0 otherwise). */
-int mdg_task_mode(mdg_ctx* ctx, int* mode, float* ms_directed, float* ms_per_bond);
+/* The REBO task mode in use (1 directed, 2 per bond, 3 per bond on lane
+ * pairs) and, when the autotuner ran, its timings of one force evaluation in
+ * each mode (ms; 0 otherwise).  No reference counterpart. */
+int mdg_task_mode(mdg_ctx* ctx, int* mode, float* ms_directed, float* ms_per_bond, float* ms_split);
 
 /* ---- Thermal bath and adaptive time step ----
  * The SimLoop step's thermal bath (SimLoop.cxx:352-388, geometries

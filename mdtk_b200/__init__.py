@@ -108,7 +108,7 @@ def lib():
                                     ctypes.POINTER(ctypes.c_uint8)]
         L.mdg_batch_energies.argtypes = [vp, dp]
         L.mdg_task_mode.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
-                                    ctypes.POINTER(ctypes.c_float)]
+                                    ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.mdg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.mdg_tuned_launch.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.mdg_set_dependent_launch.argtypes = [vp, ctypes.c_int]
@@ -275,13 +275,15 @@ class Context:
         self.nsys = len(systems)
 
     def task_mode(self):
-        """(mode, ms_directed, ms_per_bond): REBO task mode in use (1 directed,
-        2 per bond) and the autotuner's timings (0 when it did not run)."""
+        """(mode, ms_directed, ms_per_bond, ms_split): REBO task mode in use
+        (1 directed, 2 per bond, 3 per bond on lane pairs) and the autotuner's
+        timings (0 when it did not run)."""
         m = ctypes.c_int()
         a = ctypes.c_float()
         b = ctypes.c_float()
-        _check(lib().mdg_task_mode(self.h, ctypes.byref(m), ctypes.byref(a), ctypes.byref(b)))
-        return m.value, a.value, b.value
+        d = ctypes.c_float()
+        _check(lib().mdg_task_mode(self.h, ctypes.byref(m), ctypes.byref(a), ctypes.byref(b), ctypes.byref(d)))
+        return m.value, a.value, b.value, d.value
 
     def set_thermal_bath(self, geom: int, T0: float = 0.0, gamma: float = 0.01, params=None, apply=None):
         """SimLoop's thermal bath: geom TB_* , T0 (K), gamma (1/time unit),

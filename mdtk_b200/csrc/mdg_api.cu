@@ -237,7 +237,9 @@ __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
     }
   }
   if (!K.ctr) return;  // uniform over the launch
-  const unsigned long long need = ok ? (unsigned long long)nb * bond_rec_size(nb) : 0ull;
+  // records: one per bond slot, then (split mode with torsion) one per C-C bond
+  const int nrec = nb + ((K.pairs == 2 && K.tors) ? ncc : 0);
+  const unsigned long long need = ok ? (unsigned long long)nrec * bond_rec_size(nb) : 0ull;
   const unsigned long long rb = warp_alloc(need, &K.ctr[2]);
   // queued slots: all (one task per directed slot) or those to higher
   // partners (one task per bond)
@@ -258,6 +260,7 @@ __global__ void k_brev(BondBuild B, BondTasks K, unsigned int* status)
   } else {
     K.rbase[a] = (long)rb;
   }
+  K.nrec[a] = nrec;
   int f = (int)i0, b = (int)i1;
   for (int s = 0; s < nb; s++) {
     const int j = B.bj[a * B.mb + s];
@@ -328,6 +331,220 @@ __global__ void __launch_bounds__(128) k_rebo_pair_task(const ReboParams* P, con
   }
 }
 
+// The other lane's value of a lane pair (mask pm).
+__device__ __forceinline__ double pair_swap(double v, unsigned pm) { return __shfl_xor_sync(pm, v, 1); }
+__device__ __forceinline__ f32 pair_swap(f32 v, unsigned pm)
+{
+  f32 r;
+  r.v = __shfl_xor_sync(pm, v.v, 1);
+  return r;
+}
+
+// b-bar of bond (i, j), i < j, p = i -> j (REBO::Baver, REBO.cxx:200-211)
+// split over the lane pair of the bond: lane e evaluates p^{sigma pi} of its
+// own end (i for e = 0, j for e = 1) with its gradient, its half of N^conj
+// and its end's third-shell terms; the two lanes trade p^{sigma pi} and the
+// N^conj halves by shuffles and both evaluate pi^rc (and pi^dh, whose
+// pair-vector pieces lane 0 keeps).  Every term is the one the whole-bond
+// evaluation computes, in the same order within each end's record.
+template <class Real, class TB>
+__device__ Real baver_end(const ReboT<Real, TB>& R, int e, int i, int j, const PairGT<Real>& p, Real V,
+                          EndSinkT<Real>& sink, unsigned pm)
+{
+  const PairGT<Real> q = pair_reverse(p);
+  const Real half = V / 2.0;
+  // one call on both lanes with this lane's end selected (branching on e
+  // would make the warp run the two ends one after the other)
+  const Real pmine = R.p_sigma_pi(e ? j : i, e ? i : j, e ? q : p, half, sink);
+  const Real pother = pair_swap(pmine, pm);
+  const Real pij = e == 0 ? pmine : pother, pji = e == 0 ? pother : pmine;
+  Real val = (pij + pji) / 2.0;
+  const int ti = R.type(i), tj = R.type(j);
+  // pi_rc (REBO.cxx:659-714): the H-C order evaluates as C-H with i and j swapped
+  int ci = i, cj = j;
+  const PairGT<Real>* pc = &p;
+  const PairGT<Real>* qc = &q;
+  if (ti == kH && tj == kC) { ci = j; cj = i; pc = &q; qc = &p; }
+  const int tci = R.type(ci), tcj = R.type(cj);
+  const int fam = (tci == kC && tcj == kC) ? 0 : ((tci == kC && tcj == kH) ? 1 : 2);
+  const Real Nti = R.Nval(ci, cj, *pc, 0);
+  const Real Ntj = R.Nval(cj, ci, *qc, 0);
+  const int me = e == 0 ? i : j;
+  const bool is_ci = me == ci;
+  const Real smine = R.nconj_sum(me, is_ci ? cj : ci);
+  const Real sother = pair_swap(smine, pm);
+  const Real s1 = is_ci ? smine : sother, s2 = is_ci ? sother : smine;
+  Real Nconj = 1.0;
+  Nconj += SQR(s1);
+  Nconj += SQR(s2);
+  Real F[4];
+  t_eval(R.T, fam, Nti, Ntj, Nconj, F, R.status);
+  val += F[0];
+  Real cNti = 0.0, cNtj = 0.0, cNconj = 0.0;
+  if (V != 0.0) {
+    cNti = F[1] * V;
+    cNtj = F[2] * V;
+    cNconj = F[3] * V;
+  }
+  // pi_dh (REBO.cxx:761-814): C-C only, T_ij nonzero only near (2,2,.)
+  if (ti == kC && tj == kC) {
+    Real Tv[4];
+    t_eval(R.T, 3, Nti, Ntj, Nconj, Tv, R.status);
+    if (Tv[0] != 0.0) {
+      const Real ts = R.dh_sum(i, j, p, 0.0, sink);
+      val += Tv[0] * ts;
+      if (V != 0.0) {
+        if (ts != 0.0) {
+          const Real Vt = ts * V;
+          cNti += Tv[1] * Vt;
+          cNtj += Tv[2] * Vt;
+          cNconj += Tv[3] * Vt;
+        }
+        const bool on = sink.pair_on;
+        sink.pair_on = e == 0;
+        R.dh_sum(i, j, p, Tv[0] * V, sink);
+        sink.pair_on = on;
+      }
+    }
+  }
+  if (V != 0.0) {
+    const int oc = is_ci ? cj : ci;  // the other end
+    R.dfthem(me, oc, is_ci ? cNti : cNtj, 0, sink);
+    // REBO::Nconj's gradient (nconj_grad): each end its own half
+    const Real sm = is_ci ? s1 : s2;
+    if (cNconj != 0.0 && sm != 0.0) R.nconj_sum_grad(me, oc, 2.0 * sm * cNconj, sink);
+  }
+  return val;
+}
+
+// REBO of bond slot s of atom lo (partner hi) on a lane pair: lane e
+// writes the record of its end (lo for e = 0, hi for e = 1); lane 0 adds
+// V_R, the bond energy and V_A's pair pieces.  The torsion of the bond is
+// a separate task.
+template <class Real, class TB>
+__device__ void rebo_end_task(const ReboT<Real, TB>& R, int do_rebo, double* rec, int e, int lo, int s, int hi)
+{
+  const auto& B = R.B;
+  const unsigned pm = 3u << ((threadIdx.x & 31) & ~1);
+  const int me = e ? hi : lo;
+  const int nbm = B.nb[me];
+  EndSinkT<Real> sink;
+  sink.me = me;
+  sink.lo = lo;
+  sink.hi = hi;
+  sink.pair_on = true;
+  sink.glo = v3(0, 0, 0);
+  sink.ghi = v3(0, 0, 0);
+  sink.A = rec + 5;
+  sink.W = rec + 5 + 3 * nbm;
+  for (int t = 0; t < 4 * nbm; t++) sink.A[t] = 0.0;  // A and W are contiguous
+  const PairGT<Real> p = pair_from_slot<Real>(B, lo * B.mb + s);
+  double er = 0.0;
+  if (do_rebo) {
+    // REBO::operator() for one bond (REBO.cxx:43-59), as ReboT::bond does
+    // V_R and V_A's pair pieces from lane 0 (lane 1 takes the values only)
+    SinkT<Real> dummy;
+    const Real vav = R.VA(lo, hi, p, 0.0, dummy);
+    Real E = R.VR(lo, hi, p, e == 0 ? 1.0 : 0.0, sink);
+    if (vav != 0.0) {
+      const Real bav = baver_end(R, e, lo, hi, p, vav, sink, pm);
+      E += bav * R.VA(lo, hi, p, e == 0 ? bav : Real(0.0), sink);
+    }
+    er = dbl(E);
+  }
+  // each end's own gradient: its lane's pieces plus the other lane's pair-vector pieces
+  const double ox = __shfl_xor_sync(pm, e ? sink.glo.x : sink.ghi.x, 1);
+  const double oy = __shfl_xor_sync(pm, e ? sink.glo.y : sink.ghi.y, 1);
+  const double oz = __shfl_xor_sync(pm, e ? sink.glo.z : sink.ghi.z, 1);
+  const V3 g = e ? sink.ghi : sink.glo;
+  rec[0] = g.x + ox;
+  rec[1] = g.y + oy;
+  rec[2] = g.z + oz;
+  rec[3] = e ? 0.0 : er;
+  rec[4] = 0.0;
+}
+
+// Torsion of C-C bond slot s of atom lo (partner hi, slot sh in hi's list)
+// into the two ends' torsion records (ETors::operator(), AIREBO_ETors.cxx:32-115).
+template <class Real, class TB>
+__device__ void rebo_tors_task(const ReboT<Real, TB>& R, const TorsParams& TP, double* rlo, double* rhi, int lo,
+                               int s, int hi)
+{
+  const auto& B = R.B;
+  const int na = B.nb[lo], nb = B.nb[hi];
+  PairSinkT<Real> sink;
+  sink.a = lo;
+  sink.b = hi;
+  sink.ga = v3(0, 0, 0);
+  sink.gb = v3(0, 0, 0);
+  sink.Aa = rlo + 5;
+  sink.Wa = rlo + 5 + 3 * na;
+  sink.Ab = rhi + 5;
+  sink.Wb = rhi + 5 + 3 * nb;
+  for (int t = 0; t < 4 * na; t++) sink.Aa[t] = 0.0;
+  for (int t = 0; t < 4 * nb; t++) sink.Ab[t] = 0.0;
+  const PairGT<Real> p = pair_from_slot<Real>(B, lo * B.mb + s);
+  const double et = dbl(etors_bond(R, TP, lo, hi, p, sink));
+  rlo[0] = sink.ga.x;
+  rlo[1] = sink.ga.y;
+  rlo[2] = sink.ga.z;
+  rlo[3] = 0.0;
+  rlo[4] = et;
+  rhi[0] = sink.gb.x;
+  rhi[1] = sink.gb.y;
+  rhi[2] = sink.gb.z;
+  rhi[3] = 0.0;
+  rhi[4] = 0.0;
+}
+
+// Index of slot s among atom a's C-C bond slots (its torsion record).
+__device__ __forceinline__ int cc_index(const BondList& B, int a, int s)
+{
+  int k = 0;
+  for (int t = 0; t < s; t++) k += ((int)B.nco[B.bj[a * B.mb + t]].w == kC);
+  return k;
+}
+
+// REBO by bond ends on lane pairs, torsion by C-C bond: the work items are
+// [0, 2 n0) the ends of the C-C bonds, [2 n0, 2 n0 + ntor) their torsions,
+// then (from an even index) the ends of the other bonds; lanes 2m and 2m+1
+// always hold items t and t^1, the two ends of one bond.
+template <class Real, class TB>
+__global__ void __launch_bounds__(128) k_rebo_split_task(const ReboParams* P, const TB* T, BondList B, TorsParams TP,
+                                                         int do_rebo, int do_tors, BondTasks K, unsigned int* status)
+{
+  pdl_enter();
+  const long n0 = (long)K.ctr[0], n1 = (long)K.ctr[1];
+  const long ntor = do_tors ? n0 : 0;
+  const long base1 = (2 * n0 + ntor + 1) & ~1L;
+  const long total = base1 + 2 * n1;
+  ReboT<Real, TB> R{*P, *T, B, status};
+  // rounds alternate direction: a thread whose round-0 item was heavy (the
+  // queue's front) takes one of the last, lightest items next, or none
+  const long stride = (long)gridDim.x * blockDim.x, t0 = spread_task_index();
+  for (long r = 0; r * stride < total; r++) {
+    const long t = r * stride + ((r & 1) ? stride - 1 - t0 : t0);
+    if (t >= total) continue;  // the same for both lanes of a pair (total is even)
+    const bool cc_end = t < 2 * n0, tors = !cc_end && t < 2 * n0 + ntor;
+    if (!cc_end && !tors && t < base1) continue;  // the padding item (its lane has no partner work)
+    const long b = cc_end ? (t >> 1) : (tors ? t - 2 * n0 : ((t - base1) >> 1));
+    const int q = (cc_end || tors) ? K.q[b] : K.q[K.cap - 1 - b];
+    const int lo = q / B.mb, s = q - lo * B.mb;
+    const int hi = B.bj[q], sh = B.brev[q];
+    const long rl = K.rbase[lo], rh = K.rbase[hi];
+    if (rl < 0 || rh < 0 || sh < 0) continue;  // already flagged (the same for both lanes of a pair)
+    const int rsl = bond_rec_size(B.nb[lo]), rsh = bond_rec_size(B.nb[hi]);
+    if (tors) {
+      rebo_tors_task(R, TP, K.rec + rl + (long)(B.nb[lo] + cc_index(B, lo, s)) * rsl,
+                     K.rec + rh + (long)(B.nb[hi] + cc_index(B, hi, sh)) * rsh, lo, s, hi);
+    } else {
+      const int e = (int)(t & 1);
+      double* rec = e ? K.rec + rh + (long)sh * rsh : K.rec + rl + (long)s * rsl;
+      rebo_end_task(R, do_rebo, rec, e, lo, s, hi);
+    }
+  }
+}
+
 // Per-atom sums of the bond-task records (REBO + torsion) and the special LJ
 // records, a group of G lanes per atom.  Lane l owns elements l, l+G, ... of
 //   [g_own(3), e_rebo, e_tors, g_lj(3), e_lj, A(3 nb), W(nb)]
@@ -345,6 +562,7 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
   const int nb = B.nb[a];
   const int nel = 9 + 4 * nb;
   const long rb = rebo_tasks ? K.rbase[a] : -1;
+  const int nrec = rebo_tasks ? K.nrec[a] : 0;
   const int rs = bond_rec_size(nb);
   int t0 = 0, t1 = 0;
   if (with_lj) {
@@ -373,7 +591,7 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
     if (roff < 0 && loff < 0) continue;
     double acc = roff >= 0 ? 0.0 : *dst;
     if (roff >= 0 && rb >= 0)
-      for (int s = 0; s < nb; s++) acc += K.rec[rb + (long)s * rs + roff];
+      for (int s = 0; s < nrec; s++) acc += K.rec[rb + (long)s * rs + roff];
     if (loff >= 0) {
       int t = t0;
       for (; t + 3 < t1; t += 4) {
@@ -1124,7 +1342,7 @@ struct mdg_ctx {
   int* lj_inr = nullptr;      // [n * LJ list cap] in-range LJ partners of the step, list order
   int* lj_inr_cnt = nullptr;  // [n]
   bool tuned = false;        // the autotuner ran for this system
-  float tune_ms[2] = {0, 0};  // its timings of one force evaluation per task mode
+  float tune_ms[3] = {0, 0, 0};  // its timings of one force evaluation per task mode
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
@@ -1347,7 +1565,7 @@ void free_system(mdg_ctx* c)
   c->h_first.clear();
   c->h_boxes.clear();
   c->h_sys.clear();
-  void* bq[] = {c->bt.q, c->bt.ctr, c->bt.rbase, c->bt.rec};
+  void* bq[] = {c->bt.q, c->bt.ctr, c->bt.rbase, c->bt.nrec, c->bt.rec};
   for (void* p : bq)
     if (p) cudaFree(p);
   std::memset(&c->bt, 0, sizeof(c->bt));
@@ -1621,7 +1839,15 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
   if (tasks) {
     const int ir = rebo ? 1 : 0, it = tors ? 1 : 0;
     const int grid = c->rebo_grid > 0 ? c->rebo_grid : c->rebo_task_blocks;
-    if (f32p && c->bt.pairs) {
+    if (f32p && c->bt.pairs == 2) {
+      auto kern = k_rebo_split_task<f32, ReboTables32>;
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
+                c->d_status);
+    } else if (c->bt.pairs == 2) {
+      auto kern = k_rebo_split_task<double, ReboTables>;
+      LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables, B, c->tp, ir, it, c->bt,
+                c->d_status);
+    } else if (f32p && c->bt.pairs) {
       auto kern = k_rebo_pair_task<f32, ReboTables32>;
       LAUNCH_ON(c, rs, "rebo_tors", kern, grid, kThreads, c->d_rp, c->d_tables32, B, c->tp, ir, it, c->bt,
                 c->d_status);
@@ -2110,13 +2336,15 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
   if (c->prm.potentials & (MDG_POT_REBO | MDG_POT_ETORS) && !(c->prm.potentials & MDG_POT_BRENNER)) {
     BondTasks& K = c->bt;
     K.cap = n * mb;
-    K.pairs = c->prm.task_mode == 2 ? 1 : 0;
+    K.pairs = c->prm.task_mode >= 2 ? c->prm.task_mode - 1 : 0;
+    K.tors = (c->prm.potentials & MDG_POT_ETORS) ? 1 : 0;
     K.rec_cap = (long)n * c->prm.bond_rec_avg;
     K.q = dalloc<int>((size_t)K.cap);
     K.ctr = dalloc<unsigned long long>(4);
     K.rbase = dalloc<long>(n);
+    K.nrec = dalloc<int>(n);
     K.rec = dalloc<double>((size_t)K.rec_cap);
-    if (!K.q || !K.ctr || !K.rbase || !K.rec) return fail(MDG_ERR_CUDA, "cudaMalloc (bond tasks)");
+    if (!K.q || !K.ctr || !K.rbase || !K.nrec || !K.rec) return fail(MDG_ERR_CUDA, "cudaMalloc (bond tasks)");
     CK(cudaMemset(K.ctr, 0, 4 * sizeof(unsigned long long)));
     int dev = 0, sms = 148, per = 0;
     cudaGetDevice(&dev);
@@ -2409,7 +2637,7 @@ static int autotune(mdg_ctx* c)
   // configuration, which never changes results, is still chosen
   if (c->prm.task_mode != 0 && !lj) return MDG_OK;
   const int mode0 = c->prm.task_mode ? c->prm.task_mode - 1 : 0;
-  const int mode1 = c->prm.task_mode ? c->prm.task_mode : 2;
+  const int mode1 = c->prm.task_mode ? c->prm.task_mode : 3;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2805,12 +3033,13 @@ int mdg_set_dependent_launch(mdg_ctx* c, int on)
   return MDG_OK;
 }
 
-int mdg_task_mode(mdg_ctx* c, int* mode, float* ms_directed, float* ms_per_bond)
+int mdg_task_mode(mdg_ctx* c, int* mode, float* ms_directed, float* ms_per_bond, float* ms_split)
 {
   if (!c) return fail(MDG_ERR_ARG, "null context");
-  if (mode) *mode = c->bt.pairs ? 2 : 1;
+  if (mode) *mode = c->bt.pairs + 1;
   if (ms_directed) *ms_directed = c->tune_ms[0];
   if (ms_per_bond) *ms_per_bond = c->tune_ms[1];
+  if (ms_split) *ms_split = c->tune_ms[2];
   return MDG_OK;
 }
 

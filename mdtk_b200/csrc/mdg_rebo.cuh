@@ -145,6 +145,45 @@ struct PairSinkT {
   }
 };
 
+// One end of a bond (lo, hi) evaluated on its own lane: the bond-slot
+// pieces and third-shell coefficients of this end's atom (me) go to its
+// record, the pieces along the pair vector itself to both ends' own
+// gradients (glo, ghi; the two lanes' sums are added at the end).  pair_on
+// off: pair-vector pieces dropped (a term both lanes evaluate whose pair
+// pieces one lane keeps).
+template <class Real>
+struct EndSinkT {
+  static constexpr bool kAdj = false;
+  MDG_HD void par(int, int, double) {}
+  int me, lo, hi;
+  bool pair_on;
+  V3 glo, ghi;
+  double *A, *W;     // this end's record
+  MDG_HD void pair(int p, int q, V3T<Real> v)
+  {
+    if (!pair_on) return;
+    const V3 d = to_d(v);
+    if (p == lo) glo += d;
+    else if (q == lo) glo -= d;
+    if (p == hi) ghi += d;
+    else if (q == hi) ghi -= d;
+  }
+  MDG_HD void cbond(int c, int s, V3T<Real> v)
+  {
+    if (c != me) return;
+    const V3 d = to_d(v);
+    if (me == lo) glo += d;
+    else ghi += d;
+    A[3 * s + 0] -= d.x;
+    A[3 * s + 1] -= d.y;
+    A[3 * s + 2] -= d.z;
+  }
+  MDG_HD void wt(int c, int s, Real w)
+  {
+    if (c == me) W[s] += dbl(w);
+  }
+};
+
 template <class Real, class TB>
 struct ReboT {
   typedef typename Wide<Real>::T Wd;

@@ -348,10 +348,15 @@ MDG_HD void rebo_atom(const ReboT<Real, TB>& R, const TorsParams& TP, int do_reb
 // longest serial chain from all of a carbon's bonds to one bond.
 struct BondTasks {
   int cap;                  // queue capacity (n * mb)
-  int pairs;                // 0: one task per directed slot; 1: one task per bond (slots to higher partners)
+  // 0: one task per directed slot; 1: one task per bond (slots to higher
+  // partners); 2: per bond, the two ends' bond-order terms on a lane pair and
+  // the torsion of each C-C bond as a task of its own
+  int pairs;
+  int tors;                 // torsion on (mode 2 gives C-C bonds a torsion record at each end)
   int* q;                   // slots a*mb+s: C-C bonds from the front, the rest from the back
   unsigned long long* ctr;  // [0] C-C tasks, [1] other tasks, [2] record doubles handed out
   long* rbase;              // [n] first record double of atom a (-1: over capacity, flagged)
+  int* nrec;                // [n] records of atom a: its bond slots, then (mode 2) its C-C torsion records
   double* rec;
   long rec_cap;
 };
