@@ -672,6 +672,12 @@ def _row_impacts(M, local, out):
                "atoms_per_impact": nb, "atom_steps_per_s": nb * sum(iters) / wall,
                "workload": f"C projectile on a {nb - 1}-atom graphite slab (2 layers) to 20 fs, adaptive dt, "
                            "application potential set, one batched context"}
+        # what a persistent fused step could save at most: the floor of a
+        # step's 24 dependent phases as graph launches and as one cooperative
+        # kernel, beside the wall time per step of this batch
+        g_us, c_us = M.launch_floor(local, 24)
+        row["per_step"] = {"wall_us": 1e6 * wall / max(iters), "steps": max(iters),
+                           "launch_floor_graph_us": g_us, "launch_floor_cooperative_us": c_us, "phases": 24}
         app = os.path.join(ROOT, "oracle", "_ref", "mdtrajsim")
         if os.path.exists(app):
             rd = os.path.join(tmp, "ref")
@@ -811,10 +817,10 @@ STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
 # on one GPU), keyed by the REBO work split the timed step ran (the
 # autotuner's choice: "per bond" or "directed"); None when not captured.
 TRAFFIC_PER_LAUNCH = {
-    ("rebo_tors", "per bond"): 10.95e6, ("rebo_tors", "directed"): 22.83e6,
-    ("lj_special", "per bond"): 25.68e6, ("lj_special", "directed"): 22.89e6,
-    ("lj_plain", "per bond"): 22.89e6, ("lj_plain", "directed"): 22.89e6,
-    ("lj_filter", "per bond"): 36.64e6, ("lj_filter", "directed"): 36.64e6,
+    ("rebo_tors", "per bond"): 10.91e6, ("rebo_tors", "directed"): 22.83e6,
+    ("lj_special", "per bond"): 25.76e6, ("lj_special", "directed"): 22.89e6,
+    ("lj_plain", "per bond"): 22.84e6, ("lj_plain", "directed"): 22.84e6,
+    ("lj_filter", "per bond"): 36.36e6, ("lj_filter", "directed"): 36.36e6,
 }
 
 

@@ -201,6 +201,15 @@ int mdg_profile_read(mdg_ctx* ctx, int max, char* names, double* ms, int64_t* co
  * the bond-order kernels.  No reference counterpart. */
 int mdg_pipe_peak(int device, int fp32, double* tflops);
 
+/* The floor of one step of `phases` dependent phases that do no work, on
+ * `device`, two ways: a CUDA graph of `phases` empty kernels, each a
+ * programmatic dependent launch (how mdg_run's steps are launched), and one
+ * cooperative kernel with a grid-wide barrier between its phases (a
+ * persistent fused step); both over two blocks per SM, microseconds per step
+ * (best of three 200-step samples).  A diagnostic with no reference
+ * counterpart: it bounds what fusing a step's kernels could save. */
+int mdg_launch_floor(int device, int phases, double* graph_us, double* coop_us);
+
 /* ---- Parameters and the adjoint ----
  * The adjoint differentiates a velocity-Verlet trajectory (the step of
  * mdg_run) with respect to the initial positions and velocities and to the

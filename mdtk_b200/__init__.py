@@ -125,6 +125,7 @@ def lib():
         L.mdg_profile_read.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_int)]
         L.mdg_pipe_peak.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.mdg_launch_floor.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
         L.mdg_debug_brenner_tables.argtypes = [ctypes.c_int, dp, ctypes.c_int64]
         L.mdg_debug_brenner_tables.restype = ctypes.c_int64
         L.mdg_debug_spline.argtypes = [ctypes.c_int] * 4 + [dp, dp]
@@ -182,6 +183,15 @@ def pipe_peak(device: int = 0, fp32: bool = False) -> float:
     out = np.zeros(1)
     _check(lib().mdg_pipe_peak(device, 1 if fp32 else 0, _dp(out)))
     return float(out[0])
+
+
+def launch_floor(device: int = 0, phases: int = 22):
+    """(graph_us, coop_us): per-step floor of `phases` empty dependent phases
+    as a graph of dependent launches and as one cooperative kernel."""
+    g = np.zeros(1)
+    c = np.zeros(1)
+    _check(lib().mdg_launch_floor(device, phases, _dp(g), _dp(c)))
+    return float(g[0]), float(c[0])
 
 
 def debug_brenner_tables(set_: int) -> np.ndarray:

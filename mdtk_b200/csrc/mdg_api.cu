@@ -6,6 +6,7 @@
 //   gather (deterministic per-atom force sum) -> integration / energy.
 // All launches go to one stream; list rebuilds are decided on the device, so
 // a device-resident MD run needs no host round trip per step.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -3165,6 +3166,86 @@ int mdg_pipe_peak(int device, int fp32, double* tflops)
   cudaFree(buf);
   CK(cudaGetLastError());
   *tflops = best;
+  return MDG_OK;
+}
+
+// The floor of a step of `phases` dependent phases with no work in them, two
+// ways: phases empty kernels of a graph, each a programmatic dependent launch
+// (how the step runs), and one cooperative kernel with a grid-wide barrier
+// between phases (a persistent fused step).  Both over two blocks per SM.
+__global__ void k_floor_phase()
+{
+  pdl_enter();
+}
+
+__global__ void k_floor_coop(int phases)
+{
+  cooperative_groups::grid_group g = cooperative_groups::this_grid();
+  for (int p = 0; p < phases; p++) g.sync();
+}
+
+int mdg_launch_floor(int device, int phases, double* graph_us, double* coop_us)
+{
+  if (!graph_us || !coop_us || phases < 1 || phases > 1000) return fail(MDG_ERR_ARG, "bad argument");
+  CK(cudaSetDevice(device));
+  int sms = 0, coop = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  if (!coop) return fail(MDG_ERR_CUDA, "no cooperative launch on this device");
+  const int blocks = 2 * sms, threads = 128, reps = 200;
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  // the graph of dependent launches
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = st;
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  for (int p = 0; p < phases; p++) cudaLaunchKernelEx(&cfg, k_floor_phase);
+  cudaError_t ce = cudaStreamEndCapture(st, &g);
+  if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ge, g, 0);
+  if (g) cudaGraphDestroy(g);
+  double best_graph = 1e30, best_coop = 1e30;
+  for (int rep = 0; rep < 3 && ce == cudaSuccess; rep++) {
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && ce == cudaSuccess; r++) ce = cudaGraphLaunch(ge, st);
+    cudaEventRecord(e1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    best_graph = std::min(best_graph, 1e3 * ms / reps);
+  }
+  if (ge) cudaGraphExecDestroy(ge);
+  // the cooperative kernel, launched back to back
+  int ph = phases;
+  void* args[] = {&ph};
+  for (int rep = 0; rep < 3 && ce == cudaSuccess; rep++) {
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && ce == cudaSuccess; r++)
+      ce = cudaLaunchCooperativeKernel((const void*)k_floor_coop, dim3(blocks), dim3(threads), args, 0, st);
+    cudaEventRecord(e1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    best_coop = std::min(best_coop, 1e3 * ms / reps);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("launch floor: ") + cudaGetErrorString(ce));
+  *graph_us = best_graph;
+  *coop_us = best_coop;
   return MDG_OK;
 }
 
