@@ -1,6 +1,6 @@
 // Per-atom work items of one force evaluation and one velocity-Verlet step.
 // Each function is the body of one thread of the matching kernel in
-// mdg_kernels.cu; thread a only ever writes atom a's own outputs.
+// mdg_api.cu; thread a only ever writes atom a's own outputs.
 #pragma once
 
 #include "mdg_common.cuh"
