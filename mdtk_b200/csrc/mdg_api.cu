@@ -445,11 +445,13 @@ __device__ void rebo_end_task(const ReboT<Real, TB>& R, int do_rebo, double* rec
     // REBO::operator() for one bond (REBO.cxx:43-59), as ReboT::bond does
     // V_R and V_A's pair pieces from lane 0 (lane 1 takes the values only)
     SinkT<Real> dummy;
-    const Real vav = R.VA(lo, hi, p, 0.0, dummy);
+    double va_val = 0.0, va_der = 0.0;
+    if (p.f != 0.0) R.VA_terms(lo, hi, p, va_val, va_der);
+    const Real vav = R.VA_from(lo, hi, p, va_val, va_der, 0.0, dummy);
     Real E = R.VR(lo, hi, p, e == 0 ? 1.0 : 0.0, sink);
     if (vav != 0.0) {
       const Real bav = baver_end(R, e, lo, hi, p, vav, sink, pm);
-      E += bav * R.VA(lo, hi, p, e == 0 ? bav : Real(0.0), sink);
+      E += bav * R.VA_from(lo, hi, p, va_val, va_der, e == 0 ? bav : Real(0.0), sink);
     }
     er = dbl(E);
   }

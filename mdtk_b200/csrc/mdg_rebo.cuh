@@ -235,10 +235,12 @@ struct ReboT {
 
   // ---- angular term G (REBO::G, REBO.cxx:280-326) ----
   // Returns G; with V != 0 routes V * dG to the pair c-o, the bond c-k and
-  // (carbon centre) through N_co to c's switching bonds.
+  // (carbon centre) through N_co to c's switching bonds.  Sp = S'(N_co) and
+  // SpDer = dS'(N_co) of a carbon centre are the same for every k, so the
+  // callers evaluate them once per pass (SpDer only when V may be nonzero).
   template <class S>
-  MDG_HD Real G(int c, int o, const PairGT<Real>& p, int s_k, V3T<Real> bk_rv, Real bk_r, V3T<Real> bk_u, Real Nco,
-                  Real V, S& sink) const
+  MDG_HD Real G(int c, int o, const PairGT<Real>& p, int s_k, V3T<Real> bk_rv, Real bk_r, V3T<Real> bk_u, Real Sp,
+                  Real SpDer, Real V, S& sink) const
   {
     Real e1 = dot(p.rv, bk_rv);
     Real e2 = p.r * bk_r;
@@ -248,11 +250,9 @@ struct ReboT {
     if (cost > 1.0) cost = 1.0;
     Real Vc = 0.0, val;
     if (type(c) == kC) {
-      Real Sp = Sprime(Nco, P.Ntot[0], P.Ntot[1]);
       Real g1 = g_eval(T.G[0], cost, 0);
       Real g2 = g_eval(T.G[1], cost, 0);
       if (V != 0.0) {
-        Real SpDer = dSprime(Nco, P.Ntot[0], P.Ntot[1]);
         Real g1d = g_eval(T.G[0], cost, 1);
         Real g2d = g_eval(T.G[1], cost, 1);
         if (g2d != 0.0 || g1d != 0.0) Vc = g2d * V + g1d * Sp * V + (-g2d * Sp * V);
@@ -292,6 +292,7 @@ struct ReboT {
     SinkT<Real> dummy;
     Real Dij = 1.0;
     Real Nco = Nval(c, o, p, 0);
+    const Real Sp = type(c) == kC ? Sprime(Nco, P.Ntot[0], P.Ntot[1]) : Real(0.0);
     const int nb = B.nb[c];
     for (int s = 0; s < nb; s++) {
       const int q = c * B.mb + s;
@@ -301,7 +302,7 @@ struct ReboT {
       const auto u = B.bu[q];
       Real ex = expterm(c, o, p, k, rv.w);
       if (ex != 0.0) {
-        Real gv = G(c, o, p, s, xyz<Real>(rv), rv.w, xyz<Real>(u), Nco, 0.0, dummy);
+        Real gv = G(c, o, p, s, xyz<Real>(rv), rv.w, xyz<Real>(u), Sp, Real(0.0), 0.0, dummy);
         Dij += gv * u.w * ex;
       }
     }
@@ -314,6 +315,9 @@ struct ReboT {
   MDG_HD void D_grad(int c, int o, const PairGT<Real>& p, Real V, S& sink) const
   {
     Real Nco = Nval(c, o, p, 0);
+    const bool ccen = type(c) == kC;
+    const Real Sp = ccen ? Sprime(Nco, P.Ntot[0], P.Ntot[1]) : Real(0.0);
+    const Real SpDer = ccen ? dSprime(Nco, P.Ntot[0], P.Ntot[1]) : Real(0.0);
     const int nb = B.nb[c];
     const bool hcen = type(c) == kH;
     for (int s = 0; s < nb; s++) {
@@ -325,10 +329,9 @@ struct ReboT {
       V3T<Real> brv = xyz<Real>(rv), bu3 = xyz<Real>(u);
       Real ex = expterm(c, o, p, k, rv.w);
       if (ex == 0.0) continue;
-      SinkT<Real> dummy;
-      Real gv = G(c, o, p, s, brv, rv.w, bu3, Nco, 0.0, dummy);
+      // one evaluation: the value G returns does not depend on the seed
       Real fv = u.w;
-      G(c, o, p, s, brv, rv.w, bu3, Nco, fv * ex * V, sink);
+      Real gv = G(c, o, p, s, brv, rv.w, bu3, Sp, SpDer, fv * ex * V, sink);
       Real df = B.bd[q].x;
       if (df != 0.0) sink.cbond(c, s, bu3 * ((gv * ex * V) * df));
       if (hcen) {
@@ -589,23 +592,36 @@ struct ReboT {
     }
     return Real(dbl(f) * val);
   }
-  template <class S>
-  MDG_HD Real VA(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
+  // V_A's sum of exponentials and its radial derivative, evaluated once per
+  // bond: the value seeds b-bar and the gradient pass reuses both.
+  MDG_HD void VA_terms(int i, int j, const PairGT<Real>& p, Wd& val, Wd& der) const
   {
-    const Real f = p.f;
-    if (f == 0.0) return 0.0;
     int ti = type(i), tj = type(j);
     const Wd r = p.rd;
     const Wd t1 = P.B[0][ti][tj] * exp(-P.beta[0][ti][tj] * r);
     const Wd t2 = P.B[1][ti][tj] * exp(-P.beta[1][ti][tj] * r);
     const Wd t3 = P.B[2][ti][tj] * exp(-P.beta[2][ti][tj] * r);
-    const Wd val = t1 + t2 + t3;
+    val = t1 + t2 + t3;
+    der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
+  }
+  template <class S>
+  MDG_HD Real VA_from(int i, int j, const PairGT<Real>& p, Wd val, Wd der, Real V, S& sink) const
+  {
+    const Real f = p.f;
+    if (f == 0.0) return 0.0;
     if (V != 0.0) {
-      const Wd der = (-P.beta[0][ti][tj]) * t1 + (-P.beta[1][ti][tj]) * t2 + (-P.beta[2][ti][tj]) * t3;
       sink.pair(i, j, p.u * Real(-der * dbl(f) * dbl(V)));
       if (p.df != 0.0) sink.pair(i, j, p.u * Real((-val * dbl(V)) * dbl(p.df)));
     }
     return Real(-dbl(f) * val);
+  }
+  template <class S>
+  MDG_HD Real VA(int i, int j, const PairGT<Real>& p, Real V, S& sink) const
+  {
+    if (p.f == 0.0) return 0.0;
+    Wd val, der;
+    VA_terms(i, j, p, val, der);
+    return VA_from(i, j, p, val, der, V, sink);
   }
 
   // One REBO bond i < j (REBO::operator(), REBO.cxx:43-59): returns its energy.
@@ -613,12 +629,14 @@ struct ReboT {
   MDG_HD Real bond(int i, int j, const PairGT<Real>& p, S& sink) const
   {
     SinkT<Real> dummy;
-    Real vav = VA(i, j, p, 0.0, dummy);
+    Wd va_val = 0.0, va_der = 0.0;
+    if (p.f != 0.0) VA_terms(i, j, p, va_val, va_der);
+    Real vav = VA_from(i, j, p, va_val, va_der, 0.0, dummy);
     Real E = VR(i, j, p, 1.0, sink);
     Real bav = 0.0;
     if (vav != 0.0) {
       bav = baver(i, j, p, vav, sink);
-      E += bav * VA(i, j, p, bav, sink);
+      E += bav * VA_from(i, j, p, va_val, va_der, bav, sink);
     }
     if constexpr (S::kAdj) {
       // derivatives of this bond's energy by the C-C pair parameters: V_R is
