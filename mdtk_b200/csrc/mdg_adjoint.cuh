@@ -162,7 +162,8 @@ __global__ void k_adj_lj_plain(LJParams P, CijTableT<dual> T, State S, NList L, 
   dual e = 0.0;
   const int cnt = L.cnt[a];
   const int* lst = L.list + (long)a * L.cap;
-  for (int s = 0; s < cnt; s++) lj_plain_pair<dual>(P, T, S, a, lst[s], xa, ta, sk, e, tan);
+  const unsigned long long amask = T.mask[a];
+  for (int s = 0; s < cnt; s++) lj_plain_pair<dual>(P, T, S, a, lst[s], xa, ta, amask, sk, e, tan);
   O.glj[a] = make_dual4(sk.g.x, sk.g.y, sk.g.z, 0.0);
   O.e_lj[a] = e;
 }

@@ -698,6 +698,7 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
   const int cnt = live ? inr_cnt[a] : 0;
+  const unsigned long long amask = T.mask[a];
   const int* q = inr + (long)a * L.cap;
   const unsigned gmask = (kLjGroup == 32) ? 0xffffffffu : (((1u << kLjGroup) - 1u) << gbase);
   const unsigned below = ((1u << lane) - 1u) & gmask;
@@ -714,7 +715,7 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
     int kind = 0, b = -1;
     if (base + gl < cnt) {
       b = q[base + gl];
-      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, sk, e);
+      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, amask, sk, e);
     }
     const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
     if (kind == 2) {

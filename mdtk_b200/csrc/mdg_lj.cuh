@@ -470,12 +470,12 @@ MDG_HD PairGT<Real> pair_geom(V3 rv, double r, const double4* tan, int lo, int h
 }
 
 // Classifies one LJ pair seen from atom a: returns 0 (skip), 1 (plain: C = 1
-// and S(t_r) = 0, so E = VLJ) or 2 (special).  For plain pairs adds the own
+// and S(t_r) = 0, so E = VLJ) or 2 (special); amask = T.mask[a].  For plain pairs adds the own
 // gradient and, at the lower end, the energy.  The classification is made in
 // double on every path (the adjoint path's pairs are the FP64 path's).
 template <class Real, class S, class W>
 MDG_HD int lj_plain_pair(const LJParams& P, const CijTableT<W>& T, const State& St, int a, int b, V3 xa, int ta,
-                         S& sink, W& e, const double4* tan = nullptr)
+                         unsigned long long amask, S& sink, W& e, const double4* tan = nullptr)
 {
   const double4 pb = St.pos[b];
   const int tb = (int)pb.w;
@@ -487,7 +487,11 @@ MDG_HD int lj_plain_pair(const LJParams& P, const CijTableT<W>& T, const State& 
   const double d2 = norm2(rv);
   const double R1 = P.R[ta][tb][0], R2 = P.R[ta][tb][1];
   if (d2 > R2 * R2) return 0;
-  const int ei = cij_find(T, lo, hi);
+  // amask is a's own connectivity mask (T.mask[a]).  Reachability within
+  // three bonds is symmetric, so a clear bit for b in it proves w = 0 without
+  // the lower-index atom's table, which may be b's: its lookup is only made
+  // for the pairs the mask admits.
+  const int ei = ((amask >> (b & 63)) & 1ull) ? cij_find(T, lo, hi) : -1;
   const double w = ei >= 0 ? val(T.w[(long)lo * T.cap + ei]) : 0.0;
   const double C = 1 - w;
   if (!(C > 0.0)) return 0;
