@@ -105,3 +105,39 @@ def test_full_size_diamond_512000():
     assert np.isfinite(e) and _net_force_ok(g)
     _, _, g32 = _ctx(s, precision=M.PREC_FP32_MIXED).compute()
     assert np.linalg.norm(g32 - g) <= 1e-5 * np.linalg.norm(g)
+
+
+def test_step_host_multi_step_calls_equal_device_runs():
+    """mdg_step_host with k steps per call from a host-held state gives the
+    state and energies of k device-resident steps, bit for bit."""
+    s = B.ethane_liquid(60, seed=91, min_dist=1.6, jitter=0.4)
+    a = M.Context(potentials=M.POT_AIREBO, task_mode=2)
+    a.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    b = M.Context(potentials=M.POT_AIREBO, task_mode=2)
+    b.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    pos, vel, _ = b.get_state()
+    ep_h, et_h = [], []
+    for _ in range(3):
+        ep, et = b.step_host(10, 0.25, pos, vel)
+        ep_h.append(ep)
+        et_h.append(et)
+    ep_d, et_d = a.run(30, 0.25)
+    pa, va, _ = a.get_state()
+    assert np.array_equal(np.concatenate(ep_h), ep_d) and np.array_equal(np.concatenate(et_h), et_d)
+    assert np.array_equal(pos, pa) and np.array_equal(vel, va)
+
+
+def test_nl_update_reports_rebuilds():
+    s = B.ethane_liquid(60, seed=92, min_dist=1.6, jitter=0.4)
+    c = M.Context(potentials=M.POT_AIREBO)
+    c.set_system(s["z"], s["pos"], s["vel"], s["box"], s["pbc"], s["fixed"])
+    assert list(c.nl_update(force=True)[:2]) == [1, 1]
+    assert list(c.nl_update()[:2]) == [0, 0]       # nothing moved since
+    pos, vel, _ = c.get_state()
+    c.set_state(pos + 1.3, vel)                   # every atom 2.25 A: past both triggers
+    assert list(c.nl_update()[:2]) == [1, 1]
+
+
+def test_launch_floor_diagnostic():
+    g, c = M.launch_floor(0, 24)
+    assert 0.0 < g < 1e4 and 0.0 < c < 1e4
