@@ -807,20 +807,19 @@ def precision_study(args, local, rank):
 # workload (ethane liquid, 43,688 atoms, step-0 state, seed 1), from the
 # op-counting restatement: `python oracle/opcount.py` (add/mul 1, div/sqrt 4,
 # exp/cos 12, pow 24; energy + gradient = 3 x energy).  rebo_tors = REBO +
-# torsion terms; lj_plain = the LJ pair terms (V_LJ, switches, C_ij path
-# products); lj_special = the b*_ij bond orders of close non-bonded pairs.
-FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_plain": 5151.5, "lj_special": 5205.5}
+# torsion terms; lj_pairs = the plain LJ pair terms (V_LJ, switches, C_ij
+# path products); lj_special = the b*_ij bond orders of close non-bonded pairs.
+FLOPS_PER_ATOM = {"rebo_tors": 2541.0 + 504.0, "lj_pairs": 5151.5, "lj_special": 5205.5}
 STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
 # DRAM read + write bytes per launch of each kernel on this workload, from
 # one ncu capture of the kernel (profiles/, captured with
 #   ncu --set full --clock-control none -k regex:<kernel> -c <few> ...
 # on one GPU), keyed by the REBO work split the timed step ran (the
-# autotuner's choice: "per bond" or "directed"); None when not captured.
+# autotuner's choice: "per bond", "directed" or "lane pairs"); None when not
+# captured.
 TRAFFIC_PER_LAUNCH = {
     ("rebo_tors", "per bond"): 10.91e6, ("rebo_tors", "directed"): 22.83e6,
-    ("lj_special", "per bond"): 25.76e6, ("lj_special", "directed"): 22.89e6,
-    ("lj_plain", "per bond"): 22.84e6, ("lj_plain", "directed"): 22.84e6,
-    ("lj_filter", "per bond"): 36.36e6, ("lj_filter", "directed"): 36.36e6,
+    ("rebo_tors", "lane pairs"): 13.6e6,
 }
 
 

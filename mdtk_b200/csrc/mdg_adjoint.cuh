@@ -173,7 +173,7 @@ __global__ void k_adj_lj_special(const ReboParams* P, const ReboTables* Tb, LJPa
                                  unsigned int* status)
 {
   pdl_enter();
-  const int total = min(Tk.off[S.n], Tk.task_cap);
+  const int total = spc_total(Tk);
   ReboT<dual, ReboTables> R{*P, *Tb, B, status};
   LJT<dual, ReboTables> X{LP, R, T};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
@@ -403,6 +403,7 @@ int adj_dual_pass(mdg_ctx* c, int transpose = 1)
     Tk.roff = P.roff;
     Tk.flat = P.flat;
     Tk.trec = P.trec;
+    Tk.ctr = P.ctr;
     Tk.rec = w->trec;
     Tk.mid = w->tmid;
     Tk.midc = w->tmidc;

@@ -568,10 +568,7 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
   const int nrec = rebo_tasks ? K.nrec[a] : 0;
   const int rs = bond_rec_size(nb);
   int t0 = 0, t1 = 0;
-  if (with_lj) {
-    t0 = Tk.off[a];
-    t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
-  }
+  if (with_lj) spc_range(Tk, a, t0, t1);
   // the LJ pass over REBO sums already in place: an atom without special
   // pair records keeps every element as it is
   if (!rebo_tasks && with_lj && t1 <= t0) return;
@@ -629,20 +626,26 @@ __global__ void k_brenner(const BrennerParams* P, const BrennerTables* T, BondLi
 
 constexpr int kCijLocal = 128;  // per-thread connectivity table capacity
 
-__global__ void k_cij(BondList B, CijTable T, unsigned int* status)
+// Also zeroes the special-pair counters that the special-pair finder after it
+// hands ranges out of.
+__global__ void k_cij(BondList B, CijTable T, unsigned long long* spc_ctr, unsigned int* status)
 {
   pdl_enter();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0 && spc_ctr) spc_ctr[0] = spc_ctr[kCtrStride] = spc_ctr[2 * kCtrStride] = 0ull;
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
 
 // LJ pairs inside their cutoff, one warp per atom: the atom's LJ list is
 // read 32 entries at a time and the entries within the pair's cutoff R2 are
-// appended, in list order, to the atom's in-range list (about a quarter of
-// the list).  It needs only positions and the list, so it runs concurrently
+// appended, in list order, to the atom's far list (front of its in-range
+// row, count far_cnt[a]) or, inside the S(t_r) window, its close list (back of
+// the row, growing down; count close_cnt[a]); together about a quarter of
+// the list.  It needs only positions and the list, so it runs concurrently
 // with the bond and connectivity kernels; its few registers let many warps
 // hide the position gathers.
-__global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NList L, int* inr, int* inr_cnt)
+__global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NList L, int* inr, int* far_cnt,
+                                                        int* close_cnt)
 {
   pdl_enter();
   const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -651,78 +654,148 @@ __global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NLi
   const double4 pa = S.pos[a];
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
-  const Box& box = box_of(S, a);
+  const Box box = box_of(S, a);
   const int cnt = L.cnt[a];
   const int* lst = L.list + (long)a * L.cap;
   int* out = inr + (long)a * L.cap;
+  int* top = out + L.cap - 1;
   const unsigned below = (1u << lane) - 1u;
-  int k = 0;
+  int kf = 0, kc = 0;
   for (int base = 0; base < cnt; base += 32) {
     const int s = base + lane;
-    bool in = false;
+    bool in = false, close = false;
     int b = -1;
     if (s < cnt) {
       b = lst[s];
       const double4 pb = S.pos[b];
-      const double R2 = P.R[ta][(int)pb.w][1];
+      const int tb = (int)pb.w;
+      const double R2 = P.R[ta][tb][1];
       const V3 rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
-      in = !(norm2(rv) > R2 * R2);
+      const double d2 = norm2(rv);
+      in = !(d2 > R2 * R2);
+      close = in && lj_close(P, ta, tb, d2);  // lj_class's test, on the same d2
     }
-    const unsigned m = __ballot_sync(0xffffffffu, in);
-    if (in) out[k + __popc(m & below)] = b;
-    k += __popc(m);
+    const unsigned mf = __ballot_sync(0xffffffffu, in && !close);
+    const unsigned mc = __ballot_sync(0xffffffffu, close);
+    if (in && !close) out[kf + __popc(mf & below)] = b;
+    if (close) top[-(kc + __popc(mc & below))] = b;
+    kf += __popc(mf);
+    kc += __popc(mc);
   }
-  if (lane == 0) inr_cnt[a] = k;
+  if (lane == 0) {
+    far_cnt[a] = kf;
+    close_cnt[a] = kc;
+  }
 }
 
-// Plain LJ pairs, one warp per atom over its in-range list, 32 pairs per
-// round with every lane busy (the last round excepted).  Pairs that need
-// b*_ij or a connectivity gradient are compacted, in list order, into the
-// atom's special list.
-constexpr int kLjGroup = 16;  // lanes per atom in the plain LJ pair kernel (a divisor of 32)
+// Exclusive offsets of this thread's v[0..2] within ranges handed out to the
+// block by one atomicAdd per counter (ctr[0], ctr[kCtrStride],
+// ctr[2 kCtrStride]).  Every thread of the block (blockDim.x == NT) calls it.
+template <int NT>
+__device__ void block_alloc3(const unsigned long long v[3], unsigned long long* ctr, unsigned long long out[3])
+{
+  __shared__ unsigned long long ws[3][NT / 32];
+  __shared__ unsigned long long base[3];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long x[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    x[k] = v[k];
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(0xffffffffu, x[k], o);
+      if (lane >= o) x[k] += t;
+    }
+    if (lane == 31) ws[k][wid] = x[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int k = threadIdx.x;
+    unsigned long long run = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      const unsigned long long t = ws[k][w];
+      ws[k][w] = run;
+      run += t;
+    }
+    base[k] = run ? atomicAdd(ctr + k * kCtrStride, run) : 0ull;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 3; k++) out[k] = base[k] + ws[k][wid] + x[k] - v[k];
+}
+
+// The LJ pairs of each atom, kLjGroup lanes per atom: the plain pairs of its
+// far list are evaluated here, and its special pairs (lj_class kind 2: the
+// close pairs with C > 0, then the far pairs with 0 < w < 1, each in list
+// order) are made into tasks for the special-pair kernels.  The filter has
+// already split the in-range pairs by the S(t_r) window, so a close pair
+// needs only its w (no positions).  w is looked up in the atom's own
+// connectivity table, and only for the pairs its mask admits.  The atom's
+// tasks, records and (with `pairs`) the work items of the pairs it owns as
+// the lower index take ranges handed out per block.
+constexpr int kLjGroup = 16;     // lanes per atom (a divisor of 32): ~30 in-range partners
+constexpr int kLjThreads = 128;  // 8 atoms per block
+constexpr int kReduceLanes = 8;
 template <class Real>
-__global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, State S, NList L, const int* inr,
-                                                       const int* inr_cnt, const int* nbonds, ForceOut O,
-                                                       SpecialTasks Tk, unsigned int* status)
+__global__ void __launch_bounds__(kLjThreads, 7) k_lj_pairs(LJParams P, CijTable T, State S, int lcap, const int* inr,
+                                                         const int* far_cnt, const int* close_cnt,
+                                                         const int* nbonds, ForceOut O, SpecialTasks Tk, int pairs,
+                                                         unsigned int* status)
 {
   pdl_enter();
-  if (blockIdx.x == 0 && threadIdx.x == 0 && Tk.wcnt) *Tk.wcnt = 0;  // work list of this step
-  // kLjGroup lanes per atom: an atom has ~30 in-range partners, so a group
-  // of 16 keeps more lanes busy than a whole warp would
   const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLjGroup;
   const int lane = threadIdx.x & 31, gl = lane % kLjGroup, gbase = lane - gl;
-  const bool live = gid < S.n;
-  if (__all_sync(0xffffffffu, !live)) return;  // whole warps
+  const bool live = gid < S.n;  // every thread stays for the block's allocation
   const int a = live ? gid : S.n - 1;
   const double4 pa = S.pos[a];
   const V3 xa = v3(pa.x, pa.y, pa.z);
   const int ta = (int)pa.w;
-  const int cnt = live ? inr_cnt[a] : 0;
+  const int nc = live ? close_cnt[a] : 0;
+  const int nf = live ? far_cnt[a] : 0;
   const unsigned long long amask = T.mask[a];
-  const int* q = inr + (long)a * L.cap;
+  const int* row = inr + (long)a * lcap;
+  int* part = Tk.part + (long)a * Tk.cap;
   const unsigned gmask = (kLjGroup == 32) ? 0xffffffffu : (((1u << kLjGroup) - 1u) << gbase);
   const unsigned below = ((1u << lane) - 1u) & gmask;
+  int nsp = 0, nhi = 0;
+  // appends this lane's b (when special) to the atom's special list
+  auto note = [&](bool special, int b) {
+    const unsigned m = __ballot_sync(0xffffffffu, special);
+    const int pos = nsp + __popc(m & below);
+    const bool keep = special && pos < Tk.cap;
+    if (keep) part[pos] = b;
+    nhi += __popc(__ballot_sync(0xffffffffu, keep && b > a) & gmask);
+    nsp += __popc(m & gmask);
+  };
+  // the warp's longest lists bound its loops
+  int wc = nc, wf = nf;
+  for (int o = 16; o > 0; o >>= 1) {
+    wc = max(wc, __shfl_xor_sync(0xffffffffu, wc, o));
+    wf = max(wf, __shfl_xor_sync(0xffffffffu, wf, o));
+  }
+  for (int base = 0; base < wc; base += kLjGroup) {
+    const int s = base + gl;
+    int b = -1;
+    bool sp = false;
+    if (s < nc) {
+      b = row[lcap - 1 - s];
+      sp = lj_kind(lj_w_own(T, a, b, amask), true) == 2;
+    }
+    note(sp, b);
+  }
   SinkT<Real> sk;
   sk.a = a;
   sk.g = v3(0, 0, 0);
   sk.A = nullptr;
   sk.W = nullptr;
   double e = 0.0;
-  int nsp = 0;
-  int wcnt = cnt;  // the warp's longest list bounds its loop
-  for (int o = 16; o > 0; o >>= 1) wcnt = max(wcnt, __shfl_xor_sync(0xffffffffu, wcnt, o));
-  for (int base = 0; base < wcnt; base += kLjGroup) {
-    int kind = 0, b = -1;
-    if (base + gl < cnt) {
-      b = q[base + gl];
-      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, amask, sk, e);
+  for (int base = 0; base < wf; base += kLjGroup) {
+    const int s = base + gl;
+    int b = -1, kind = 0;
+    if (s < nf) {
+      b = row[s];
+      kind = lj_plain_pair<Real>(P, T, S, a, b, xa, ta, amask, sk, e, nullptr, true);
     }
-    const unsigned m = __ballot_sync(0xffffffffu, kind == 2);
-    if (kind == 2) {
-      const int pos = nsp + __popc(m & below);
-      if (pos < Tk.cap) Tk.part[(long)a * Tk.cap + pos] = b;
-    }
-    nsp += __popc(m & gmask);
+    note(kind == 2, b);
   }
   double gx = sk.g.x, gy = sk.g.y, gz = sk.g.z;
   for (int o = kLjGroup / 2; o > 0; o >>= 1) {
@@ -731,139 +804,49 @@ __global__ void __launch_bounds__(kThreads) k_lj_plain(LJParams P, CijTable T, S
     gz += __shfl_xor_sync(0xffffffffu, gz, o);
     e += __shfl_xor_sync(0xffffffffu, e, o);
   }
-  if (live && gl == 0) {
+  if (nsp > Tk.cap) {
+    if (live && gl == 0) atomicOr(status, ST_RECORD_OVERFLOW);
+    nsp = Tk.cap;
+  }
+  const int rs = rec_size(live ? nbonds[a] : 0);
+  const bool lead = live && gl == 0;
+  unsigned long long v[3] = {lead && pairs ? (unsigned long long)nhi : 0ull, lead ? (unsigned long long)nsp : 0ull,
+                             lead ? (unsigned long long)nsp * rs : 0ull};
+  unsigned long long r[3];
+  block_alloc3<kLjThreads>(v, Tk.ctr, r);  // also orders this block's part[] writes before the reads below
+  // every lane of the group holds its leader's offsets
+  const long wb = (long)__shfl_sync(0xffffffffu, r[0], gbase);
+  const long o = (long)__shfl_sync(0xffffffffu, r[1], gbase);
+  const long ro = (long)__shfl_sync(0xffffffffu, r[2], gbase);
+  if (!live) return;
+  if (gl == 0) {
     O.glj[a] = make_double4(gx, gy, gz, 0.0);
     O.e_lj[a] = e;
-    if (nsp > Tk.cap) {
-      atomicOr(status, ST_RECORD_OVERFLOW);
-      nsp = Tk.cap;
-    }
     Tk.cnt[a] = nsp;
-    Tk.rsz[a] = nsp * rec_size(nbonds[a]);
+    Tk.rsz[a] = nsp * rs;
+    Tk.roff[a] = ro;
+    if (o + nsp > Tk.task_cap) atomicOr(status, ST_RECORD_OVERFLOW);
+    Tk.off[a] = o < Tk.task_cap ? (int)o : Tk.task_cap;
   }
-}
-
-// Tiled exclusive scan of two int arrays at once (blockIdx.y picks the
-// array) in one launch: each tile block scans its tile into part (offsets
-// within the tile) and stores the tile's sum; the last block to finish (a
-// counter, no waiting) turns the tile sums into tile offsets and writes the
-// totals out[y][n].  The element offset is part[y][i] + tile[y][i / kScanTile],
-// added by the compaction kernel that follows.
-struct ScanPair {
-  const int* in[2];
-  int* out[2];    // [n + 1]: only out[y][n] (the total) is written here
-  int* part[2];   // [n] offsets within the tile
-  int* tile[2];   // [ntiles] tile sums, then tile offsets
-  unsigned int* done;  // tile blocks finished (back to 0 by the last one)
-  int n, ntiles;
-};
-constexpr int kScanTile = 1024;
-constexpr int kReduceLanes = 8;
-
-__global__ void __launch_bounds__(kScanTile) k_scan_tiles(ScanPair P)
-{
-  pdl_enter();
-  __shared__ int wsum[32];
-  __shared__ int last;
-  const int y = blockIdx.y;
-  // the array's pointers by selection (an index into the parameter arrays
-  // would copy them to local memory)
-  const int* in = y ? P.in[1] : P.in[0];
-  int* part = y ? P.part[1] : P.part[0];
-  int* tile = y ? P.tile[1] : P.tile[0];
-  const int i = blockIdx.x * kScanTile + threadIdx.x;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int v = (i < P.n) ? in[i] : 0;
-  int x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += t;
-  }
-  if (lane == 31) wsum[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    int w = wsum[lane];
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += t;
-    }
-    wsum[lane] = w;
-  }
-  __syncthreads();
-  const int incl = x + (wid > 0 ? wsum[wid - 1] : 0);
-  if (i < P.n) part[i] = incl - v;
-  if (threadIdx.x == kScanTile - 1) tile[blockIdx.x] = incl;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(P.done, 1u) == gridDim.x * gridDim.y - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  if (wid < 2) {  // warp 0 / 1 scans the tile sums of array 0 / 1, 32 at a time
-    int* ty = wid ? P.tile[1] : P.tile[0];
-    int carry = 0;
-    for (int t0 = 0; t0 < P.ntiles; t0 += 32) {
-      const int t = t0 + lane;
-      const int u = t < P.ntiles ? __ldcg(ty + t) : 0;
-      int z = u;
-      for (int o = 1; o < 32; o <<= 1) {
-        int q = __shfl_up_sync(0xffffffffu, z, o);
-        if (lane >= o) z += q;
-      }
-      if (t < P.ntiles) ty[t] = carry + z - u;
-      carry += __shfl_sync(0xffffffffu, z, 31);
-    }
-    if (lane == 0) (wid ? P.out[1] : P.out[0])[P.n] = carry;
-  }
-  if (threadIdx.x == 0) *P.done = 0u;
-}
-
-// Flat task list (atom, partner) and record offsets; with `pairs`, also the
-// work list of tasks owned by the lower index of their pair and, for each,
-// the partner's task of the same pair (a linear search in its special list).
-__global__ void k_spc_compact(SpecialTasks Tk, ScanPair P, const int* nbonds, int n, int pairs, unsigned int* status)
-{
-  pdl_enter();
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool ok = a < n;
-  int c = 0, o = 0, nhi = 0;
-  if (ok) {
-    c = Tk.cnt[a];
-    o = P.part[0][a] + P.tile[0][a / kScanTile];
-    const int ra = P.part[1][a] + P.tile[1][a / kScanTile];
-    Tk.off[a] = o;
-    Tk.roff[a] = ra;
-    const int rs = rec_size(nbonds[a]);
-    for (int q = 0; q < c; q++) {
-      const int t = o + q;
-      const long ro = (long)ra + (long)q * rs;
-      const int b = Tk.part[(long)a * Tk.cap + q];
-      if (t < Tk.task_cap) {
-        Tk.flat[t] = make_int2(a, b);
-        if (ro + rs <= Tk.rec_cap) Tk.trec[t] = ro;
-        else { Tk.trec[t] = -1; atomicOr(status, ST_RECORD_OVERFLOW); }
-        nhi += (b > a);
-      } else {
-        atomicOr(status, ST_RECORD_OVERFLOW);
-      }
-    }
+  for (int k = gl; k < nsp; k += kLjGroup) {
+    const long t = o + k;
+    if (t >= Tk.task_cap) break;
+    Tk.flat[t] = make_int2(a, part[k]);
+    const long rt = ro + (long)k * rs;
+    if (rt + rs <= Tk.rec_cap) Tk.trec[t] = rt;
+    else { Tk.trec[t] = -1; atomicOr(status, ST_RECORD_OVERFLOW); }
   }
   if (!pairs) return;  // uniform over the launch
-  const unsigned long long w0 = warp_alloc(nhi, Tk.wcnt);
-  if (!ok) return;
-  int w = (int)w0;
-  for (int q = 0; q < c; q++) {
-    const int t = o + q;
-    if (t >= Tk.task_cap) break;
-    const int b = Tk.part[(long)a * Tk.cap + q];
-    if (b < a) continue;
-    int t2 = -1;
-    const int cb = Tk.cnt[b], ob = P.part[0][b] + P.tile[0][b / kScanTile];
-    for (int u = 0; u < cb; u++)
-      if (Tk.part[(long)b * Tk.cap + u] == a) { t2 = ob + u; break; }
-    if (t2 >= Tk.task_cap) t2 = -1;
-    Tk.wrev[t] = t2;
-    Tk.work[w++] = t;
+  // the pairs this atom owns (b > a), in list order, as work items; a task
+  // beyond the capacity leaves a -1 in its place
+  int k = 0;
+  for (int q0 = 0; q0 < nsp; q0 += kLjGroup) {
+    const int qq = q0 + gl;
+    const bool own = qq < nsp && part[qq] > a;
+    const unsigned m = __ballot_sync(gmask, own);
+    const long w = wb + k + __popc(m & below);
+    if (own && w < Tk.task_cap) Tk.work[w] = (o + qq < Tk.task_cap) ? (int)(o + qq) : -1;
+    k += __popc(m);
   }
 }
 
@@ -873,27 +856,43 @@ __global__ void k_lj_special(const ReboParams* P, const TB* Tb, LJParams LP, Bon
                              SpecialTasks Tk, unsigned int* status)
 {
   pdl_enter();
-  const int total = min(Tk.off[S.n], Tk.task_cap);
+  const int total = spc_total(Tk);
   ReboT<Real, TB> R{*P, *Tb, B, status};
   LJT<Real, TB> X{LP, R, T};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
     lj_special_task(X, S, Tk, t, status);
 }
 
-// Special LJ pairs, one thread per pair (both ends' records).
+// Special LJ pairs, one thread per pair (both ends' records): the work item
+// is the lower-index end's task; the partner's task of the same pair is found
+// by a linear search of the partner's special list.  The loop runs whole
+// warps (w0 is uniform over a warp) and the lanes meet again after the
+// search, so the pair terms that follow run with the warp converged.
 template <class Real, class TB>
 __global__ void k_lj_special_pair(const ReboParams* P, const TB* Tb, LJParams LP, BondList B, CijTable T, State S,
                                   SpecialTasks Tk, unsigned int* status)
 {
   pdl_enter();
-  const long total = (long)*Tk.wcnt;
+  const long total = (long)min(Tk.ctr[0], (unsigned long long)Tk.task_cap);
   ReboT<Real, TB> R{*P, *Tb, B, status};
   LJT<Real, TB> X{LP, R, T};
-  for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < total; w += (long)gridDim.x * blockDim.x) {
-    const int t = Tk.work[w];
-    const int t2 = Tk.wrev[t];
-    if (t2 < 0) { atomicOr(status, ST_RECORD_OVERFLOW); continue; }
-    lj_special_pair_task(X, S, Tk, t, t2, status);
+  const int lane = threadIdx.x & 31;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long w0 = (long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); w0 < total; w0 += stride) {
+    const long w = w0 + lane;
+    const int t = w < total ? Tk.work[w] : -1;  // -1: none, or beyond the task capacity (already flagged)
+    int t2 = -1;
+    if (t >= 0) {
+      const int2 ab = Tk.flat[t];
+      int u0, u1;
+      spc_range(Tk, ab.y, u0, u1);
+      const int* pb = Tk.part + (long)ab.y * Tk.cap;
+      for (int u = 0; u < u1 - u0; u++)
+        if (pb[u] == ab.x) { t2 = u0 + u; break; }
+      if (t2 < 0) atomicOr(status, ST_RECORD_OVERFLOW);
+    }
+    __syncwarp();
+    if (t2 >= 0) lj_special_pair_task(X, S, Tk, t, t2, status);
   }
 }
 
@@ -950,7 +949,8 @@ __device__ V3 gather_lanes(const BondList& B, const ForceOut& O, const SpecialTa
     }
     if (with_lj) {
       // middle-bond terms of the LJ special pairs (mid_gather_atom)
-      const int t0 = X.off[k], t1 = X.off[k + 1] < X.task_cap ? X.off[k + 1] : X.task_cap;
+      int t0, t1;
+      spc_range(X, k, t0, t1);
       for (int t = t0; t < t1; t++) {
         const int4 e = X.mid[t];
         if (!e.w || e.x != a) continue;
@@ -961,7 +961,8 @@ __device__ V3 gather_lanes(const BondList& B, const ForceOut& O, const SpecialTa
       const int nbk = B.nb[k];
       for (int qq = 0; qq < nbk; qq++) {
         const int lo = B.bj[k * B.mb + qq];
-        const int u0 = X.off[lo], u1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+        int u0, u1;
+        spc_range(X, lo, u0, u1);
         for (int t = u0; t < u1; t++) {
           const int4 e = X.mid[t];
           if (!e.w || e.x != k || e.z != a) continue;
@@ -1343,14 +1344,13 @@ struct mdg_ctx {
   bool overlap = false;
   cudaStream_t side = nullptr, side2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
-  int* lj_inr = nullptr;      // [n * LJ list cap] in-range LJ partners of the step, list order
-  int* lj_inr_cnt = nullptr;  // [n]
+  int* lj_inr = nullptr;      // [n * LJ list cap] in-range LJ partners of the step: far from the front, close from the back
+  int* lj_inr_cnt = nullptr;  // [2n] far counts, close counts
   bool tuned = false;        // the autotuner ran for this system
   float tune_ms[3] = {0, 0, 0};  // its timings of one force evaluation per task mode
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
-  int* scan_tiles = nullptr;  // 2 (n / 1024 + 2) tile sums, a counter, 2 n offsets within tiles
 
   // one MD step captured as a CUDA graph (replayed when no per-step energies are wanted)
   cudaGraphExec_t step_graph = nullptr;
@@ -1541,11 +1541,10 @@ void free_system(mdg_ctx* c)
     c->has_list[l] = false;
   }
   void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
-                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work, c->spc.wrev,
-                c->spc.wcnt, c->scan_tiles, c->lj_inr, c->lj_inr_cnt};
+                c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work,
+                c->spc.ctr, c->lj_inr, c->lj_inr_cnt};
   c->lj_inr = nullptr;
   c->lj_inr_cnt = nullptr;
-  c->scan_tiles = nullptr;
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   c->step_graph = nullptr;
   for (void* p : lq)
@@ -1817,7 +1816,7 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     rc = rebuild_list(c, 1, c->side2);
     if (rc) return rc;
     LAUNCH_ON(c, c->side2, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
-              c->lj_inr_cnt);
+              c->lj_inr_cnt, c->lj_inr_cnt + c->n);
     CK(cudaEventRecord(c->ev_join2, c->side2));
     rc = rebuild_list(c, 0, c->stream);
     if (rc) return rc;
@@ -1826,7 +1825,7 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     if (rc) return rc;
     if (lj)
       LAUNCH(c, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
-             c->lj_inr_cnt);
+             c->lj_inr_cnt, c->lj_inr_cnt + c->n);
   }
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
@@ -1882,30 +1881,16 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
   if (pot & MDG_POT_BRENNER)
     LAUNCH(c, "brenner", k_brenner, nblk(c->n), kThreads, c->d_bp, c->d_btables, B, c->fo, c->d_status);
   if (lj) {
-    LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->d_status);
+    LAUNCH(c, "cij_table", k_cij, nblk(c->n), kThreads, B, c->cij, c->spc.ctr, c->d_status);
     if (ovl) CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
-    if (f32p)
-      LAUNCH(c, "lj_plain", k_lj_plain<f32>, nblk(c->n * kLjGroup), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
-             c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
-    else
-      LAUNCH(c, "lj_plain", k_lj_plain<double>, nblk(c->n * kLjGroup), kThreads, c->ljp, c->cij, S, c->nl[1], c->lj_inr,
-             c->lj_inr_cnt, c->bb.nb, c->fo, c->spc, c->d_status);
-    ScanPair sp;
-    sp.in[0] = c->spc.cnt;
-    sp.in[1] = c->spc.rsz;
-    sp.out[0] = c->spc.off;
-    sp.out[1] = c->spc.roff;
-    const int tstride = c->n / kScanTile + 2;
-    sp.tile[0] = c->scan_tiles;
-    sp.tile[1] = c->scan_tiles + tstride;
-    sp.done = (unsigned int*)(c->scan_tiles + 2 * tstride);
-    sp.part[0] = c->scan_tiles + 2 * tstride + 1;
-    sp.part[1] = sp.part[0] + c->n;
-    sp.n = c->n;
-    sp.ntiles = (c->n + kScanTile - 1) / kScanTile;
-    LAUNCH(c, "lj_scan_tiles", k_scan_tiles, dim3(sp.ntiles, 2), kScanTile, sp);
     const int pairs = (c->bt.ctr && c->bt.pairs) ? 1 : 0;
-    LAUNCH(c, "lj_compact", k_spc_compact, nblk(c->n), kThreads, c->spc, sp, c->bb.nb, c->n, pairs, c->d_status);
+    const int lgrid = nblk(c->n * kLjGroup, kLjThreads);
+    if (f32p)
+      LAUNCH(c, "lj_pairs", k_lj_pairs<f32>, lgrid, kLjThreads, c->ljp, c->cij, S, c->nl[1].cap, c->lj_inr,
+             c->lj_inr_cnt, c->lj_inr_cnt + c->n, c->bb.nb, c->fo, c->spc, pairs, c->d_status);
+    else
+      LAUNCH(c, "lj_pairs", k_lj_pairs<double>, lgrid, kLjThreads, c->ljp, c->cij, S, c->nl[1].cap, c->lj_inr,
+             c->lj_inr_cnt, c->lj_inr_cnt + c->n, c->bb.nb, c->fo, c->spc, pairs, c->d_status);
     // b*_ij of close non-bonded pairs stays FP64 in the mixed mode too: the
     // S(t_b) window (0.04 wide for C-C) multiplies an error of b* by up to
     // 1/0.04^2 in the pair force, beyond what float b* can carry.
@@ -2286,7 +2271,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     if (!L.cnt || !L.list || !L.pos0) return fail(MDG_ERR_CUDA, "cudaMalloc (neighbour list)");
     if (l == 1) {
       c->lj_inr = dalloc<int>((size_t)n * L.cap);
-      c->lj_inr_cnt = dalloc<int>(n);
+      c->lj_inr_cnt = dalloc<int>(2 * (size_t)n);  // far counts, then close counts
       if (!c->lj_inr || !c->lj_inr_cnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ in-range list)");
     }
     int rc = nsys > 1 ? setup_grid_batch(c, l, hpos) : setup_grid(c, l, hpos);
@@ -2373,28 +2358,22 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     X.cnt = dalloc<int>(n);
     X.rsz = dalloc<int>(n);
     X.part = dalloc<int>((size_t)n * X.cap);
-    X.off = dalloc<int>(n + 1);
-    X.roff = dalloc<int>(n + 1);
+    X.off = dalloc<int>(n);
+    X.roff = dalloc<long>(n);
     X.flat = dalloc<int2>(X.task_cap);
     X.trec = dalloc<long>(X.task_cap);
     X.rec = dalloc<double>(X.rec_cap);
     X.mid = dalloc<int4>(X.task_cap);
     X.midc = dalloc<double>(X.task_cap);
     X.work = dalloc<int>(X.task_cap);
-    X.wrev = dalloc<int>(X.task_cap);
-    X.wcnt = dalloc<unsigned long long>(1);
-    if (!X.work || !X.wrev || !X.wcnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ work list)");
-    CK(cudaMemset(X.wcnt, 0, sizeof(unsigned long long)));
+    X.ctr = dalloc<unsigned long long>(3 * kCtrStride);
+    if (!X.work || !X.ctr) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ work list)");
+    CK(cudaMemset(X.ctr, 0, 3 * kCtrStride * sizeof(unsigned long long)));
     if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->cij.mask || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
         !X.trec || !X.rec || !X.mid || !X.midc)
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
     CK(cudaMemset(X.cnt, 0, n * sizeof(int)));
-    CK(cudaMemset(X.off, 0, (n + 1) * sizeof(int)));
-    // tile sums of both arrays, the finished-tiles counter, offsets within the tiles
-    const size_t scan_ints = 2 * (size_t)(n / kScanTile + 2) + 1 + 2 * (size_t)n;
-    c->scan_tiles = dalloc<int>(scan_ints);
-    if (!c->scan_tiles) return fail(MDG_ERR_CUDA, "cudaMalloc (scan)");
-    CK(cudaMemset(c->scan_tiles, 0, scan_ints * sizeof(int)));
+    CK(cudaMemset(X.off, 0, n * sizeof(int)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2797,9 +2776,11 @@ static int run_steps(mdg_ctx* c, int nsteps, double dt, double* epot, double* et
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
   const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
-  int rc = init_first_step(c);
+  // the split is chosen before the initial forces, so that they come from
+  // the split every step uses
+  int rc = autotune(c);
   if (rc) return rc;
-  rc = autotune(c);
+  rc = init_first_step(c);
   if (rc) return rc;
   rc = io_run_start(c, dtf, fresh);
   if (rc) return rc;
@@ -2876,9 +2857,9 @@ int mdg_batch_run(mdg_ctx* c, int nsteps, double dt, double* epot, double* etot)
   if (nsteps < 0) return fail(MDG_ERR_ARG, "negative step count");
   if (!epot && !etot) return mdg_run(c, nsteps, dt, nullptr, nullptr);
   const double dtf = (c->prm.units == MDG_UNITS_CGS) ? dt / kFs : dt;
-  int rc = init_first_step(c);
+  int rc = autotune(c);
   if (rc) return rc;
-  rc = autotune(c);
+  rc = init_first_step(c);
   if (rc) return rc;
   rc = io_run_start(c, dtf, true);
   if (rc) return rc;

@@ -196,11 +196,8 @@ MDG_HD void cij_build_atom(const BondList& B, CijTable& T, int i, unsigned int* 
 // Lookup of target j in the table of i (binary search).  Returns the entry
 // index or -1.
 template <class W>
-MDG_HD int cij_find(const CijTableT<W>& T, int i, int j)
+MDG_HD int cij_search(const CijTableT<W>& T, int i, int j)
 {
-  // most LJ partners are beyond three bonds: one mask load rules them out
-  // without the dependent loads of the search
-  if (!((T.mask[i] >> (j & 63)) & 1ull)) return -1;
   int lo = 0, hi = T.cnt[i] - 1;
   const int4* e = T.ent + (long)i * T.cap;
   while (lo <= hi) {
@@ -211,6 +208,15 @@ MDG_HD int cij_find(const CijTableT<W>& T, int i, int j)
     else hi = mid - 1;
   }
   return -1;
+}
+
+// The same, after the mask test: most LJ partners are beyond three bonds,
+// and one mask load rules them out without the dependent loads of the search.
+template <class W>
+MDG_HD int cij_find(const CijTableT<W>& T, int i, int j)
+{
+  if (!((T.mask[i] >> (j & 63)) & 1ull)) return -1;
+  return cij_search(T, i, j);
 }
 
 // S(t) switch (AIREBO::S / dS, AIREBO_LJ.cxx:116-156).
@@ -416,7 +422,10 @@ typedef LJT<double, ReboTables> LJ;
 
 // Special LJ pairs (those needing b*_ij or a connectivity gradient) are
 // evaluated one task per (atom, pair); each task writes its own record and a
-// per-atom pass sums an atom's records in list order.
+// per-atom pass sums an atom's records in list order.  An atom's tasks take
+// the contiguous range [off[a], off[a] + cnt[a]) of the task arrays and its
+// records the range from roff[a]; where those ranges lie depends on
+// scheduling (one atomicAdd per block), the order within them does not.
 template <class W>
 struct SpecialTasksT {
   int cap;          // special pairs per atom
@@ -425,23 +434,41 @@ struct SpecialTasksT {
   int* cnt;         // [n] special pairs of each atom (LJ-list order)
   int* rsz;         // [n] record doubles of each atom: cnt * rec_size(bonds)
   int* part;        // [n * cap] partner of each
-  int* off;         // [n + 1] exclusive prefix of cnt; off[n] = total
-  int* roff;        // [n + 1] exclusive prefix of rsz
+  int* off;         // [n] first task of each atom
+  long* roff;       // [n] first record double of each atom
   int2* flat;       // [task_cap] (atom, partner)
-  long* trec;       // [task_cap] record offset of each task
+  long* trec;       // [task_cap] record offset of each task (-1: beyond rec_cap)
   W* rec;           // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]
   int4* mid;        // [task_cap] middle-bond output (k, slot of m in k, m, valid)
   W* midc;          // [task_cap]
   W* dp;            // [task_cap * kNParam] energy derivatives by parameter (adjoint path only)
   // one evaluation per pair (the lower-index end's task writes both records):
-  int* work;        // [task_cap] tasks whose owner is the lower index
-  int* wrev;        // [task_cap] the partner's task of the same pair (-1: none)
-  unsigned long long* wcnt;  // number of work items
+  int* work;        // [task_cap] tasks whose owner is the lower index (-1: beyond task_cap)
+  unsigned long long* ctr;  // work items, tasks, record doubles handed out this evaluation, at
+                            // ctr[0], ctr[kCtrStride], ctr[2 kCtrStride] (one 128-byte line each)
 };
+constexpr int kCtrStride = 16;
 typedef SpecialTasksT<double> SpecialTasks;
 
 // Record size of a task owned by an atom with nb bonds.
 MDG_HD int rec_size(int nb) { return 4 + 4 * nb; }
+
+// Atom a's tasks [t0, t1), clipped to the task capacity.
+template <class W>
+MDG_HD void spc_range(const SpecialTasksT<W>& X, int a, int& t0, int& t1)
+{
+  t0 = X.off[a];
+  const long e = (long)t0 + X.cnt[a];
+  t1 = e < X.task_cap ? (int)e : X.task_cap;
+}
+
+// Number of tasks handed out by the last special-pair search, clipped.
+template <class W>
+MDG_HD int spc_total(const SpecialTasksT<W>& X)
+{
+  const unsigned long long t = X.ctr[kCtrStride];
+  return t < (unsigned long long)X.task_cap ? (int)t : X.task_cap;
+}
 
 // Geometry of a pair lo -> hi (rv = x_lo - x_hi, r = |rv| as the FP64 path
 // computes them) in the arithmetic type; on the adjoint path with the
@@ -469,43 +496,100 @@ MDG_HD PairGT<Real> pair_geom(V3 rv, double r, const double4* tan, int lo, int h
   return p;
 }
 
-// Classifies one LJ pair seen from atom a: returns 0 (skip), 1 (plain: C = 1
-// and S(t_r) = 0, so E = VLJ) or 2 (special); amask = T.mask[a].  For plain pairs adds the own
-// gradient and, at the lower end, the energy.  The classification is made in
-// double on every path (the adjoint path's pairs are the FP64 path's).
+// Class of one LJ pair seen from atom a: kind 0 (skip: beyond the cutoff or
+// C = 0), 1 (plain: C = 1 and S(t_r) = 0, so E = VLJ) or 2 (special: needs
+// b*_ij or a connectivity gradient); amask = T.mask[a].  The classification
+// is made in double on every path (the adjoint path's pairs are the FP64
+// path's), and the special-pair finder and the plain-pair kernels make it
+// with the same expressions.
+struct LJClass {
+  int kind, lo, hi, tb;
+  V3 rv;     // x_lo - x_hi
+  double r;  // |rv| (kinds 1 and 2)
+  double C;  // 1 - w_ij (kinds 1 and 2)
+};
+
+// w_ij of the pair (a, b) as a's own connectivity table holds it; amask =
+// T.mask[a] (a clear bit for b proves w = 0 without the search).  The
+// special-pair evaluation takes w from the lower index's table, whose
+// product of bond cutoffs may differ from a's in rounding (the factors are
+// multiplied in the reverse order); the class of the pair does not: it
+// depends on w only through w == 0 (no path within three bonds: the bonds
+// are symmetric) and w == 1 (a path whose cutoffs are all 1; a product with
+// a factor below 1 never rounds up to 1), and both read the same from
+// either end.  So each end classifies from its own table, which the atom's
+// lanes share in L1.
+template <class W>
+MDG_HD double lj_w_own(const CijTableT<W>& T, int a, int b, unsigned long long amask)
+{
+  if (!((amask >> (b & 63)) & 1ull)) return 0.0;
+  const int ei = cij_search(T, a, b);
+  return ei >= 0 ? val(T.w[(long)a * T.cap + ei]) : 0.0;
+}
+
+// The pair at squared distance d2 may lie in the window where S(t_r) != 0
+// and E_LJ takes b*_ij (when C > 0): r below the window's upper end
+// 2^(1/6) sigma, with a relative margin of 1e-12 on r^2, so that rounding
+// never puts a pair with S(t_r) != 0 outside.  A pair inside the margin is
+// evaluated by the special-pair path, which computes S(t_r) itself (0 there).
+MDG_HD bool lj_close(const LJParams& P, int ta, int tb, double d2)
+{
+  const double rmax = P.RLJ[ta][tb][1];
+  return d2 < rmax * rmax * (1.0 + 1e-12);
+}
+
+// The class of a pair from its geometry and w: far = !lj_close.
+MDG_HD int lj_kind(double w, bool close)
+{
+  if (!(1 - w > 0.0)) return 0;
+  return (close || w != 0.0) ? 2 : 1;
+}
+
+template <class W>
+MDG_HD LJClass lj_class(const LJParams& P, const CijTableT<W>& T, const State& St, int a, int b, V3 xa, int ta,
+                        unsigned long long amask, bool known_far = false)
+{
+  LJClass c;
+  const double4 pb = St.pos[b];
+  c.tb = (int)pb.w;
+  c.lo = a;
+  c.hi = b;
+  c.kind = 0;
+  c.r = 0.0;
+  c.C = 0.0;
+  const Box box = box_of(St, a);
+  if (a < b) c.rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
+  else { c.lo = b; c.hi = a; c.rv = depos(box, v3(pb.x, pb.y, pb.z), xa); }
+  const double d2 = norm2(c.rv);
+  const double R2 = P.R[ta][c.tb][1];
+  if (d2 > R2 * R2) return c;
+  const double w = lj_w_own(T, a, b, amask);
+  c.C = 1 - w;  // exact for the plain pairs (w = 0); kind 2 takes C from the lower index's table
+  if (!(c.C > 0.0)) return c;
+  c.r = sqrt(d2);
+  c.kind = lj_kind(w, !known_far && lj_close(P, ta, c.tb, d2));
+  return c;
+}
+
+// One LJ pair seen from atom a: returns its lj_class kind; for plain pairs
+// adds the own gradient and, at the lower end, the energy.  known_far: the
+// pair is known to lie outside the S(t_r) window (the in-range filter's far
+// list).
 template <class Real, class S, class W>
 MDG_HD int lj_plain_pair(const LJParams& P, const CijTableT<W>& T, const State& St, int a, int b, V3 xa, int ta,
-                         unsigned long long amask, S& sink, W& e, const double4* tan = nullptr)
+                         unsigned long long amask, S& sink, W& e, const double4* tan = nullptr,
+                         bool known_far = false)
 {
-  const double4 pb = St.pos[b];
-  const int tb = (int)pb.w;
-  int lo = a, hi = b;
-  V3 rv;
-  const Box& box = box_of(St, a);
-  if (a < b) rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
-  else { lo = b; hi = a; rv = depos(box, v3(pb.x, pb.y, pb.z), xa); }
-  const double d2 = norm2(rv);
-  const double R1 = P.R[ta][tb][0], R2 = P.R[ta][tb][1];
-  if (d2 > R2 * R2) return 0;
-  // amask is a's own connectivity mask (T.mask[a]).  Reachability within
-  // three bonds is symmetric, so a clear bit for b in it proves w = 0 without
-  // the lower-index atom's table, which may be b's: its lookup is only made
-  // for the pairs the mask admits.
-  const int ei = ((amask >> (b & 63)) & 1ull) ? cij_find(T, lo, hi) : -1;
-  const double w = ei >= 0 ? val(T.w[(long)lo * T.cap + ei]) : 0.0;
-  const double C = 1 - w;
-  if (!(C > 0.0)) return 0;
-  const double r = sqrt(d2);
-  const double Str = Slj(r, P.RLJ[ta][tb][0], P.RLJ[ta][tb][1]);
-  if (Str != 0.0 || w != 0.0) return 2;
+  const LJClass c = lj_class(P, T, St, a, b, xa, ta, amask, known_far);
+  if (c.kind != 1) return c.kind;
   // the pair term itself in the arithmetic type
-  PairGT<Real> p = pair_geom<Real>(rv, r, tan, lo, hi);
-  cutoff(p.r, R1, R2, p.f, p.df);
+  PairGT<Real> p = pair_geom<Real>(c.rv, c.r, tan, c.lo, c.hi);
+  cutoff(p.r, P.R[ta][c.tb][0], P.R[ta][c.tb][1], p.f, p.df);
   W LJv, val;
-  const int tlo = lo == a ? ta : tb, thi = lo == a ? tb : ta;
-  vlj(P, tlo, thi, lo, hi, p, Real(1.0 * C), sink, LJv, val);
-  if constexpr (S::kAdj) lj_par(P, tlo, thi, lo, p, W(C), W(1.0), W(0.0), val, sink);
-  if (a == lo) e += 1.0 * C * LJv;
+  const int tlo = c.lo == a ? ta : c.tb, thi = c.lo == a ? c.tb : ta;
+  vlj(P, tlo, thi, c.lo, c.hi, p, Real(1.0 * c.C), sink, LJv, val);
+  if constexpr (S::kAdj) lj_par(P, tlo, thi, c.lo, p, W(c.C), W(1.0), W(0.0), val, sink);
+  if (a == c.lo) e += 1.0 * c.C * LJv;
   return 1;
 }
 
@@ -518,7 +602,8 @@ MDG_HD V3T<W> mid_gather_atom(const BondListT<W>& B, const SpecialTasksT<W>& X, 
   const int nb = B.nb[a];
   for (int s = 0; s < nb; s++) {
     const int lo = B.bj[a * B.mb + s];
-    const int t0 = X.off[lo], t1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+    int t0, t1;
+    spc_range(X, lo, t0, t1);
     for (int t = t0; t < t1; t++) {
       int4 e = X.mid[t];
       if (!e.w || e.x != a) continue;
@@ -532,7 +617,8 @@ MDG_HD V3T<W> mid_gather_atom(const BondListT<W>& B, const SpecialTasksT<W>& X, 
     const int nbk = B.nb[k];
     for (int q = 0; q < nbk; q++) {
       const int lo = B.bj[k * B.mb + q];
-      const int t0 = X.off[lo], t1 = X.off[lo + 1] < X.task_cap ? X.off[lo + 1] : X.task_cap;
+      int t0, t1;
+      spc_range(X, lo, t0, t1);
       for (int t = t0; t < t1; t++) {
         int4 e = X.mid[t];
         if (!e.w || e.x != k || e.z != a) continue;
@@ -660,7 +746,8 @@ MDG_HD void lj_reduce_atom(const BondListT<Wd>& B, const SpecialTasksT<Wd>& Tk, 
   Wd e = O.e_lj[a];
   Wd* A = O.A + (long)a * O.mb * 3;
   Wd* W = O.W + (long)a * O.mb;
-  const int t0 = Tk.off[a], t1 = Tk.off[a + 1] < Tk.task_cap ? Tk.off[a + 1] : Tk.task_cap;
+  int t0, t1;
+  spc_range(Tk, a, t0, t1);
   for (int t = t0; t < t1; t++) {
     const long ro = Tk.trec[t];
     if (ro < 0) continue;
