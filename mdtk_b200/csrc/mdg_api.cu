@@ -62,29 +62,31 @@ __device__ __forceinline__ void top2_merge(double& t1, double& t2, double u1, do
 
 // Start of a step: the position update x += v dt + a dt^2/2 (do_pos, eq 1
 // of the step) and, per block, the two largest displacements since each
-// list's last build (lists 0..nl-1; partials of list l at part + 2 gridDim.x l).
-// The last block to finish (a counter, no waiting) reduces the partials of
-// each list to its rebuild flag: need[l] = force[l] || top1 + top2 > trigger
-// (NeighbourList::MovedTooMuch, NeighbourList.cxx:109-133), then clears force[l].
-__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, int mask, double* part,
-                             int* need, int* force, unsigned int* done)
+// list's last build (lists 0-2 and, as slot 3, the LJ list's near sublist;
+// partials of slot l at part + 2 gridDim.x l).  The last block to finish (a
+// counter, no waiting) reduces the partials of each slot to its rebuild flag:
+// need[l] = force[l] || top1 + top2 > trigger (NeighbourList::MovedTooMuch,
+// NeighbourList.cxx:109-133), then clears force[l].
+constexpr int kNSlots = 4;
+__global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1, NList L2, NList L3, int mask,
+                             double* part, int* need, int* force, unsigned int* done)
 {
   pdl_enter();
-  __shared__ double s1[3][kThreads / 32], s2[3][kThreads / 32];
+  __shared__ double s1[kNSlots][kThreads / 32], s2[kNSlots][kThreads / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double d1[3] = {0.0, 0.0, 0.0}, d2[3] = {0.0, 0.0, 0.0};
+  double d1[kNSlots] = {0.0, 0.0, 0.0, 0.0}, d2[kNSlots] = {0.0, 0.0, 0.0, 0.0};
   for (int a = i; a < S.n; a += gridDim.x * blockDim.x) {
     if (do_pos) verlet_pos_atom(S, step_dt(P, S, a), a);
 #pragma unroll
-    for (int l = 0; l < 3; l++) {
+    for (int l = 0; l < kNSlots; l++) {
       if (!((mask >> l) & 1)) continue;
-      const double d = disp_atom(S, l == 0 ? L0 : (l == 1 ? L1 : L2), a);
+      const double d = disp_atom(S, l == 0 ? L0 : (l == 1 ? L1 : (l == 2 ? L2 : L3)), a);
       if (d >= d1[l]) { d2[l] = d1[l]; d1[l] = d; }
       else if (d >= d2[l]) d2[l] = d;
     }
   }
 #pragma unroll
-  for (int l = 0; l < 3; l++) {
+  for (int l = 0; l < kNSlots; l++) {
     if (!((mask >> l) & 1)) continue;
     for (int o = 16; o > 0; o >>= 1) {
       const double u1 = __shfl_down_sync(0xffffffffu, d1[l], o), u2 = __shfl_down_sync(0xffffffffu, d2[l], o);
@@ -96,7 +98,7 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
     }
   }
   __syncthreads();
-  if (threadIdx.x < 3 && ((mask >> threadIdx.x) & 1)) {
+  if (threadIdx.x < kNSlots && ((mask >> threadIdx.x) & 1)) {
     const int l = threadIdx.x;
     double t1 = 0.0, t2 = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) top2_merge(t1, t2, s1[l][w], s2[l][w]);
@@ -113,7 +115,7 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
   // warp l: each lane keeps the two largest of a strided share of the
   // partials, then the lanes' pairs are merged by shuffles (the two largest
   // of a set do not depend on the order they are met in)
-  if (wid < 3 && ((mask >> wid) & 1)) {
+  if (wid < kNSlots && ((mask >> wid) & 1)) {
     const int l = wid;
     const double* pl = part + 2 * gridDim.x * l;
     double t1 = 0.0, t2 = 0.0;
@@ -123,7 +125,7 @@ __global__ void k_step_start(State S, StepDev P, int do_pos, NList L0, NList L1,
       top2_merge(t1, t2, u1, u2);
     }
     if (lane == 0) {
-      const double trig = l == 0 ? L0.trigger : (l == 1 ? L1.trigger : L2.trigger);
+      const double trig = l == 0 ? L0.trigger : (l == 1 ? L1.trigger : (l == 2 ? L2.trigger : L3.trigger));
       need[l] = force[l] || (t1 + t2 > trig);
       force[l] = 0;
     }
@@ -636,6 +638,57 @@ __global__ void k_cij(BondList B, CijTable T, unsigned long long* spc_ctr, unsig
   if (a < B.n) cij_build_atom<kCijLocal>(B, T, a, status);
 }
 
+// The LJ list's near sublist: the entries within R2 + kLjNearSkin of the
+// atom, in list order, one warp per atom (the filter's loop with a wider
+// radius), and the positions it was taken at.  Rebuilt when the LJ list is
+// (need[1]) or when the two largest displacements since the last near build
+// exceed kLjNearSkin (need[3]); returns at once otherwise.  Every pair within
+// R2 is in it: such a pair was within R2 + (its two displacements) <=
+// R2 + kLjNearSkin at the near build, and in the LJ list.  The filter reads
+// this sublist (about 0.3 of the LJ list) in place of the whole list; its
+// order is the list's, so the in-range lists, and every sum over them, are
+// the same.  A fixed grid of warps strides over the atoms, so the launch
+// that finds no flag set costs a few blocks, not one per four atoms.
+constexpr double kLjNearSkin = 0.5;  // Angstrom
+__global__ void __launch_bounds__(kThreads) k_lj_near(LJParams P, State S, NList L, NList T, const int* need,
+                                                      unsigned int* status)
+{
+  pdl_enter();
+  if (!need[1] && !need[3]) return;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < S.n; a += nw) {  // whole warps
+    const double4 pa = S.pos[a];
+    const V3 xa = v3(pa.x, pa.y, pa.z);
+    const int ta = (int)pa.w;
+    const Box box = box_of(S, a);
+    const int cnt = L.cnt[a];
+    const int* lst = L.list + (long)a * L.cap;
+    int* out = T.list + (long)a * T.cap;
+    const unsigned below = (1u << lane) - 1u;
+    int k = 0;
+    for (int base = 0; base < cnt; base += 32) {
+      const int s = base + lane;
+      bool in = false;
+      int b = -1;
+      if (s < cnt) {
+        b = lst[s];
+        const double4 pb = S.pos[b];
+        const double R = P.R[ta][(int)pb.w][1] + kLjNearSkin;
+        const V3 rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
+        in = norm2(rv) <= R * R * (1.0 + 1e-12);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, in);
+      if (in) out[k + __popc(m & below)] = b;
+      k += __popc(m);
+    }
+    if (lane == 0) {
+      T.cnt[a] = k;
+      T.pos0[a] = pa;
+    }
+  }
+}
+
 // LJ pairs inside their cutoff, one warp per atom: the atom's LJ list is
 // read 32 entries at a time and the entries within the pair's cutoff R2 are
 // appended, in list order, to the atom's far list (front of its in-range
@@ -648,43 +701,44 @@ __global__ void __launch_bounds__(kThreads) k_lj_filter(LJParams P, State S, NLi
                                                         int* close_cnt)
 {
   pdl_enter();
-  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (a >= S.n) return;  // whole warps
-  const double4 pa = S.pos[a];
-  const V3 xa = v3(pa.x, pa.y, pa.z);
-  const int ta = (int)pa.w;
-  const Box box = box_of(S, a);
-  const int cnt = L.cnt[a];
-  const int* lst = L.list + (long)a * L.cap;
-  int* out = inr + (long)a * L.cap;
-  int* top = out + L.cap - 1;
-  const unsigned below = (1u << lane) - 1u;
-  int kf = 0, kc = 0;
-  for (int base = 0; base < cnt; base += 32) {
-    const int s = base + lane;
-    bool in = false, close = false;
-    int b = -1;
-    if (s < cnt) {
-      b = lst[s];
-      const double4 pb = S.pos[b];
-      const int tb = (int)pb.w;
-      const double R2 = P.R[ta][tb][1];
-      const V3 rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
-      const double d2 = norm2(rv);
-      in = !(d2 > R2 * R2);
-      close = in && lj_close(P, ta, tb, d2);  // lj_class's test, on the same d2
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < S.n; a += nw) {  // whole warps
+    const double4 pa = S.pos[a];
+    const V3 xa = v3(pa.x, pa.y, pa.z);
+    const int ta = (int)pa.w;
+    const Box box = box_of(S, a);
+    const int cnt = L.cnt[a];
+    const int* lst = L.list + (long)a * L.cap;
+    int* out = inr + (long)a * L.cap;
+    int* top = out + L.cap - 1;
+    const unsigned below = (1u << lane) - 1u;
+    int kf = 0, kc = 0;
+    for (int base = 0; base < cnt; base += 32) {
+      const int s = base + lane;
+      bool in = false, close = false;
+      int b = -1;
+      if (s < cnt) {
+        b = lst[s];
+        const double4 pb = S.pos[b];
+        const int tb = (int)pb.w;
+        const double R2 = P.R[ta][tb][1];
+        const V3 rv = depos(box, xa, v3(pb.x, pb.y, pb.z));
+        const double d2 = norm2(rv);
+        in = !(d2 > R2 * R2);
+        close = in && lj_close(P, ta, tb, d2);  // lj_class's test, on the same d2
+      }
+      const unsigned mf = __ballot_sync(0xffffffffu, in && !close);
+      const unsigned mc = __ballot_sync(0xffffffffu, close);
+      if (in && !close) out[kf + __popc(mf & below)] = b;
+      if (close) top[-(kc + __popc(mc & below))] = b;
+      kf += __popc(mf);
+      kc += __popc(mc);
     }
-    const unsigned mf = __ballot_sync(0xffffffffu, in && !close);
-    const unsigned mc = __ballot_sync(0xffffffffu, close);
-    if (in && !close) out[kf + __popc(mf & below)] = b;
-    if (close) top[-(kc + __popc(mc & below))] = b;
-    kf += __popc(mf);
-    kc += __popc(mc);
-  }
-  if (lane == 0) {
-    far_cnt[a] = kf;
-    close_cnt[a] = kc;
+    if (lane == 0) {
+      far_cnt[a] = kf;
+      close_cnt[a] = kc;
+    }
   }
 }
 
@@ -736,13 +790,11 @@ constexpr int kLjGroup = 16;     // lanes per atom (a divisor of 32): ~30 in-ran
 constexpr int kLjThreads = 128;  // 8 atoms per block
 constexpr int kReduceLanes = 8;
 template <class Real>
-__global__ void __launch_bounds__(kLjThreads, 7) k_lj_pairs(LJParams P, CijTable T, State S, int lcap, const int* inr,
-                                                         const int* far_cnt, const int* close_cnt,
-                                                         const int* nbonds, ForceOut O, SpecialTasks Tk, int pairs,
-                                                         unsigned int* status)
+__device__ __forceinline__ void lj_pairs_block(const LJParams& P, const CijTable& T, const State& S, int lcap,
+                                               const int* inr, const int* far_cnt, const int* close_cnt,
+                                               const int* nbonds, const ForceOut& O, const SpecialTasks& Tk,
+                                               int pairs, unsigned int* status, int gid)
 {
-  pdl_enter();
-  const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLjGroup;
   const int lane = threadIdx.x & 31, gl = lane % kLjGroup, gbase = lane - gl;
   const bool live = gid < S.n;  // every thread stays for the block's allocation
   const int a = live ? gid : S.n - 1;
@@ -848,6 +900,17 @@ __global__ void __launch_bounds__(kLjThreads, 7) k_lj_pairs(LJParams P, CijTable
     if (own && w < Tk.task_cap) Tk.work[w] = (o + qq < Tk.task_cap) ? (int)(o + qq) : -1;
     k += __popc(m);
   }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kLjThreads, 7) k_lj_pairs(LJParams P, CijTable T, State S, int lcap, const int* inr,
+                                                         const int* far_cnt, const int* close_cnt,
+                                                         const int* nbonds, ForceOut O, SpecialTasks Tk, int pairs,
+                                                         unsigned int* status)
+{
+  pdl_enter();
+  lj_pairs_block<Real>(P, T, S, lcap, inr, far_cnt, close_cnt, nbonds, O, Tk, pairs, status,
+                       (blockIdx.x * blockDim.x + threadIdx.x) / kLjGroup);
 }
 
 // Special LJ pairs, one thread per (atom, pair) task.
@@ -1306,9 +1369,10 @@ struct mdg_ctx {
 
   // lists: 0 = REBO range, 1 = LJ range
   NList nl[3];             // 0 REBO range, 1 AIREBO LJ range, 2 metal and ion pairs
+  NList ljt;               // the LJ list's near sublist (entries within R2 + kLjNearSkin; flag slot 3)
   Grid grid[3];
-  int* d_need = nullptr;   // [3]
-  int* d_force = nullptr;  // [3]
+  int* d_need = nullptr;   // [4]: lists 0-2, the LJ near sublist
+  int* d_force = nullptr;  // [4]
   unsigned int* d_disp_done = nullptr;  // blocks of step_start finished (back to 0 by the last)
   double* d_part = nullptr;
   double rcut[3] = {0, 0, 0};
@@ -1351,6 +1415,7 @@ struct mdg_ctx {
 
   unsigned int* d_status = nullptr;
   int special_blocks = 0;
+  int warp_blocks = 0;        // resident blocks of the warp-per-atom LJ list kernels (grid-stride over atoms)
 
   // one MD step captured as a CUDA graph (replayed when no per-step energies are wanted)
   cudaGraphExec_t step_graph = nullptr;
@@ -1542,7 +1607,8 @@ void free_system(mdg_ctx* c)
   }
   void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
                 c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work,
-                c->spc.ctr, c->lj_inr, c->lj_inr_cnt};
+                c->spc.ctr, c->lj_inr, c->lj_inr_cnt, c->ljt.cnt, c->ljt.list, c->ljt.pos0};
+  std::memset(&c->ljt, 0, sizeof(NList));
   c->lj_inr = nullptr;
   c->lj_inr_cnt = nullptr;
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
@@ -1742,7 +1808,7 @@ constexpr int kBathBlocks = 120;
 int step_start(mdg_ctx* c, const StepDev* step)
 {
   State S = c->S();
-  const int mask = (c->has_list[0] ? 1 : 0) | (c->has_list[1] ? 2 : 0) | (c->has_list[2] ? 4 : 0);
+  const int mask = (c->has_list[0] ? 1 : 0) | (c->has_list[1] ? 2 | 8 : 0) | (c->has_list[2] ? 4 : 0);
   if (step && step->tb_geom) {
     const int bps = std::max(1, kBathBlocks / c->nsys);
     LAUNCH(c, "bath_temp_partial", k_bath_partial, dim3(bps, c->nsys), kThreads, S, *step,
@@ -1752,7 +1818,7 @@ int step_start(mdg_ctx* c, const StepDev* step)
   StepDev none;
   std::memset(&none, 0, sizeof(none));
   LAUNCH(c, step ? "verlet_pos_disp" : "nl_disp", k_step_start, kDispParts, kThreads, S,
-         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], c->nl[2], mask, c->d_part, c->d_need, c->d_force,
+         step ? *step : none, step ? 1 : 0, c->nl[0], c->nl[1], c->nl[2], c->ljt, mask, c->d_part, c->d_need, c->d_force,
          c->d_disp_done);
   return MDG_OK;
 }
@@ -1775,6 +1841,9 @@ int rebuild_list(mdg_ctx* c, int l, cudaStream_t st)
   }
   LAUNCH_ON(c, st, l == 0 ? "nl_build_rebo" : (l == 1 ? "nl_build_lj" : "nl_build_metal"), k_nl_build, nblk(c->n),
             kThreads, S, g, L, need, c->d_status);
+  if (l == 1)
+    LAUNCH_ON(c, st, "nl_build_lj_near", k_lj_near, std::min(nblk(c->n * 32), c->warp_blocks), kThreads, c->ljp, S,
+              L, c->ljt, c->d_need, c->d_status);
   return MDG_OK;
 }
 
@@ -1815,8 +1884,8 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     CK(cudaStreamWaitEvent(c->side2, c->ev_fork2, 0));
     rc = rebuild_list(c, 1, c->side2);
     if (rc) return rc;
-    LAUNCH_ON(c, c->side2, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
-              c->lj_inr_cnt, c->lj_inr_cnt + c->n);
+    LAUNCH_ON(c, c->side2, "lj_filter", k_lj_filter, std::min(nblk(c->n * 32), c->warp_blocks), kThreads, c->ljp, S,
+              c->ljt, c->lj_inr, c->lj_inr_cnt, c->lj_inr_cnt + c->n);
     CK(cudaEventRecord(c->ev_join2, c->side2));
     rc = rebuild_list(c, 0, c->stream);
     if (rc) return rc;
@@ -1824,8 +1893,8 @@ int evaluate(mdg_ctx* c, const StepDev* step = nullptr)
     rc = rebuild_lists(c, step);
     if (rc) return rc;
     if (lj)
-      LAUNCH(c, "lj_filter", k_lj_filter, nblk(c->n * 32), kThreads, c->ljp, S, c->nl[1], c->lj_inr,
-             c->lj_inr_cnt, c->lj_inr_cnt + c->n);
+      LAUNCH(c, "lj_filter", k_lj_filter, std::min(nblk(c->n * 32), c->warp_blocks), kThreads, c->ljp, S, c->ljt,
+             c->lj_inr, c->lj_inr_cnt, c->lj_inr_cnt + c->n);
   }
   LAUNCH(c, "bonds", k_bonds, nblk(c->n), kThreads, S, c->nl[0], c->rp, c->bb, c->bt, c->d_status);
   BondList B = c->BL();
@@ -2074,8 +2143,8 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   }
   c->stream = c->own_stream;
   c->d_status = dalloc<unsigned int>(1);
-  c->d_need = dalloc<int>(3);
-  c->d_force = dalloc<int>(3);
+  c->d_need = dalloc<int>(4);
+  c->d_force = dalloc<int>(4);
   c->d_disp_done = dalloc<unsigned int>(1);
   c->d_energy = dalloc<double>(8);
   if (!c->d_status || !c->d_need || !c->d_force || !c->d_disp_done || !c->d_energy) {
@@ -2083,8 +2152,8 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
     return fail(MDG_ERR_CUDA, "cudaMalloc");
   }
   cudaMemset(c->d_status, 0, sizeof(unsigned int));
-  cudaMemset(c->d_need, 0, 3 * sizeof(int));
-  cudaMemset(c->d_force, 0, 3 * sizeof(int));
+  cudaMemset(c->d_need, 0, 4 * sizeof(int));
+  cudaMemset(c->d_force, 0, 4 * sizeof(int));
   cudaMemset(c->d_disp_done, 0, sizeof(unsigned int));
   if (cudaGetLastError() != cudaSuccess) { mdg_destroy(c); return fail(MDG_ERR_CUDA, "setup copies failed"); }
   *out = c;
@@ -2272,14 +2341,24 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     if (l == 1) {
       c->lj_inr = dalloc<int>((size_t)n * L.cap);
       c->lj_inr_cnt = dalloc<int>(2 * (size_t)n);  // far counts, then close counts
-      if (!c->lj_inr || !c->lj_inr_cnt) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ in-range list)");
+      NList& T = c->ljt;
+      T.cap = L.cap;
+      T.sorted = L.sorted;
+      T.pairs = L.pairs;
+      T.range2 = 0.0;  // per pair: (R2 + kLjNearSkin)^2
+      T.trigger = kLjNearSkin;
+      T.cnt = dalloc<int>(n);
+      T.list = dalloc<int>((size_t)n * T.cap);
+      T.pos0 = dalloc<double4>(n);
+      if (!c->lj_inr || !c->lj_inr_cnt || !T.cnt || !T.list || !T.pos0)
+        return fail(MDG_ERR_CUDA, "cudaMalloc (LJ in-range lists)");
     }
     int rc = nsys > 1 ? setup_grid_batch(c, l, hpos) : setup_grid(c, l, hpos);
     if (rc) return rc;
   }
-  int one[3] = {1, 1, 1};
+  int one[4] = {1, 1, 1, 1};
   CK(cudaMemcpy(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice));
-  c->d_part = dalloc<double>(2 * 3 * kDispParts);
+  c->d_part = dalloc<double>(2 * 4 * kDispParts);
   if (c->has_list[2]) {
     if (!c->d_metal) {
       MetalParams hmp;
@@ -2378,6 +2457,9 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     c->special_blocks = sms * 8;
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_lj_filter, kThreads, 0);
+    c->warp_blocks = sms * (per > 0 ? per : 1);
   }
   if (cudaHostAlloc((void**)&c->h_stage, 2 * (size_t)n * sizeof(double4), cudaHostAllocDefault) != cudaSuccess)
     return fail(MDG_ERR_CUDA, "cudaHostAlloc (staging)");
@@ -2522,7 +2604,7 @@ int mdg_nl_update(mdg_ctx* c, int force, int32_t* rebuilt)
 {
   if (!c || !c->n) return fail(MDG_ERR_STATE, "no system loaded");
   if (force) {
-    const int one[3] = {1, 1, 1};
+    static const int one[4] = {1, 1, 1, 1};
     CK(cudaMemcpyAsync(c->d_force, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
   }
   int rc = rebuild_lists(c);
