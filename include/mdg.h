@@ -81,8 +81,9 @@ typedef struct mdg_params {
                          0 = default (48) */
   int device;         /* CUDA device ordinal */
   int bond_rec_avg;   /* capacity of the per-bond REBO records over the whole system, doubles per
-                         atom on average (a bond slot of an atom with b bonds takes 5 + 4b);
-                         0 = default (174: six bonds per atom) */
+                         atom on average (a bond slot of an atom with b bonds takes 5 + 4b, and in
+                         the lane-pair split each C-C bond adds a torsion record of that size);
+                         0 = default (256: five bonds per atom in every split) */
   int task_mode;      /* REBO work split: 1 = one task per directed bond (both ends evaluate each
                          bond, shortest critical path), 2 = one task per bond writing both ends'
                          records (half the work), 3 = per bond on a pair of lanes, each lane the

@@ -2084,7 +2084,7 @@ int mdg_create(const mdg_params* p, mdg_ctx** out)
   mdg_ctx* c = new mdg_ctx();
   c->prm = *p;
   if (c->prm.cap_bonds <= 0) c->prm.cap_bonds = 16;
-  if (c->prm.bond_rec_avg <= 0) c->prm.bond_rec_avg = 6 * (5 + 4 * 6);
+  if (c->prm.bond_rec_avg <= 0) c->prm.bond_rec_avg = 256;
   if (c->prm.cap_rebo_list <= 0) c->prm.cap_rebo_list = 64;
   if (c->prm.cap_lj_list <= 0) c->prm.cap_lj_list = 512;
   if (c->prm.cap_cij <= 0) c->prm.cap_cij = 128;

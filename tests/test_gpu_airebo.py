@@ -98,6 +98,25 @@ def test_md_run_tracks_oracle():
     assert np.abs(vel - out["vel"]).max() < 1e-9
 
 
+def test_lj_near_sublist_through_rebuilds():
+    # A hot liquid moves its atoms several Angstrom in 300 steps, so the LJ
+    # list's 0.5 A near sublist (which the in-range filter reads) is taken
+    # again many times and the LJ list itself too; the forces at the end equal
+    # the oracle's, whose lists are built afresh at those positions.
+    s = B.ethane_liquid(30, seed=39, temp_k=2000.0)
+    ctx = _gpu(s)
+    ctx.run(300, 0.25, energies=False)
+    pos, vel, _ = ctx.get_state()
+    moved = pos - s["pos"]
+    moved -= s["box"] * np.round(moved / s["box"])
+    assert np.sqrt((moved ** 2).sum(1)).max() > 2.0
+    e, et, g = ctx.compute()
+    s2 = dict(s, pos=pos, vel=vel)
+    eo, eto, go = _oracle(s2).compute()
+    floor = oracle_floor(lambda: ref.RefSystem(ref.POT_AIREBO), s2)
+    assert_parity(e, g, eo, go, floor, label="hot ethane30 after 300 steps")
+
+
 def test_deterministic_repeat():
     s = SYSTEMS["diamond4_hot"]()
     ctx = _gpu(s)

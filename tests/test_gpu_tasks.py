@@ -50,6 +50,16 @@ def test_task_modes_same_trajectory(mode):
     assert np.abs(a.get_state()[0] - b.get_state()[0]).max() < 1e-10
 
 
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_hot_diamond_runs_in_every_split(mode):
+    # atoms pushed 0.25 A off the lattice heat up and some take a fifth
+    # bond: the default record capacity holds every split's records
+    s = B.diamond(4, disp_sigma=0.25, seed=33)
+    c = _ctx(s, mode)
+    c.run(20, 0.25, energies=False)
+    assert np.isfinite(c.get_state()[0]).all()
+
+
 def test_autotuner_picks_a_mode():
     s = SYSTEMS["ach300"]()
     c = _ctx(s, 0)
