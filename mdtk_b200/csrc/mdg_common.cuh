@@ -4,6 +4,7 @@
 // Internal units: Angstrom, eV, fs, amu.  The reference works in CGS
 // (mdtk/consts.cxx:28-36); conversion happens only at the C ABI edge.
 #pragma once
+#include <type_traits>
 
 #include <stdint.h>
 #include <math.h>
@@ -269,8 +270,15 @@ MDG_HD void cutoff(Real r, double R1, double R2, Real& f, Real& df)
 {
   if (r < R1) { f = 1.0; df = 0.0; return; }
   if (r < R2) {
-    f = (1.0 + cos(kPi * (r - R1) / (R2 - R1))) / 2.0;
-    df = (-(kPi / (R2 - R1)) * sin(kPi * (r - R1) / (R2 - R1))) / 2.0;
+    if constexpr (std::is_same<Real, double>::value) {
+      double sn, cs;
+      sincos(kPi * (r - R1) / (R2 - R1), &sn, &cs);
+      f = (1.0 + cs) / 2.0;
+      df = (-(kPi / (R2 - R1)) * sn) / 2.0;
+    } else {
+      f = (1.0 + cos(kPi * (r - R1) / (R2 - R1))) / 2.0;
+      df = (-(kPi / (R2 - R1)) * sin(kPi * (r - R1) / (R2 - R1))) / 2.0;
+    }
     return;
   }
   f = 0.0;
