@@ -12,6 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmdg.so")
+# the per-kernel timeline build (MDG_TIMELINE: pdl_enter() stamps the global
+# timer; see mdtk_b200/timeline.py), a separate library never loaded by default
+OUT_TIMELINE = os.path.join(HERE, "libmdg_timeline.so")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -30,18 +33,21 @@ def headers():
         os.path.join(ROOT, "include", "mdg.h")]
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(OUT):
+def up_to_date(out: str = OUT) -> bool:
+    if not os.path.exists(out):
         return False
-    t = os.path.getmtime(OUT)
+    t = os.path.getmtime(out)
     return all(os.path.getmtime(f) <= t for f in sources() + headers())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return OUT
+def build(force: bool = False, verbose: bool = False, timeline: bool = False) -> str:
+    out = OUT_TIMELINE if timeline else OUT
+    if not force and up_to_date(out):
+        return out
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-shared", *sources(), "-lz", "-o", OUT]
+    extra = ["-DMDG_TIMELINE"] if timeline else []
+    cmd = [nvcc, *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-shared", *sources(), "-lz",
+           "-o", out]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -50,8 +56,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libmdg.so")
     if verbose:
         sys.stderr.write(r.stderr)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, timeline="--timeline" in sys.argv))

@@ -3250,6 +3250,31 @@ __global__ void k_floor_coop(int phases)
   for (int p = 0; p < phases; p++) g.sync();
 }
 
+#if defined(MDG_TIMELINE)
+// The timeline build's stamps (see pdl_enter): reset before a step, read
+// after it; slot = the source line of a kernel's pdl_enter() in this file.
+int mdg_timeline_reset(void)
+{
+  static unsigned long long hi[kTimelineSlots], lo[kTimelineSlots];
+  for (int i = 0; i < kTimelineSlots; i++) { hi[i] = ~0ull; lo[i] = 0ull; }
+  if (cudaMemcpyToSymbol(g_tl_start, hi, sizeof(hi)) != cudaSuccess ||
+      cudaMemcpyToSymbol(g_tl_wait, hi, sizeof(hi)) != cudaSuccess ||
+      cudaMemcpyToSymbol(g_tl_end, lo, sizeof(lo)) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+    return fail(MDG_ERR_CUDA, "timeline reset");
+  return MDG_OK;
+}
+int mdg_timeline_read(uint64_t* start, uint64_t* wait, uint64_t* end, int slots)
+{
+  if (slots < kTimelineSlots) return fail(MDG_ERR_ARG, "timeline arrays hold kTimelineSlots entries");
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpyFromSymbol(start, g_tl_start, kTimelineSlots * 8) != cudaSuccess ||
+      cudaMemcpyFromSymbol(wait, g_tl_wait, kTimelineSlots * 8) != cudaSuccess ||
+      cudaMemcpyFromSymbol(end, g_tl_end, kTimelineSlots * 8) != cudaSuccess)
+    return fail(MDG_ERR_CUDA, "timeline read");
+  return MDG_OK;
+}
+#endif
+
 int mdg_launch_floor(int device, int phases, double* graph_us, double* coop_us)
 {
   if (!graph_us || !coop_us || phases < 1 || phases > 1000) return fail(MDG_ERR_ARG, "bad argument");

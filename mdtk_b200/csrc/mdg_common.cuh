@@ -55,11 +55,45 @@ enum StatusBits : unsigned int {
 // are visible (griddepcontrol.wait, a no-op for a kernel launched without the
 // attribute), and then lets the next grid be scheduled in turn.  Completion
 // is thereby transitive along the stream, as with ordinary launches.
+#if !defined(MDG_TIMELINE)
 __device__ __forceinline__ void pdl_enter()
 {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+#else
+// The timeline build (python -m mdtk_b200.build --timeline, a separate
+// library): pdl_enter() also stamps, per kernel (keyed by the source line of
+// its pdl_enter() call), the global timer when the first block started, when
+// it passed the wait, and when the last warp left (a destructor on every
+// return path).  Atomics on 8192-entry arrays; read back by
+// mdg_timeline_read.  Never in the product library.
+constexpr int kTimelineSlots = 8192;
+__device__ unsigned long long g_tl_start[kTimelineSlots];
+__device__ unsigned long long g_tl_wait[kTimelineSlots];
+__device__ unsigned long long g_tl_end[kTimelineSlots];
+__device__ __forceinline__ unsigned long long tl_now()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+struct TimelineStamp {
+  int id;
+  __device__ __forceinline__ explicit TimelineStamp(int line) : id(line % kTimelineSlots)
+  {
+    if (threadIdx.x == 0) atomicMin(&g_tl_start[id], tl_now());
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (threadIdx.x == 0) atomicMin(&g_tl_wait[id], tl_now());
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  }
+  __device__ __forceinline__ ~TimelineStamp()
+  {
+    if ((threadIdx.x & 31) == 0) atomicMax(&g_tl_end[id], tl_now());
+  }
+};
+#define pdl_enter() TimelineStamp mdg_timeline_stamp_(__LINE__)
+#endif
 #endif
 
 // FP32 scalar of the mixed-precision path: float arithmetic; double operands
