@@ -1802,7 +1802,7 @@ inline void launch_kernel(bool pdl, cudaStream_t st, void (*k)(P...), dim3 grid,
 // The displacement partials of both lists (after the step's position update
 // when a step is given; before it, the bath temperature) in one pass over
 // the atoms.
-constexpr int kDispParts = 296;  // 2 blocks per SM of a B200
+constexpr int kDispParts = 592;  // 4 blocks per SM of a B200: at most one atom per thread on the liquid
 constexpr int kMetalListCap = 320;  // metal / ion list partners per atom (fcc Cu holds ~180 within 7.92 A)
 constexpr int kBathBlocks = 120;
 int step_start(mdg_ctx* c, const StepDev* step)
