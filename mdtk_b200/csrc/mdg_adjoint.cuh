@@ -397,10 +397,8 @@ int adj_dual_pass(mdg_ctx* c, int transpose = 1)
     Tk.task_cap = P.task_cap;
     Tk.rec_cap = P.rec_cap;
     Tk.cnt = P.cnt;
-    Tk.rsz = P.rsz;
     Tk.part = P.part;
     Tk.off = P.off;
-    Tk.roff = P.roff;
     Tk.flat = P.flat;
     Tk.trec = P.trec;
     Tk.ctr = P.ctr;

@@ -875,8 +875,6 @@ __device__ __forceinline__ void lj_pairs_block(const LJParams& P, const CijTable
     O.glj[a] = make_double4(gx, gy, gz, 0.0);
     O.e_lj[a] = e;
     Tk.cnt[a] = nsp;
-    Tk.rsz[a] = nsp * rs;
-    Tk.roff[a] = ro;
     if (o + nsp > Tk.task_cap) atomicOr(status, ST_RECORD_OVERFLOW);
     Tk.off[a] = o < Tk.task_cap ? (int)o : Tk.task_cap;
   }
@@ -1605,7 +1603,7 @@ void free_system(mdg_ctx* c)
     std::memset(&c->grid[l], 0, sizeof(Grid));
     c->has_list[l] = false;
   }
-  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.rsz, c->spc.part, c->spc.off, c->spc.roff,
+  void* lq[] = {c->cij.cnt, c->cij.ent, c->cij.w, c->cij.mask, c->spc.cnt, c->spc.part, c->spc.off,
                 c->spc.flat, c->spc.trec, c->spc.rec, c->spc.mid, c->spc.midc, c->spc.work,
                 c->spc.ctr, c->lj_inr, c->lj_inr_cnt, c->ljt.cnt, c->ljt.list, c->ljt.pos0};
   std::memset(&c->ljt, 0, sizeof(NList));
@@ -2435,10 +2433,8 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     X.task_cap = (int)std::min<long>((long)n * c->prm.special_avg, 1L << 30);
     X.rec_cap = (long)X.task_cap * rec_size(6);
     X.cnt = dalloc<int>(n);
-    X.rsz = dalloc<int>(n);
     X.part = dalloc<int>((size_t)n * X.cap);
     X.off = dalloc<int>(n);
-    X.roff = dalloc<long>(n);
     X.flat = dalloc<int2>(X.task_cap);
     X.trec = dalloc<long>(X.task_cap);
     X.rec = dalloc<double>(X.rec_cap);
@@ -2448,7 +2444,7 @@ static int set_systems(mdg_ctx* c, int nsys, const int64_t* first, const int32_t
     X.ctr = dalloc<unsigned long long>(3 * kCtrStride);
     if (!X.work || !X.ctr) return fail(MDG_ERR_CUDA, "cudaMalloc (LJ work list)");
     CK(cudaMemset(X.ctr, 0, 3 * kCtrStride * sizeof(unsigned long long)));
-    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->cij.mask || !X.cnt || !X.rsz || !X.part || !X.off || !X.roff || !X.flat ||
+    if (!c->cij.cnt || !c->cij.ent || !c->cij.w || !c->cij.mask || !X.cnt || !X.part || !X.off || !X.flat ||
         !X.trec || !X.rec || !X.mid || !X.midc)
       return fail(MDG_ERR_CUDA, "cudaMalloc (LJ)");
     CK(cudaMemset(X.cnt, 0, n * sizeof(int)));

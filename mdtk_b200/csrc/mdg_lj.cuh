@@ -424,18 +424,17 @@ typedef LJT<double, ReboTables> LJ;
 // evaluated one task per (atom, pair); each task writes its own record and a
 // per-atom pass sums an atom's records in list order.  An atom's tasks take
 // the contiguous range [off[a], off[a] + cnt[a]) of the task arrays and its
-// records the range from roff[a]; where those ranges lie depends on
-// scheduling (one atomicAdd per block), the order within them does not.
+// records one contiguous range of the record pool; where those ranges lie depends on
+// scheduling (one atomicAdd per block), the order within them does not; trec
+// holds each task's record offset.
 template <class W>
 struct SpecialTasksT {
   int cap;          // special pairs per atom
   int task_cap;     // total tasks
   long rec_cap;     // total record doubles
   int* cnt;         // [n] special pairs of each atom (LJ-list order)
-  int* rsz;         // [n] record doubles of each atom: cnt * rec_size(bonds)
   int* part;        // [n * cap] partner of each
   int* off;         // [n] first task of each atom
-  long* roff;       // [n] first record double of each atom
   int2* flat;       // [task_cap] (atom, partner)
   long* trec;       // [task_cap] record offset of each task (-1: beyond rec_cap)
   W* rec;           // [rec_cap] per task: own gradient xyz, energy, A[nb][3], W[nb]

@@ -102,3 +102,14 @@ def test_no_device_fails_loudly():
     with pytest.raises(M.MdgError) as e:
         M.Context(potentials=M.POT_REBO)
     assert e.value.code == -2
+
+
+def test_timeline_names_every_kernel_entry():
+    # the timeline build keys its stamps by the source line of pdl_enter();
+    # every such line in mdg_api.cu maps to the kernel that opens it
+    from mdtk_b200 import timeline
+    names = timeline.kernel_names()
+    assert len(names) >= 30
+    assert "?" not in names.values()
+    for k in ("k_step_start", "k_lj_near", "k_lj_filter", "k_lj_pairs", "k_lj_special_pair", "k_gather_vv"):
+        assert k in names.values(), k
