@@ -574,6 +574,15 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
   // the LJ pass over REBO sums already in place: an atom without special
   // pair records keeps every element as it is
   if (!rebo_tasks && with_lj && t1 <= t0) return;
+  // an atom's special-pair records are handed out as one block, rec_size(nb)
+  // doubles apart: when its first and last lie so (none beyond the pool),
+  // every element reads them by stride instead of through trec
+  long lbase = -1;
+  const int lrs = rec_size(nb);
+  if (with_lj && t1 > t0) {
+    const long f = Tk.trec[t0], z = Tk.trec[t1 - 1];
+    if (f >= 0 && z == f + (long)(t1 - 1 - t0) * lrs) lbase = f;
+  }
   for (int e = l; e < nel; e += G) {
     int roff = -1, loff = -1;
     double* dst;
@@ -594,7 +603,10 @@ __global__ void k_bond_reduce(BondList B, BondTasks K, int rebo_tasks, SpecialTa
     double acc = roff >= 0 ? 0.0 : *dst;
     if (roff >= 0 && rb >= 0)
       for (int s = 0; s < nrec; s++) acc += K.rec[rb + (long)s * rs + roff];
-    if (loff >= 0) {
+    if (loff >= 0 && lbase >= 0) {
+      const double* r = Tk.rec + lbase + loff;
+      for (int t = 0; t < t1 - t0; t++) acc += r[(long)t * lrs];
+    } else if (loff >= 0) {
       int t = t0;
       for (; t + 3 < t1; t += 4) {
         const long r0 = Tk.trec[t], r1 = Tk.trec[t + 1], r2 = Tk.trec[t + 2], r3 = Tk.trec[t + 3];
