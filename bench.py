@@ -818,7 +818,7 @@ STEP_FLOPS_PER_ATOM = 2541.0 + 504.0 + 10357.0
 # autotuner's choice: "per bond", "directed" or "lane pairs"); None when not
 # captured.
 TRAFFIC_PER_LAUNCH = {
-    ("rebo_tors", "per bond"): 10.91e6, ("rebo_tors", "directed"): 22.83e6,
+    ("rebo_tors", "per bond"): 10.88e6, ("rebo_tors", "directed"): 22.83e6,
     ("rebo_tors", "lane pairs"): 13.6e6,
 }
 
